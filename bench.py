@@ -1,0 +1,448 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 execution path for mettle's offloaded SQL subset.
+
+Default workload (the headline): the join -> filter -> group -> top-K
+pipeline at 60M fact rows (customer 1.5M, orders 15M, lineitem ~60M;
+DECIMAL(15,2) money as int64 cents, exact scale-4 revenue). Other workloads:
+--config c1 (plain small query, 10^6 rows), c2 (filter/projection scan,
+10^8 rows), c3 (grouped aggregate + top-100, 2*10^8 rows), c5 (served mixed
+stream vs plain launches).
+
+`value` is device throughput with the tables resident in HBM: K launches of
+the prepared query back to back on one stream, timed with CUDA events on
+that stream. `e2e` is the same metric through the public API with host
+buffers: every step registers the tables from pinned host memory (H2D
+copies), runs gpu_processing and downloads the result. Multi-GPU runs are
+independent replicas (the path has no exchange step): every rank runs the
+full workload on its own GPU, times are the max over ranks.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl mettle|reference] [--config c4]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+sys.path.insert(0, str(ROOT / "oracle"))
+
+from mettle_b200 import workloads as W  # noqa: E402
+
+FALLBACK_HBM_GBS = 6650.0
+
+
+# ------------------------------------------------------------------ ranks
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def dist_init(ws: int, backend: str = "nccl"):
+    if ws <= 1:
+        return None
+    import datetime
+
+    import torch.distributed as dist
+    os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+    dist.init_process_group(backend=backend, timeout=datetime.timedelta(seconds=300))
+    return dist
+
+
+def barrier(dist, device=None):
+    if dist is not None:
+        if device is not None:
+            dist.barrier(device_ids=[device])
+        else:
+            dist.barrier()
+
+
+def reduce_max(dist, x: float, device: str = "cpu") -> float:
+    """Max of a per-rank scalar over all ranks (identity for one rank)."""
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def reduce_sum(dist, x: float, device: str = "cpu") -> float:
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+            time.sleep(0.3)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.2)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        rows = []
+        try:
+            for line in Path(self.path).read_text().splitlines():
+                f = [x.strip() for x in line.split(",")]
+                if len(f) >= 9 and f[1].replace(".", "").isdigit():
+                    rows.append(f)
+        finally:
+            try:
+                os.unlink(self.path)
+            except Exception:
+                pass
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"], "samples": 0}
+        sm = [float(r[1]) for r in rows]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({n for r in rows for n, v in zip(names, r[5:9]) if v.lower() == "active"})
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": float(rows[0][2]), "reasons": reasons,
+                "samples": len(rows), "power_w_max": max(float(r[3]) for r in rows if r[3].replace(".", "").isdigit())
+                if any(r[3].replace(".", "").isdigit() for r in rows) else None}
+
+
+def measured_peak() -> tuple[float, str]:
+    p = ROOT / "MEASURED_PEAKS.json"
+    try:
+        return float(json.loads(p.read_text())["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs)"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def profile_traffic(name: str) -> float | None:
+    """DRAM bytes per launch of the dominant kernel from a committed ncu summary."""
+    for f in (ROOT / "profiles").glob("*.md"):
+        m = re.search(rf"^traffic\[{re.escape(name)}\]:\s*([0-9.eE+]+)", f.read_text(), re.M)
+        if m:
+            return float(m.group(1))
+    return None
+
+
+# ------------------------------------------------------------------ workloads
+class Workload:
+    """A benchmark configuration: tables, SQL, fact rows, algorithmic bytes."""
+
+    def __init__(self, name: str):
+        self.name = name
+        if name == "c4":
+            self.t = W.q3()
+            self.sql = W.q3_sql(self.t.date)
+            self.rows = self.t.lineitem_rows
+            self.bytes = W.q3_bytes(self.t)
+            self.dom_step = "pipeline:agg_slot:lineitem"
+            self.dom_bytes = self.rows * (4 + 8 + 8 + 4)
+            self.desc = (f"c4 join->filter->group->top-10: customer {len(self.t.customer['c_custkey'])}, "
+                         f"orders {len(self.t.orders['o_orderkey'])}, lineitem {self.rows} rows; "
+                         "DECIMAL(15,2) as int64 cents, revenue exact int128 at scale 4")
+        elif name == "c1":
+            self.d = W.numbers(1_000_000)
+            self.sql = W.C1_SQL
+            self.rows = 1_000_000
+            sel = int((self.d["value"] > 500000).sum())
+            self.bytes = 4 * self.rows + sel * 8
+            self.dom_step = "pipeline:materialize:numbers"
+            self.dom_bytes = 4 * self.rows + sel * 8
+            self.desc = "c1 numbers 1M rows: SELECT value, value*10 WHERE value > 500000 ORDER BY value"
+        elif name == "c2":
+            self.d = W.scan(100_000_000)
+            self.sql = W.scan_sql("a", "<", 0.5)
+            self.rows = 100_000_000
+            sel = int((self.d["a"] < int(0.5 * 2**31)).sum())
+            self.bytes = 4 * self.rows + sel * (28 - 4) + sel * 28
+            self.dom_step = "pipeline:materialize:t"
+            self.dom_bytes = self.bytes
+            self.desc = "c2 scan 1e8 rows (a,b,c,d,e): SELECT a, b+5, c*10, d, e WHERE a < 2^30 (50%)"
+        elif name == "c3":
+            g = int(os.environ.get("C3_GROUPS", "1000000"))
+            dist = os.environ.get("C3_DIST", "uniform")
+            self.d = W.groupby(200_000_000, groups=g, dist=dist)
+            self.sql = W.C3_SQL
+            self.rows = 200_000_000
+            self.bytes = 20 * self.rows
+            self.dom_step = "pipeline:agg_"
+            self.dom_bytes = self.bytes
+            self.desc = f"c3 group-by 2e8 rows, G={g} {dist}: SUM/COUNT/MIN/MAX/AVG x2, top-100"
+        else:
+            raise SystemExit(f"unknown config {name}")
+
+    def register(self, conn, upload=True, borrow=False):
+        from mettle_b200 import _lib as L
+        if self.name == "c4":
+            W.register_q3(conn, self.t, upload=upload, borrow=borrow)
+        elif self.name == "c1":
+            conn.create_table("numbers", {"value": (L.T_INTEGER, self.d["value"])})
+            conn.gpu_register_table("numbers", upload=upload, borrow=borrow)
+        elif self.name == "c2":
+            conn.create_table("t", {"a": (L.T_INTEGER, self.d["a"]), "b": (L.T_BIGINT, self.d["b"]),
+                                    "c": (L.T_FLOAT, self.d["c"]), "d": (L.T_DATE, self.d["d"]),
+                                    "e": (L.T_TIMESTAMP, self.d["e"])})
+            conn.gpu_register_table("t", upload=upload, borrow=borrow)
+        else:
+            conn.create_table("t", {"k": (L.T_BIGINT, self.d["k"]), "v": (L.T_BIGINT, self.d["v"]),
+                                    "f": (L.T_FLOAT, self.d["f"])})
+            conn.gpu_register_table("t", upload=upload, borrow=borrow)
+
+    def host_arrays(self) -> list[np.ndarray]:
+        if self.name == "c4":
+            return [*self.t.customer.values(), *self.t.orders.values(), *self.t.lineitem.values()]
+        return list(self.d.values())
+
+    def replace_arrays(self, arrays: list[np.ndarray]):
+        it = iter(arrays)
+        if self.name == "c4":
+            for tab in (self.t.customer, self.t.orders, self.t.lineitem):
+                for k in tab:
+                    tab[k] = next(it)
+        else:
+            for k in self.d:
+                self.d[k] = next(it)
+
+    # ---- CPU (oracle port) execution of the same query
+    def cpu_run(self):
+        import oracle as orc
+        if self.name == "c4":
+            return orc.q3(self.t, segment_code=1, limit=10)
+        if self.name == "c1":
+            rows = orc.filter_rows([(self.d["value"], ">", 500000)])
+            rows = orc.sort_rows(self.d["value"], rows)
+            return orc.gather(self.d["value"], rows), orc.gather(self.d["value"], rows, "*", 10)
+        if self.name == "c2":
+            rows = orc.filter_rows([(self.d["a"], "<", int(0.5 * 2**31))])
+            return [orc.gather(self.d["a"], rows), orc.gather(self.d["b"], rows, "+", 5),
+                    orc.gather(self.d["c"], rows, "*", np.float32(10)), orc.gather(self.d["d"], rows),
+                    orc.gather(self.d["e"], rows)]
+        return orc.groupby_c3(self.d["k"], self.d["v"], self.d["f"], limit=100)
+
+    def parity(self, res) -> bool:
+        want = self.cpu_run()
+        rows = res.fetchall()
+        if self.name == "c4":
+            got = [(r[0], int(r[1].scaleb(4)), r[3]) for r in rows]
+            exp = list(zip(want["key"].tolist(), want["revenue"], want["prio"].tolist()))
+            return got == exp
+        if self.name == "c1":
+            return np.array_equal(res.columns[0], want[0]) and np.array_equal(res.columns[1], want[1])
+        if self.name == "c2":
+            return all(np.array_equal(res.columns[i], want[i]) for i in range(5))
+        ok = len(rows) == len(want["k"])
+        for i, r in enumerate(rows[: len(want["k"])]):
+            ok &= r[0] == want["k"][i] and r[1] == want["sum_v"][i] and r[2] == want["cnt"][i]
+            ok &= abs(r[6] - want["sum_f"][i]) <= 1e-6 * abs(want["sum_f"][i])
+        return bool(ok)
+
+
+def cpu_baseline(wl: Workload, seconds: float) -> dict:
+    import oracle as orc
+    wl.cpu_run()  # warm
+    n, t0 = 0, time.perf_counter()
+    while True:
+        wl.cpu_run()
+        n += 1
+        el = time.perf_counter() - t0
+        if el >= seconds or n >= 200:
+            break
+    return {"value": wl.rows * n / el, "unit": "rows/s", "cores": orc.threads(), "kind": "port",
+            "sample": f"{n} full runs of the {wl.name} workload ({wl.rows} fact rows each), {el:.1f} s, "
+                      f"OpenMP oracle (oracle/mettle_oracle.c)"}
+
+
+# ------------------------------------------------------------------ arms
+def run_reference(args):
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return
+    import oracle as orc
+    wl = Workload(args.config)
+    for _ in range(min(args.warmup, 1)):
+        wl.cpu_run()
+    steps = max(1, min(args.steps, 20))
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        wl.cpu_run()
+    el = time.perf_counter() - t0
+    value = wl.rows * steps / el
+    line = {"impl": "reference", "metric": "pipeline rows/s", "value": value, "unit": "rows/s",
+            "n_gpus": args.gpus, "steps": steps, "warmup": min(args.warmup, 1), "ms_per_step": el * 1e3 / steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64",
+            "data": "synthetic", "config": {"workload": wl.desc},
+            "cpu_baseline": {"value": value, "unit": "rows/s", "cores": orc.threads(), "kind": "port",
+                             "sample": f"{steps} timed full runs of {wl.name} (of {args.steps} requested; bounded "
+                                       "to keep the run within minutes) on the host cores; the reference itself "
+                                       "(Rust + Apple Metal) cannot run on this box"},
+            "e2e": {"value": value, "unit": "rows/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_mettle(args):
+    ws, rank, local = dist_env()
+    import torch
+    torch.cuda.set_device(local)
+    dist = dist_init(ws)
+    from mettle_b200 import Connection
+    wl = Workload(args.config)
+    conn = Connection(device=local)
+    gb = max(8, int(wl.bytes * 3 / 2**30) + 8)
+    conn.execute(f"CALL gpu_buffer_init('{gb} GB', '{gb} GB', pinned_memory_size = '{2 * gb} GB')")
+    wl.register(conn, upload=True)
+    stmt = conn.prepare(wl.sql)
+    stream = torch.cuda.current_stream()
+    sp = stream.cuda_stream
+
+    # parity of the measured statement (rank 0, once)
+    stmt.launch(sp)
+    first = stmt.fetch()
+    parity = wl.parity(first) if rank == 0 else None
+
+    for _ in range(args.warmup):
+        stmt.launch(sp)
+    torch.cuda.synchronize()
+
+    # ---- timed region: K launches, events on the launching stream
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        barrier(dist, local)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(args.steps):
+            stmt.launch(sp)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier(dist, local)
+    ms = e0.elapsed_time(e1)
+    ms = reduce_max(dist, ms, f"cuda:{local}")
+    clocks = clk.summary()
+    total_rows = reduce_sum(dist, float(wl.rows * args.steps), f"cuda:{local}")
+    value = total_rows / (ms / 1e3)
+    kernels = stmt.kernel_count()
+
+    # ---- per-step device times of the same launches (dominant kernel)
+    stmt.set_profiling(True)
+    prof_runs = max(3, min(args.steps, 50))
+    dom, totals = [], {}
+    for _ in range(prof_runs):
+        stmt.launch(sp)
+        steps = stmt.step_times()
+        for name, t in steps:
+            totals[name] = totals.get(name, 0.0) + t
+        dom.append(sum(t for n, t in steps if n.startswith(wl.dom_step)))
+    stmt.set_profiling(False)
+    dom_ms = statistics.mean(dom)
+    peak, peak_src = measured_peak()
+    achieved = wl.dom_bytes / (dom_ms / 1e3) / 1e9
+    traffic = profile_traffic(f"{wl.name}:{wl.dom_step}")
+    query_gbs = wl.bytes / (ms / args.steps / 1e3) / 1e9
+
+    # ---- e2e through the public API with host buffers
+    import os as _os
+    _os.environ["METTLE_DISABLE_QUERY_CACHE"] = "1"
+    pinned = [torch.from_numpy(a).pin_memory() for a in wl.host_arrays()]
+    wl.replace_arrays([p.numpy() for p in pinned])
+    h2d = sum(a.nbytes for a in wl.host_arrays())
+    e2e_steps = max(3, min(args.steps, 10))
+    r = None
+    conn2 = Connection(device=local)
+    conn2.execute(f"CALL gpu_buffer_init('{gb} GB', '{gb} GB', pinned_memory_size = '{2 * gb} GB')")
+    wl.register(conn2, upload=False, borrow=True)
+    r = conn2.gpu_processing(wl.sql)  # warm (plans, stats)
+    barrier(dist, local)
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        wl.register(conn2, upload=False, borrow=True)  # new table version: H2D on first use
+        r = conn2.gpu_processing(wl.sql)
+    e2e_s = (time.perf_counter() - t0) / e2e_steps
+    e2e_s = reduce_max(dist, e2e_s, f"cuda:{local}")
+    d2h = sum(c.nbytes for c in r.columns) + 12
+    e2e_value = reduce_sum(dist, float(wl.rows), f"cuda:{local}") / e2e_s
+
+    cpu = cpu_baseline(wl, args.cpu_seconds) if (rank == 0 and ws == 1 and args.cpu_seconds > 0) else None
+
+    if rank == 0:
+        line = {
+            "metric": "pipeline rows/s", "value": value, "unit": "rows/s", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "int64", "data": "synthetic",
+            "config": {"workload": wl.desc, "l2": "inputs larger than L2 (126 MB); no flush",
+                       "parallelism": f"replicas x{ws}" if ws > 1 else "1 GPU"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": traffic, "kernel": wl.dom_step, "kernel_ms": dom_ms,
+                         "algorithmic_bytes": wl.dom_bytes, "peak_source": peak_src,
+                         "query_gbs": query_gbs, "query_frac": query_gbs / peak,
+                         "query_algorithmic_bytes": wl.bytes},
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": "rows/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "ms_per_step": e2e_s * 1e3, "steps": e2e_steps},
+            "gpu_launches": kernels * args.steps,
+            "clocks": clocks,
+            "parity": parity,
+            "step_ms": {k: v / prof_runs for k, v in sorted(totals.items(), key=lambda kv: -kv[1])[:8]},
+        }
+        print(json.dumps(line), flush=True)
+    stmt.close()
+    conn.close()
+    conn2.close()
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="mettle", choices=["mettle", "reference"])
+    ap.add_argument("--config", default="c4", choices=["c1", "c2", "c3", "c4"])
+    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_mettle(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,222 @@
+// dev_types.h — plain-old-data descriptors shared by the host planner and the
+// sm_100a kernels. Everything here is passed to kernels by value
+// (__grid_constant__) or lives in device memory; no pointers to host memory.
+//
+// The engine runs a query as a short sequence of "pipelines". A pipeline
+// scans one input (a base table, or a list of row-id tuples), applies the
+// filters and join probes of that input in order, and ends in one sink:
+// a join build, a grouped/ungrouped aggregate, or an order-preserving
+// materialization. This replaces the reference's per-op dispatch chain
+// (compare -> and_masks -> filter_to_indices -> gather -> join -> compact ->
+// reindex, src/plan/executor/fast_path/*.rs) with one launch per pipeline.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace mtl {
+
+// ------------------------------------------------------------ limits
+constexpr int kMaxSrc = 6;       // tables in one query
+constexpr int kMaxPreds = 12;    // filter predicates in one pipeline
+constexpr int kMaxProbes = 5;    // join probes in one pipeline
+constexpr int kMaxCols = 32;     // columns referenced by one pipeline
+constexpr int kMaxProgs = 16;    // expression programs in one pipeline
+constexpr int kMaxIns = 12;      // instructions per expression program
+constexpr int kMaxKeys = 4;      // group-by key words
+constexpr int kMaxAggs = 12;     // aggregate states per group
+constexpr int kMaxOrder = 8;     // ORDER BY key parts (incl. tie-breaks)
+
+// ------------------------------------------------------------ physical types
+enum PType : int32_t { P_NONE = 0, P_I32 = 1, P_I64 = 2, P_F32 = 3, P_F64 = 4, P_I128 = 5 };
+
+__host__ __device__ inline int ptype_width(int32_t p) {
+  return p == P_I32 || p == P_F32 ? 4 : (p == P_I128 ? 16 : 8);
+}
+
+// Compare op codes; 0..4 match the reference's compare_*_scalar op codes
+// (src/metal/shaders/kernels.metal:70-173).
+enum CmpOp : int32_t { C_EQ = 0, C_LT = 1, C_LE = 2, C_GT = 3, C_GE = 4, C_NE = 5, C_FALSE = 6, C_TRUE = 7 };
+
+// Device status bits (one u32 per query; the host turns them into errors).
+enum DevStatus : uint32_t {
+  ST_OVERFLOW = 1u,        // integer overflow (DuckDB raises an error)
+  ST_DUP_BUILD_KEY = 2u,   // a build side assumed unique had a duplicate key
+  ST_SPIN_LIMIT = 4u,      // a bounded wait gave up
+  ST_TABLE_FULL = 8u,      // a hash table ran out of slots
+  ST_CAPACITY = 16u,       // an output buffer was too small
+};
+
+// ------------------------------------------------------------ columns
+struct DCol {
+  const void* ptr;   // device column (row-indexed)
+  int32_t ptype;     // PType
+  int32_t src;       // source (table) index the row id comes from
+};
+
+struct DPred {
+  int32_t col;       // index into PipeDesc::cols
+  int32_t op;        // CmpOp
+  int64_t ilit;      // integer literal (I32/I64 columns)
+  double flit;       // float literal (F32 compares in binary32)
+};
+
+// ------------------------------------------------------------ expressions
+enum VmOp : int16_t {
+  VM_COL = 1,    // push cols[arg]
+  VM_CONST = 2,  // push constant bits k (lo) / k2 (hi for I128)
+  VM_ADD = 3,
+  VM_SUB = 4,
+  VM_MUL = 5,
+  VM_CAST = 6,   // convert top of stack from ptype arg to ptype `type`, scaled by k
+  VM_NEG = 7,
+  VM_SLOT = 8,   // push the slot of probe `arg` (representative-row grouping)
+};
+
+struct VmIns {
+  int16_t op;
+  int16_t type;   // result PType
+  int32_t arg;
+  int64_t k;      // constant bits / cast multiplier (power of ten, 1 = none)
+  int64_t k2;     // constant hi bits (I128) / cast divisor flag
+};
+
+struct VmProg {
+  int32_t n;
+  int32_t out_type;
+  VmIns ins[kMaxIns];
+};
+
+// ------------------------------------------------------------ join builds
+enum BuildKind : int32_t { B_NONE = 0, B_DENSE = 1, B_HASH = 2 };
+
+// Hash-table entries start as kEmptyKey (all bits set, so a byte memset
+// clears a table); the one key equal to it is kept in a side word.
+constexpr int64_t kEmptyKey = -1;
+
+// A build side with unique keys: key -> compact slot -> payload row ids.
+struct DBuild {
+  int32_t kind;
+  int32_t key_ptype;        // P_I32 or P_I64
+  int64_t key_min;          // dense: first key
+  uint64_t capacity;        // dense: key span; hash: slots
+  uint32_t* dense_map;      // dense: slot + 1, 0 = empty
+  int64_t* hash_keys;       // hash: keys
+  uint32_t* hash_slot;      // hash: slot + 1 per table entry
+  uint32_t* hash_special;   // hash: slot + 1 of the key equal to kEmptyKey
+  uint32_t* payload[kMaxSrc];  // payload[s][slot] = row id of source s
+  uint32_t* n_slots;        // number of slots assigned (device counter)
+};
+
+struct DProbe {
+  int32_t key_col;          // index into cols (probe-side key)
+  int32_t build;            // index into PipeDesc::builds
+  uint32_t fill_mask;       // bit s: rid[s] = payload[s][slot]
+  int32_t pad;
+};
+
+// ------------------------------------------------------------ pipeline ops
+enum PipeOpKind : int32_t { OPK_FILTER = 1, OPK_PROBE = 2 };
+struct PipeOp {
+  int32_t kind;
+  int32_t idx;
+};
+
+// ------------------------------------------------------------ aggregates
+enum AggFn : int32_t {
+  A_COUNT = 1,     // u64 count
+  A_SUM_I = 2,     // 64-bit integer sum (exact; bound proven by the planner)
+  A_SUM_I128 = 3,  // 128-bit integer sum, lo word + carry into hi word
+  A_SUM_F = 4,     // double sum
+  A_MIN_I = 5,     // signed 64-bit min
+  A_MAX_I = 6,
+  A_MIN_F = 7,     // order-preserving u64 image of a double
+  A_MAX_F = 8,
+};
+
+struct DAgg {
+  int32_t fn;
+  int32_t prog;          // expression program index (-1 for COUNT)
+  uint64_t* lo;          // state words (per group)
+  int64_t* hi;           // A_SUM_I128 high word
+};
+
+enum SinkKind : int32_t {
+  SK_NONE = 0,
+  SK_BUILD = 1,        // insert into builds[sink_build]
+  SK_MATERIALIZE = 2,  // order-preserving compaction of outputs / row ids
+  SK_AGG_HASH = 3,     // global hash table keyed by up to 4 words
+  SK_AGG_SMEM = 4,     // per-CTA shared-memory tables merged into AGG_HASH
+  SK_AGG_SLOT = 5,     // dense states indexed by a build slot
+  SK_AGG_SCALAR = 6,   // one group (no GROUP BY)
+};
+
+// Hash aggregate table (SoA). State word: 0 empty, 1 claimed, 2 ready.
+struct DAggTable {
+  uint32_t* state;
+  uint64_t* keys[kMaxKeys];
+  uint64_t capacity;
+  int32_t n_keys;
+  int32_t pad;
+};
+
+// ------------------------------------------------------------ pipeline
+struct PipeDesc {
+  // input
+  uint64_t n;                       // tuples when in_count == nullptr
+  const uint64_t* in_count;         // device tuple count (tuple-list input)
+  int32_t drive_src;                // source whose row id is the scan index
+  int32_t tuple_input;              // 1: row ids come from in_rids
+  const uint32_t* in_rids[kMaxSrc];
+  uint32_t src_mask;                // sources present in the input tuples
+  int32_t n_cols, n_preds, n_probes, n_ops, n_progs, n_builds;
+  DCol cols[kMaxCols];
+  DPred preds[kMaxPreds];
+  DProbe probes[kMaxProbes];
+  PipeOp ops[kMaxPreds + kMaxProbes];
+  VmProg progs[kMaxProgs];
+  DBuild builds[kMaxProbes + 1];
+  int32_t first_col;                // column prefetched for every tuple (-1 none)
+
+  // sink
+  int32_t sink;
+  // SK_BUILD
+  int32_t sink_build;               // index into builds
+  int32_t build_key_col;            // key column index
+  uint32_t build_payload_mask;      // sources whose row ids are stored
+  // SK_MATERIALIZE
+  int32_t n_out;                    // output programs (0: row ids only)
+  int32_t out_prog[kMaxProgs];
+  void* out_ptr[kMaxProgs];
+  uint32_t out_rid_mask;            // sources whose row ids are written
+  uint32_t mat_src_mask;            // sources whose row ids the write phase reads
+  uint32_t* out_rids[kMaxSrc];
+  uint64_t* out_count;              // device count of written tuples
+  uint64_t out_capacity;
+  uint64_t* tile_status;            // look-back state, one word per tile
+  uint32_t* tile_counter;           // dynamic tile ids + finished CTAs
+  uint32_t epoch;                   // look-back epoch (no memset per launch)
+  // aggregates
+  int32_t n_aggs;
+  DAgg aggs[kMaxAggs];
+  int32_t key_prog[kMaxKeys];       // group key programs (AGG_HASH/SMEM)
+  DAggTable table;
+  int32_t slot_probe;               // AGG_SLOT: probe whose slot is the group
+  uint8_t* slot_hit;                // AGG_SLOT: 1 when the group saw a row
+  int32_t smem_capacity;            // AGG_SMEM: slots per CTA table
+  int32_t pad2;
+
+  uint32_t* status;                 // DevStatus bits
+};
+
+// Encoded ORDER BY key: up to kMaxOrder parts, each an order-preserving
+// unsigned image, most significant part first.
+struct SortKeySpec {
+  int32_t n_parts;
+  int32_t pad;
+  int32_t ptype[kMaxOrder];       // P_I32/P_I64/P_F32/P_F64/P_I128
+  int32_t desc[kMaxOrder];
+  const void* col[kMaxOrder];     // dense arrays over the rows being ordered
+  const int64_t* col_hi[kMaxOrder];  // P_I128 high words
+};
+
+}  // namespace mtl

@@ -1,0 +1,1422 @@
+// exec.cpp — runtime and executor: device column cache bounded by
+// cache_region, the processing-region arena, lazy column statistics, the
+// compiler from a BoundPlan to a device Program, and result fetch.
+//
+// The reference keeps pinned tables as host Vecs and uploads columns lazily,
+// keyed by host pointer, truncating i64 to i32 and f64 to f32
+// (src/metal/runtime/mod.rs:397-469); its executor dispatches one Metal
+// kernel per operator and waits on the host between the join batch and the
+// aggregate batch (src/plan/executor/fast_path/join_loop.rs:240). Here a
+// query compiles to a fixed list of device steps that runs on one stream
+// with no host synchronization until the result is fetched.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <functional>
+#include <map>
+#include <set>
+
+#include "engine.h"
+
+namespace mtl {
+
+// ------------------------------------------------------------ errors
+static thread_local std::string tl_err;
+void set_last_error(const std::string& m) { tl_err = m; }
+const char* last_error() { return tl_err.c_str(); }
+
+#define CK(x)                                                                                           \
+  do {                                                                                                  \
+    cudaError_t e_ = (x);                                                                               \
+    if (e_ != cudaSuccess) fail(MTL_DEVICE_ERROR, std::string("CUDA error: ") + cudaGetErrorString(e_) + \
+                                                      " (" #x ")");                                   \
+  } while (0)
+
+// ------------------------------------------------------------ types
+int32_t storage_ptype(const LType& t) {
+  switch (t.t) {
+    case MTL_T_INTEGER:
+    case MTL_T_DATE:
+    case MTL_T_VARCHAR: return P_I32;
+    case MTL_T_BIGINT:
+    case MTL_T_TIMESTAMP:
+    case MTL_T_DECIMAL: return P_I64;
+    case MTL_T_FLOAT: return P_F32;
+    case MTL_T_DOUBLE: return P_F64;
+    case MTL_T_HUGEINT:
+    case MTL_T_DECIMAL128: return P_I128;
+    case MTL_T_BOOLEAN: return P_I32;
+    default: return P_NONE;
+  }
+}
+
+std::string type_name(const LType& t) {
+  switch (t.t) {
+    case MTL_T_INTEGER: return "INTEGER";
+    case MTL_T_BIGINT: return "BIGINT";
+    case MTL_T_FLOAT: return "FLOAT";
+    case MTL_T_DOUBLE: return "DOUBLE";
+    case MTL_T_DATE: return "DATE";
+    case MTL_T_TIMESTAMP: return "TIMESTAMP";
+    case MTL_T_DECIMAL:
+    case MTL_T_DECIMAL128: return "DECIMAL(" + std::to_string(t.width) + "," + std::to_string(t.scale) + ")";
+    case MTL_T_VARCHAR: return "VARCHAR";
+    case MTL_T_HUGEINT: return "HUGEINT";
+    case MTL_T_BOOLEAN: return "BOOLEAN";
+    default: return "UNKNOWN";
+  }
+}
+
+uint64_t Column::width() const { return (uint64_t)ptype_width(storage_ptype(type)); }
+
+Column* Table::find(const std::string& n) const {
+  for (auto& c : cols)
+    if (c->name == n) return c.get();
+  return nullptr;
+}
+
+uint64_t Result::approx_bytes() const {
+  uint64_t b = 0;
+  for (auto& c : cols) b += c.data.size() + c.valid.size();
+  return b;
+}
+
+// ------------------------------------------------------------ arena
+Arena::~Arena() {
+  if (base_) cudaFree(base_);
+}
+
+void Arena::init(uint64_t bytes) {
+  std::lock_guard<std::mutex> g(mu_);
+  cap_ = (bytes + 255) & ~255ULL;
+  if (cap_ == 0) return;
+  cudaError_t e = cudaMalloc((void**)&base_, cap_);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    base_ = nullptr;
+    fail(MTL_OOM, std::string("cannot allocate the processing region: ") + cudaGetErrorString(e));
+  }
+  free_.clear();
+  used_.clear();
+  free_[0] = cap_;
+}
+
+void* Arena::alloc(uint64_t bytes) {
+  std::lock_guard<std::mutex> g(mu_);
+  bytes = (bytes + 255) & ~255ULL;
+  if (bytes == 0) bytes = 256;
+  for (auto it = free_.begin(); it != free_.end(); ++it) {
+    if (it->second >= bytes) {
+      uint64_t off = it->first, sz = it->second;
+      free_.erase(it);
+      if (sz > bytes) free_[off + bytes] = sz - bytes;
+      used_[off] = bytes;
+      return base_ + off;
+    }
+  }
+  return nullptr;
+}
+
+void Arena::free(void* p) {
+  if (!p) return;
+  std::lock_guard<std::mutex> g(mu_);
+  uint64_t off = (uint64_t)((char*)p - base_);
+  auto u = used_.find(off);
+  if (u == used_.end()) return;
+  uint64_t sz = u->second;
+  used_.erase(u);
+  auto nx = free_.lower_bound(off);
+  if (nx != free_.end() && nx->first == off + sz) {
+    sz += nx->second;
+    nx = free_.erase(nx);
+  }
+  if (nx != free_.begin()) {
+    auto pv = std::prev(nx);
+    if (pv->first + pv->second == off) {
+      pv->second += sz;
+      return;
+    }
+  }
+  free_[off] = sz;
+}
+
+uint64_t Arena::used() const {
+  std::lock_guard<std::mutex> g(mu_);
+  uint64_t s = 0;
+  for (auto& u : used_) s += u.second;
+  return s;
+}
+
+uint64_t Arena::largest_free() const {
+  std::lock_guard<std::mutex> g(mu_);
+  uint64_t m = 0;
+  for (auto& f : free_) m = std::max(m, f.second);
+  return m;
+}
+
+Column::~Column() {
+  if (dev) cudaFree(dev);
+  if (host_owned) {
+    if (host_owned_pinned) cudaFreeHost(host_owned);
+    else ::free(host_owned);
+  }
+}
+
+Ctx::~Ctx() {
+  serve_shutdown(*this);
+  qcache.clear();
+  tables.clear();
+  if (stream) cudaStreamDestroy(stream);
+  if (copy_stream) cudaStreamDestroy(copy_stream);
+}
+
+// ------------------------------------------------------------ column cache
+static uint64_t table_rows_of(Ctx&, const Column& c) { return c.rows; }
+
+void* column_device(Ctx& ctx, Column& c) {
+  std::lock_guard<std::recursive_mutex> g(ctx.mu);
+  c.last_use = ++ctx.tick;
+  if (c.dev) {
+    ctx.cc.hits++;
+    return c.dev;
+  }
+  ctx.cc.misses++;
+  const uint64_t rows = table_rows_of(ctx, c);
+  const uint64_t bytes = rows * c.width();
+  if (bytes > ctx.budgets.cache_region_bytes)
+    fail(MTL_BUDGET_EXCEEDED, "column \"" + c.name + "\" (" + std::to_string(bytes) +
+                                  " bytes) exceeds the cache region of gpu_buffer_init");
+  // LRU eviction of unpinned device columns
+  while (ctx.dev_cache_bytes + bytes > ctx.budgets.cache_region_bytes) {
+    Column* victim = nullptr;
+    for (auto& t : ctx.tables)
+      for (auto& cc : t.second->cols)
+        if (cc->dev && cc->pins == 0 && (!victim || cc->last_use < victim->last_use)) victim = cc.get();
+    if (!victim) fail(MTL_BUDGET_EXCEEDED, "cache region exhausted by columns in use");
+    cudaFree(victim->dev);
+    victim->dev = nullptr;
+    ctx.dev_cache_bytes -= victim->dev_bytes;
+    victim->dev_bytes = 0;
+    ctx.cc.evictions++;
+  }
+  void* d = nullptr;
+  CK(cudaMalloc(&d, bytes ? bytes : 16));
+  if (bytes) {
+    CK(cudaMemcpyAsync(d, c.host, bytes, cudaMemcpyHostToDevice, ctx.copy_stream));
+    CK(cudaStreamSynchronize(ctx.copy_stream));
+  }
+  c.dev = d;
+  c.dev_bytes = bytes;
+  ctx.dev_cache_bytes += bytes;
+  return d;
+}
+
+void column_minmax(Ctx& ctx, Column& c) {
+  std::lock_guard<std::recursive_mutex> g(ctx.mu);
+  if (c.has_minmax) return;
+  const int32_t pt = storage_ptype(c.type);
+  if (pt != P_I32 && pt != P_I64) return;
+  const uint64_t rows = table_rows_of(ctx, c);
+  if (rows == 0) return;
+  void* d = column_device(ctx, c);
+  int64_t* buf = nullptr;
+  CK(cudaMalloc(&buf, 16));
+  int64_t init[2] = {INT64_MAX, INT64_MIN};
+  CK(cudaMemcpy(buf, init, 16, cudaMemcpyHostToDevice));
+  CK(launch_minmax_i(d, pt, rows, buf, ctx.copy_stream));
+  int64_t out[2];
+  CK(cudaMemcpyAsync(out, buf, 16, cudaMemcpyDeviceToHost, ctx.copy_stream));
+  CK(cudaStreamSynchronize(ctx.copy_stream));
+  cudaFree(buf);
+  c.vmin = out[0];
+  c.vmax = out[1];
+  c.has_minmax = true;
+}
+
+void column_distinct(Ctx& ctx, Table& t, Column& c) {
+  std::lock_guard<std::recursive_mutex> g(ctx.mu);
+  if (c.has_distinct) return;
+  const int32_t pt = storage_ptype(c.type);
+  if (t.rows == 0) {
+    c.has_distinct = c.has_unique = c.unique = true;
+    c.distinct = 0;
+    return;
+  }
+  if (c.type.t == MTL_T_VARCHAR) {
+    c.has_distinct = true;
+    c.distinct = std::min<uint64_t>(c.dict.size(), t.rows);
+    return;
+  }
+  void* d = column_device(ctx, c);
+  const uint64_t cap = std::max<uint64_t>(64, 2 * t.rows);
+  int64_t* table = nullptr;
+  uint32_t* special = nullptr;
+  unsigned long long* out = nullptr;
+  CK(cudaMalloc(&table, cap * 8));
+  CK(cudaMalloc(&special, 16));
+  CK(cudaMalloc(&out, 16));
+  CK(cudaMemsetAsync(table, 0xFF, cap * 8, ctx.copy_stream));
+  CK(cudaMemsetAsync(special, 0, 16, ctx.copy_stream));
+  CK(cudaMemsetAsync(out, 0, 16, ctx.copy_stream));
+  // F32/F64 columns hash their bit patterns (distinct estimate only).
+  CK(launch_count_dups(d, pt == P_F32 ? P_I32 : (pt == P_F64 ? P_I64 : pt), t.rows, table, cap, special, out,
+                       ctx.copy_stream));
+  unsigned long long dups = 0;
+  CK(cudaMemcpyAsync(&dups, out, 8, cudaMemcpyDeviceToHost, ctx.copy_stream));
+  CK(cudaStreamSynchronize(ctx.copy_stream));
+  cudaFree(table);
+  cudaFree(special);
+  cudaFree(out);
+  c.distinct = t.rows - dups;
+  c.has_distinct = true;
+  c.has_unique = true;
+  c.unique = dups == 0;
+}
+
+void column_unique(Ctx& ctx, Table& t, Column& c) { column_distinct(ctx, t, c); }
+
+// ------------------------------------------------------------ compiler
+namespace {
+
+struct Compiler {
+  Ctx& ctx;
+  const BoundPlan& plan;
+  Program& P;
+
+  // ---- scratch
+  void* scratch(uint64_t bytes) {
+    void* p = ctx.arena.alloc(bytes);
+    if (!p)
+      fail(MTL_BUDGET_EXCEEDED, "query needs more device scratch than the processing region allows (" +
+                                    std::to_string(bytes) + " bytes requested, " +
+                                    std::to_string(ctx.arena.largest_free()) + " free)");
+    P.blocks.push_back(p);
+    P.scratch_bytes += (bytes + 255) & ~255ULL;
+    return p;
+  }
+  void memset_step(void* p, int byte, uint64_t bytes) {
+    Step s;
+    s.k = Step::MEMSET;
+    s.ptr = p;
+    s.byte = byte;
+    s.bytes = bytes;
+    P.steps.push_back(s);
+  }
+  void fill_step(void* p, uint64_t words, uint64_t v) {
+    Step s;
+    s.k = Step::FILL;
+    s.ptr = p;
+    s.bytes = words;
+    s.fill = v;
+    P.steps.push_back(s);
+    P.kernels += 1;
+  }
+
+  // ---- join tree
+  int root = 0;
+  std::vector<int> parent;          // -1 for root
+  std::vector<Column*> up_col;      // build key column of each non-root source
+  std::vector<Column*> down_col;    // parent's probe column for each non-root source
+  std::vector<std::vector<int>> children;
+  std::vector<uint32_t> subtree;    // source mask of each subtree
+
+  uint32_t subtree_mask(int s) {
+    uint32_t m = 1u << s;
+    for (int c : children[s]) m |= subtree_mask(c);
+    return subtree[s] = m;
+  }
+
+  void plan_joins() {
+    const int S = (int)plan.sources.size();
+    parent.assign(S, -1);
+    up_col.assign(S, nullptr);
+    down_col.assign(S, nullptr);
+    children.assign(S, {});
+    subtree.assign(S, 0);
+    if (S == 1) {
+      root = 0;
+      subtree_mask(0);
+      return;
+    }
+    if ((int)plan.joins.size() != S - 1)
+      fail(MTL_UNSUPPORTED, "join graph must be a tree of equi-joins (cross products and cyclic joins are "
+                            "outside the offloaded subset)");
+    std::vector<int> order(S);
+    for (int i = 0; i < S; ++i) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+      return plan.sources[a].table->rows > plan.sources[b].table->rows;
+    });
+    for (int cand : order) {
+      // orient edges away from cand
+      std::vector<int> par(S, -2);
+      std::vector<Column*> upc(S, nullptr), downc(S, nullptr);
+      par[cand] = -1;
+      std::vector<int> q{cand};
+      bool ok = true;
+      for (size_t qi = 0; qi < q.size() && ok; ++qi) {
+        int u = q[qi];
+        for (const BJoin& j : plan.joins) {
+          int v = -1;
+          Column *vc = nullptr, *uc = nullptr;
+          if (j.ls == u) { v = j.rs; vc = j.rc; uc = j.lc; }
+          else if (j.rs == u) { v = j.ls; vc = j.lc; uc = j.rc; }
+          else continue;
+          if (par[v] != -2) {
+            if (v != par[u]) ok = false;  // cycle
+            continue;
+          }
+          par[v] = u;
+          upc[v] = vc;
+          downc[v] = uc;
+          q.push_back(v);
+        }
+      }
+      if (!ok || (int)q.size() != S) fail(MTL_UNSUPPORTED, "join graph must be a connected tree of equi-joins");
+      bool unique_builds = true;
+      for (int v = 0; v < S && unique_builds; ++v) {
+        if (v == cand) continue;
+        Column* c = upc[v];
+        if (storage_ptype(c->type) != P_I32 && storage_ptype(c->type) != P_I64) {
+          unique_builds = false;
+          break;
+        }
+        if (storage_ptype(downc[v]->type) != storage_ptype(c->type) &&
+            !((storage_ptype(downc[v]->type) == P_I32 || storage_ptype(downc[v]->type) == P_I64))) {
+          unique_builds = false;
+          break;
+        }
+        column_unique(ctx, *plan.sources[v].table, *c);
+        if (!c->unique) unique_builds = false;
+      }
+      if (!unique_builds) continue;
+      root = cand;
+      parent = par;
+      parent[cand] = -1;
+      up_col = upc;
+      down_col = downc;
+      for (int v = 0; v < S; ++v)
+        if (v != cand) children[parent[v]].push_back(v);
+      subtree_mask(root);
+      return;
+    }
+    fail(MTL_UNSUPPORTED, "every join needs a unique key on its build side (non-unique join keys are "
+                          "outside the offloaded subset)");
+  }
+
+  // ---- expression programs
+  struct PipeBuilder {
+    PipeDesc d;
+    std::map<std::pair<int, const Column*>, int> colmap;
+    PipeBuilder() {
+      memset(&d, 0, sizeof(d));
+      d.first_col = -1;
+      d.slot_probe = -1;
+    }
+  };
+
+  int add_col(PipeBuilder& pb, int src, Column* c) {
+    auto key = std::make_pair(src, (const Column*)c);
+    auto it = pb.colmap.find(key);
+    if (it != pb.colmap.end()) return it->second;
+    if (pb.d.n_cols >= kMaxCols) fail(MTL_UNSUPPORTED, "too many columns in one pipeline");
+    int i = pb.d.n_cols++;
+    pb.d.cols[i].ptr = column_device(ctx, *c);
+    pb.d.cols[i].ptype = storage_ptype(c->type);
+    pb.d.cols[i].src = src;
+    pb.colmap[key] = i;
+    pinned_cols.insert(c);
+    return i;
+  }
+  std::set<Column*> pinned_cols;
+
+  void emit(PipeBuilder& pb, VmProg& p, const BExpr& e) {
+    auto push = [&](VmIns in) {
+      if (p.n >= kMaxIns) fail(MTL_UNSUPPORTED, "expression too long for the device evaluator");
+      p.ins[p.n++] = in;
+    };
+    VmIns in;
+    memset(&in, 0, sizeof(in));
+    switch (e.k) {
+      case BExpr::COL:
+        in.op = VM_COL;
+        in.type = (int16_t)storage_ptype(e.col->type);
+        in.arg = add_col(pb, e.src, e.col);
+        push(in);
+        break;
+      case BExpr::CONST:
+        in.op = VM_CONST;
+        in.type = (int16_t)e.ptype;
+        in.k = e.lo;
+        in.k2 = e.hi;
+        if (e.ptype == P_I32 || e.ptype == P_I64) in.k2 = e.lo < 0 ? -1 : 0;
+        push(in);
+        break;
+      case BExpr::ARITH:
+        emit(pb, p, *e.a[0]);
+        emit(pb, p, *e.a[1]);
+        in.op = e.op;
+        in.type = (int16_t)e.ptype;
+        push(in);
+        break;
+      case BExpr::CAST:
+        emit(pb, p, *e.a[0]);
+        in.op = VM_CAST;
+        in.type = (int16_t)e.ptype;
+        in.arg = e.a[0]->ptype;
+        in.k = e.mul;
+        in.k2 = e.div;
+        push(in);
+        break;
+      case BExpr::NEG:
+        emit(pb, p, *e.a[0]);
+        in.op = VM_NEG;
+        in.type = (int16_t)e.ptype;
+        push(in);
+        break;
+      default:
+        fail(MTL_UNSUPPORTED, "aggregate in a scalar context");
+    }
+  }
+
+  int add_prog(PipeBuilder& pb, const BExpr& e) {
+    if (pb.d.n_progs >= kMaxProgs) fail(MTL_UNSUPPORTED, "too many expressions in one pipeline");
+    int i = pb.d.n_progs++;
+    VmProg& p = pb.d.progs[i];
+    memset(&p, 0, sizeof(p));
+    emit(pb, p, e);
+    p.out_type = e.ptype;
+    return i;
+  }
+
+  static void expr_sources(const BExpr& e, uint32_t& m) {
+    if (e.k == BExpr::COL) m |= 1u << e.src;
+    for (auto& c : e.a) expr_sources(*c, m);
+  }
+
+  // ---- builds
+  std::vector<DBuild> builds;  // per source
+  std::vector<int> build_probe_index;  // per source: probe index in its parent's pipeline
+
+  DBuild make_build(int s) {
+    DBuild b;
+    memset(&b, 0, sizeof(b));
+    Table& t = *plan.sources[s].table;
+    Column& k = *up_col[s];
+    column_minmax(ctx, k);
+    const uint64_t rows = t.rows;
+    b.key_ptype = storage_ptype(k.type);
+    b.n_slots = (uint32_t*)scratch(8);
+    memset_step(b.n_slots, 0, 8);
+    bool dense = false;
+    uint64_t span = 0;
+    if (k.has_minmax) {
+      __int128 sp = (__int128)k.vmax - (__int128)k.vmin + 1;
+      if (sp > 0 && sp <= (__int128)(4 * rows + (1u << 20)) && sp < ((__int128)1 << 31)) {
+        dense = true;
+        span = (uint64_t)sp;
+      }
+    }
+    if (rows == 0) {
+      dense = true;
+      span = 1;
+      b.key_min = 0;
+    }
+    if (dense) {
+      b.kind = B_DENSE;
+      if (rows) b.key_min = k.vmin;
+      b.capacity = span;
+      b.dense_map = (uint32_t*)scratch(span * 4);
+      memset_step(b.dense_map, 0, span * 4);
+    } else {
+      b.kind = B_HASH;
+      b.capacity = std::max<uint64_t>(64, 2 * rows);
+      b.hash_keys = (int64_t*)scratch(b.capacity * 8);
+      b.hash_slot = (uint32_t*)scratch(b.capacity * 4);
+      b.hash_special = (uint32_t*)scratch(8);
+      memset_step(b.hash_keys, 0xFF, b.capacity * 8);
+      memset_step(b.hash_special, 0, 8);
+    }
+    return b;
+  }
+
+  // Sources whose row ids the root pipeline's sink needs.
+  uint32_t needed_root = 0;
+  uint32_t payload_mask(int s) const { return needed_root & subtree[s]; }
+  int rep_src = -1;
+
+  void add_filters(PipeBuilder& pb, int s) {
+    for (const BFilter& f : plan.filters) {
+      if (f.src != s) continue;
+      if (pb.d.n_preds >= kMaxPreds) fail(MTL_UNSUPPORTED, "too many predicates on one table");
+      int pi = pb.d.n_preds++;
+      DPred& p = pb.d.preds[pi];
+      p.col = add_col(pb, s, f.col);
+      p.op = f.op;
+      p.ilit = f.ilit;
+      p.flit = f.flit;
+      pb.d.ops[pb.d.n_ops].kind = OPK_FILTER;
+      pb.d.ops[pb.d.n_ops].idx = pi;
+      pb.d.n_ops++;
+    }
+  }
+
+  // Probes into the children's builds; fill masks bring the row ids listed
+  // in `want` into the pipeline.
+  void add_probes(PipeBuilder& pb, int s, uint32_t want) {
+    for (int c : children[s]) {
+      if (pb.d.n_probes >= kMaxProbes) fail(MTL_UNSUPPORTED, "too many joins on one table");
+      int pi = pb.d.n_probes++;
+      int bi = pb.d.n_builds++;
+      pb.d.builds[bi] = builds[c];
+      DProbe& pr = pb.d.probes[pi];
+      pr.key_col = add_col(pb, s, down_col[c]);
+      pr.build = bi;
+      pr.fill_mask = want & subtree[c];
+      pb.d.ops[pb.d.n_ops].kind = OPK_PROBE;
+      pb.d.ops[pb.d.n_ops].idx = pi;
+      pb.d.n_ops++;
+      build_probe_index[c] = pi;
+    }
+  }
+
+  void finish_ops(PipeBuilder& pb) {
+    if (pb.d.n_ops > 0) {
+      const PipeOp& o = pb.d.ops[0];
+      pb.d.first_col = o.kind == OPK_FILTER ? pb.d.preds[o.idx].col : pb.d.probes[o.idx].key_col;
+    }
+  }
+
+  void push_pipeline(PipeBuilder& pb, uint64_t n_hint) {
+    static const char* sinks[] = {"none", "build", "materialize", "agg_hash", "agg_smem", "agg_slot", "agg_scalar"};
+    Step s;
+    s.k = Step::PIPELINE;
+    s.pipe = pb.d;
+    s.n_hint = n_hint;
+    s.name = std::string("pipeline:") + sinks[pb.d.sink] + ":" + plan.sources[pb.d.drive_src].name;
+    P.steps.push_back(s);
+    P.kernels += 1;
+  }
+
+  // Aggregate state descriptors for the sink (shared with the rep build).
+  struct AggState {
+    int fn_dev = 0;   // AggFn
+    int prog_agg = -1;  // BAgg index whose arg feeds it (-1: COUNT)
+    uint64_t* lo = nullptr;
+    int64_t* hi = nullptr;
+  };
+  std::vector<AggState> states;      // device states
+  std::vector<int> agg_sum_state, agg_cnt_state, agg_state;  // per BAgg
+  int count_state = -1;
+
+  static bool sum_fits64(const BAgg& g, uint64_t rows) {
+    const BExpr& e = *g.arg;
+    if (!e.bounded) return false;
+    __int128 m = std::max(e.bmin < 0 ? -e.bmin : e.bmin, e.bmax < 0 ? -e.bmax : e.bmax);
+    __int128 bound = m * (__int128)(rows ? rows : 1);
+    return bound < ((__int128)1 << 63) - 1;
+  }
+
+  void plan_states(uint64_t groups, uint64_t rows, bool need_count) {
+    agg_sum_state.assign(plan.aggs.size(), -1);
+    agg_cnt_state.assign(plan.aggs.size(), -1);
+    agg_state.assign(plan.aggs.size(), -1);
+    auto new_state = [&](int fn, int agg) {
+      AggState s;
+      s.fn_dev = fn;
+      s.prog_agg = agg;
+      s.lo = (uint64_t*)scratch(groups * 8);
+      if (fn == A_SUM_I128) s.hi = (int64_t*)scratch(groups * 8);
+      states.push_back(s);
+      return (int)states.size() - 1;
+    };
+    bool any_avg = false;
+    for (auto& g : plan.aggs) any_avg |= g.fn == AG_AVG;
+    if (need_count || any_avg) count_state = new_state(A_COUNT, -1);
+    for (size_t i = 0; i < plan.aggs.size(); ++i) {
+      const BAgg& g = plan.aggs[i];
+      switch (g.fn) {
+        case AG_COUNT:
+          if (count_state < 0) count_state = new_state(A_COUNT, -1);
+          agg_state[i] = count_state;
+          break;
+        case AG_SUM:
+        case AG_AVG: {
+          const LType at = g.arg->type;
+          int fn;
+          if (is_float_family(at)) fn = A_SUM_F;
+          else if (g.fn == AG_AVG && at.t == MTL_T_INTEGER) fn = A_SUM_I;
+          else fn = sum_fits64(g, rows) ? A_SUM_I : A_SUM_I128;
+          // reuse the state of an identical sum
+          int found = -1;
+          for (size_t j = 0; j < i; ++j)
+            if (agg_sum_state[j] >= 0 && plan.aggs[j].arg && plan.aggs[j].arg->text == g.arg->text &&
+                states[agg_sum_state[j]].fn_dev == fn)
+              found = agg_sum_state[j];
+          int s = found >= 0 ? found : new_state(fn, (int)i);
+          agg_sum_state[i] = s;
+          agg_state[i] = s;
+          if (g.fn == AG_AVG) agg_cnt_state[i] = count_state;
+          break;
+        }
+        case AG_MIN:
+        case AG_MAX: {
+          bool f = is_float_family(g.arg->type);
+          int fn = g.fn == AG_MIN ? (f ? A_MIN_F : A_MIN_I) : (f ? A_MAX_F : A_MAX_I);
+          agg_state[i] = new_state(fn, (int)i);
+          break;
+        }
+      }
+    }
+    if ((int)states.size() > kMaxAggs) fail(MTL_UNSUPPORTED, "too many aggregates in one query");
+  }
+
+  void fill_aggs(PipeBuilder& pb, bool with_progs) {
+    pb.d.n_aggs = (int)states.size();
+    for (size_t i = 0; i < states.size(); ++i) {
+      DAgg& a = pb.d.aggs[i];
+      a.fn = states[i].fn_dev;
+      a.lo = states[i].lo;
+      a.hi = states[i].hi;
+      a.prog = -1;
+      if (with_progs && states[i].prog_agg >= 0) a.prog = add_prog(pb, *plan.aggs[states[i].prog_agg].arg);
+    }
+  }
+
+  // ---- final outputs of aggregate queries
+  struct DenseOut {
+    void* dev = nullptr;
+    int width = 0;
+    int32_t ptype = 0;
+  };
+  std::vector<DenseOut> dense;  // per plan output
+
+  FinalOut agg_final(int out_i, void* dst) {
+    const BOut& o = plan.outputs[out_i];
+    FinalOut f;
+    memset(&f, 0, sizeof(f));
+    f.out = dst;
+    const BAgg& g = plan.aggs[o.agg_idx];
+    const int si = agg_state[o.agg_idx];
+    const AggState& st = states[si];
+    f.a = st.lo;
+    f.a_hi = st.hi;
+    switch (g.fn) {
+      case AG_COUNT: f.kind = F_COPY_I64; break;
+      case AG_SUM:
+        f.kind = st.fn_dev == A_SUM_F ? F_COPY_F64 : st.fn_dev == A_SUM_I128 ? F_SUM_I128 : F_SUM_I64_AS_I128;
+        break;
+      case AG_MIN:
+      case AG_MAX:
+        if (st.fn_dev == A_MIN_F || st.fn_dev == A_MAX_F)
+          f.kind = g.result.t == MTL_T_FLOAT ? F_MINMAX_F32 : F_MINMAX_F64;
+        else
+          f.kind = ptype_width(storage_ptype(g.result)) == 4 ? F_COPY_I32 : F_COPY_I64;
+        break;
+      case AG_AVG: {
+        f.cnt = states[agg_cnt_state[o.agg_idx]].lo;
+        const LType at = g.arg->type;
+        if (is_float_family(at)) f.kind = F_AVG_F64;
+        else if (at.t == MTL_T_INTEGER) f.kind = F_AVG_I64_D;
+        else if (is_decimal(at)) {
+          f.kind = F_AVG_DEC;
+          f.scale = std::pow(10.0, at.scale);
+        } else f.kind = F_AVG_I128_LD;
+        if (st.fn_dev != A_SUM_I128) f.a_hi = nullptr;
+        break;
+      }
+    }
+    return f;
+  }
+
+  FinalOut* upload_finals(const std::vector<FinalOut>& fo) {
+    FinalOut* d = (FinalOut*)scratch(fo.size() * sizeof(FinalOut));
+    CK(cudaMemcpy(d, fo.data(), fo.size() * sizeof(FinalOut), cudaMemcpyHostToDevice));
+    return d;
+  }
+
+  void finalize_step(FinalOut* fd, int n, const uint32_t* idx, const uint64_t* count, uint64_t n_max) {
+    Step s;
+    s.k = Step::FINALIZE;
+    s.fin_dev = fd;
+    s.n_fin = n;
+    s.idx = idx;
+    s.count = count;
+    s.n_max = n_max;
+    P.steps.push_back(s);
+    P.kernels += 1;
+  }
+
+  // ---- ORDER BY / LIMIT over dense output arrays
+  void order_and_limit(const uint64_t* count, uint64_t n_max, const std::vector<int>& tie_outs) {
+    P.limit = plan.limit;
+    std::vector<int> vis;
+    for (size_t i = 0; i < plan.outputs.size(); ++i)
+      if (!plan.outputs[i].hidden) vis.push_back((int)i);
+    if (plan.order.empty() || plan.limit == 0 || n_max == 0) {
+      for (int i : vis) {
+        OutBuf ob;
+        ob.name = plan.outputs[i].name;
+        ob.type = plan.outputs[i].type;
+        ob.dev = dense[i].dev;
+        ob.width = dense[i].width;
+        ob.dict = plan.outputs[i].dict;
+        P.outs.push_back(ob);
+      }
+      P.out_count = count;
+      P.n_max = n_max;
+      return;
+    }
+    SortKeySpec spec;
+    memset(&spec, 0, sizeof(spec));
+    int bits = 0;
+    auto part_bits = [](int32_t pt) { return pt == P_I128 ? 128 : (pt == P_I32 || pt == P_F32) ? 32 : 64; };
+    auto add_part = [&](int out_i, bool desc) {
+      int32_t pt = dense[out_i].ptype;
+      if (bits + part_bits(pt) > 256 || spec.n_parts >= kMaxOrder) return false;
+      spec.ptype[spec.n_parts] = pt;
+      spec.desc[spec.n_parts] = desc ? 1 : 0;
+      spec.col[spec.n_parts] = dense[out_i].dev;
+      spec.n_parts++;
+      bits += part_bits(pt);
+      return true;
+    };
+    for (const BOrder& o : plan.order)
+      if (!add_part(o.out, o.desc)) fail(MTL_UNSUPPORTED, "ORDER BY keys wider than 256 bits");
+    for (int t : tie_outs) {
+      bool in_order = false;
+      for (const BOrder& o : plan.order) in_order |= o.out == t;
+      if (!in_order) add_part(t, false);
+    }
+    SortItem* keys = (SortItem*)scratch(std::max<uint64_t>(n_max, 1) * sizeof(SortItem));
+    uint32_t* kidx = (uint32_t*)scratch(std::max<uint64_t>(n_max, 1) * 4);
+    Step e;
+    e.k = Step::ENCODE;
+    e.spec = spec;
+    e.count = count;
+    e.n_max = n_max;
+    e.keys = keys;
+    e.kidx = kidx;
+    P.steps.push_back(e);
+    P.kernels += 1;
+    const uint32_t* final_idx;
+    const uint64_t* final_count;
+    uint64_t rows_max;
+    if (plan.limit > 0 && plan.limit <= 1024) {
+      const int K = (int)plan.limit;
+      uint32_t* oidx = (uint32_t*)scratch((uint64_t)K * 4);
+      uint64_t* ocnt = (uint64_t*)scratch(8);
+      Step t;
+      t.k = Step::TOPK;
+      t.keys = keys;
+      t.kidx = kidx;
+      t.count = count;
+      t.n_max = n_max;
+      t.topk = K;
+      t.out_idx = oidx;
+      t.out_count = ocnt;
+      t.temp = scratch(topk_temp_bytes(n_max, K));
+      P.steps.push_back(t);
+      P.kernels += 2;
+      final_idx = oidx;
+      final_count = ocnt;
+      rows_max = std::min<uint64_t>(n_max, (uint64_t)K);
+    } else {
+      SortItem* keys2 = (SortItem*)scratch(std::max<uint64_t>(n_max, 1) * sizeof(SortItem));
+      uint32_t* kidx2 = (uint32_t*)scratch(std::max<uint64_t>(n_max, 1) * 4);
+      Step r;
+      r.k = Step::RADIX;
+      r.keys = keys;
+      r.kidx = kidx;
+      r.keys_tmp = keys2;
+      r.kidx_tmp = kidx2;
+      r.count = count;
+      r.n_max = n_max;
+      r.key_bytes = (bits + 7) / 8;
+      r.temp = scratch(radix_sort_temp_bytes(n_max));
+      P.steps.push_back(r);
+      uint64_t tiles = (n_max + 4095) / 4096;
+      uint64_t chunks = (tiles * 256 + 4095) / 4096;
+      P.kernels += r.key_bytes * (chunks == 1 ? 3 : 5);
+      final_idx = (r.key_bytes & 1) ? kidx2 : kidx;
+      final_count = count;
+      rows_max = n_max;
+    }
+    for (int i : vis) {
+      void* outp = scratch(std::max<uint64_t>(rows_max, 1) * dense[i].width);
+      Step g;
+      g.k = Step::GATHER;
+      g.gin = dense[i].dev;
+      g.width = dense[i].width;
+      g.idx = final_idx;
+      g.count = final_count;
+      g.n_max = rows_max;
+      g.gout = outp;
+      P.steps.push_back(g);
+      P.kernels += 1;
+      OutBuf ob;
+      ob.name = plan.outputs[i].name;
+      ob.type = plan.outputs[i].type;
+      ob.dev = outp;
+      ob.width = dense[i].width;
+      ob.dict = plan.outputs[i].dict;
+      P.outs.push_back(ob);
+    }
+    P.out_count = final_count;
+    P.n_max = rows_max;
+  }
+
+  // ---- main
+  void compile() {
+    P.status = (uint32_t*)scratch(8);
+    memset_step(P.status, 0, 8);
+    plan_joins();
+    const int S = (int)plan.sources.size();
+    builds.assign(S, DBuild{});
+    build_probe_index.assign(S, -1);
+    const uint64_t root_rows = plan.sources[root].table->rows;
+
+    // what the root sink reads
+    needed_root = 0;
+    if (!plan.is_agg) {
+      for (auto& o : plan.outputs) expr_sources(*o.expr, needed_root);
+    } else {
+      for (auto& g : plan.aggs)
+        if (g.arg) expr_sources(*g.arg, needed_root);
+      rep_src = find_rep();
+      if (rep_src < 0)
+        for (auto& k : plan.group_keys) expr_sources(*k, needed_root);
+    }
+
+    // aggregate states (the representative build initializes them)
+    const bool scalar = plan.is_agg && plan.group_keys.empty();
+    uint64_t groups = 0;
+    uint64_t est_groups = 0;
+    if (plan.is_agg) {
+      if (scalar) groups = 1;
+      else if (rep_src >= 0) groups = std::max<uint64_t>(1, plan.sources[rep_src].table->rows);
+      else {
+        est_groups = estimate_groups();
+        groups = std::max<uint64_t>(1024, est_groups * 2);
+      }
+      plan_states(groups, root_rows, scalar);
+    }
+
+    // build pipelines, children before parents
+    std::vector<int> post;
+    std::function<void(int)> dfs = [&](int s) {
+      for (int c : children[s]) dfs(c);
+      if (s != root) post.push_back(s);
+    };
+    dfs(root);
+    uint8_t* slot_hit = nullptr;
+    for (int s : post) {
+      builds[s] = make_build(s);
+      PipeBuilder pb;
+      pb.d.n = plan.sources[s].table->rows;
+      pb.d.drive_src = s;
+      pb.d.src_mask = 1u << s;
+      uint32_t pay = payload_mask(s) | (s == rep_src ? (1u << s) : 0u);
+      for (int c : children[s]) builds[c].kind = builds[c].kind;  // built already
+      add_filters(pb, s);
+      add_probes(pb, s, pay);
+      finish_ops(pb);
+      pb.d.sink = SK_BUILD;
+      pb.d.builds[pb.d.n_builds] = builds[s];
+      pb.d.sink_build = pb.d.n_builds++;
+      pb.d.build_key_col = add_col(pb, s, up_col[s]);
+      pb.d.build_payload_mask = pay;
+      for (int q = 0; q < kMaxSrc; ++q)
+        if ((pay >> q) & 1u) {
+          builds[s].payload[q] = (uint32_t*)scratch(std::max<uint64_t>(1, plan.sources[s].table->rows) * 4);
+          pb.d.builds[pb.d.sink_build].payload[q] = builds[s].payload[q];
+        }
+      if (s == rep_src) {
+        fill_aggs(pb, false);
+        slot_hit = (uint8_t*)scratch(std::max<uint64_t>(1, plan.sources[s].table->rows));
+        pb.d.slot_hit = slot_hit;
+      }
+      pb.d.status = P.status;
+      push_pipeline(pb, pb.d.n);
+    }
+
+    // root pipeline
+    PipeBuilder pb;
+    pb.d.n = root_rows;
+    pb.d.drive_src = root;
+    pb.d.src_mask = 1u << root;
+    add_filters(pb, root);
+    add_probes(pb, root, needed_root);
+    finish_ops(pb);
+    pb.d.status = P.status;
+    dense.assign(plan.outputs.size(), DenseOut{});
+
+    if (!plan.is_agg) {
+      // order-preserving materialization of every output (incl. ORDER BY keys)
+      pb.d.sink = SK_MATERIALIZE;
+      const uint64_t n_max = root_rows;
+      pb.d.n_out = (int)plan.outputs.size();
+      for (size_t i = 0; i < plan.outputs.size(); ++i) {
+        const BOut& o = plan.outputs[i];
+        int pi = add_prog(pb, *o.expr);
+        pb.d.out_prog[i] = pi;
+        const int32_t pt = o.expr->ptype;
+        // outputs are stored in the logical type's storage representation
+        if (storage_ptype(o.type) != pt) {
+          fail(MTL_UNSUPPORTED, "output representation mismatch");
+        }
+        dense[i].width = ptype_width(pt);
+        dense[i].ptype = pt;
+        dense[i].dev = scratch(std::max<uint64_t>(1, n_max) * dense[i].width);
+        pb.d.out_ptr[i] = dense[i].dev;
+      }
+      uint32_t m = 0;
+      for (auto& o : plan.outputs) expr_sources(*o.expr, m);
+      pb.d.mat_src_mask = m;
+      pb.d.out_count = (uint64_t*)scratch(8);
+      pb.d.out_capacity = n_max;
+      const uint64_t tiles = (n_max + pipeline_tile_rows() - 1) / pipeline_tile_rows();
+      pb.d.tile_status = (uint64_t*)scratch(std::max<uint64_t>(tiles, 1) * 8);
+      pb.d.tile_counter = (uint32_t*)scratch(8);
+      pb.d.epoch = 1;
+      memset_step(pb.d.tile_status, 0, std::max<uint64_t>(tiles, 1) * 8);
+      memset_step(pb.d.tile_counter, 0, 8);
+      push_pipeline(pb, root_rows);
+      order_and_limit(pb.d.out_count, n_max, {});
+      return;
+    }
+
+    std::vector<int> tie;  // group-key outputs: deterministic tie order
+    for (size_t i = 0; i < plan.outputs.size(); ++i)
+      if (plan.outputs[i].group_idx >= 0) tie.push_back((int)i);
+
+    if (scalar) {
+      pb.d.sink = SK_AGG_SCALAR;
+      for (auto& s : states) {
+        uint64_t init = 0;
+        switch (s.fn_dev) {
+          case A_MIN_I: init = 0x7FFFFFFFFFFFFFFFULL; break;
+          case A_MAX_I: init = 0x8000000000000000ULL; break;
+          case A_MIN_F: init = ~0ULL; break;
+          default: init = 0;
+        }
+        fill_step(s.lo, 1, init);
+        if (s.hi) fill_step(s.hi, 1, 0);
+      }
+      fill_aggs(pb, true);
+      push_pipeline(pb, root_rows);
+      std::vector<FinalOut> fo;
+      for (size_t i = 0; i < plan.outputs.size(); ++i) {
+        const BOut& o = plan.outputs[i];
+        dense[i].ptype = storage_ptype(o.type);
+        dense[i].width = ptype_width(dense[i].ptype);
+        dense[i].dev = scratch(16);
+        fo.push_back(agg_final((int)i, dense[i].dev));
+      }
+      finalize_step(upload_finals(fo), (int)fo.size(), nullptr, nullptr, 1);
+      P.fixed_count = 1;
+      P.empty_count = states[count_state].lo;
+      order_and_limit(nullptr, 1, {});
+      P.fixed_count = 1;
+      return;
+    }
+
+    if (rep_src >= 0) {
+      // Grouping by a build's representative row: states are dense by the
+      // build slot (the reference's dense_row_id_sum_track_live_v /
+      // accumulate_revenue_dense_slots_from_indices_v, kernels.metal:1009,1076).
+      pb.d.sink = SK_AGG_SLOT;
+      pb.d.slot_probe = build_probe_index[rep_src];
+      pb.d.slot_hit = slot_hit;
+      fill_aggs(pb, true);
+      push_pipeline(pb, root_rows);
+      const uint64_t cap = std::max<uint64_t>(1, plan.sources[rep_src].table->rows);
+      uint32_t* gidx = (uint32_t*)scratch(cap * 4);
+      uint64_t* gcnt = (uint64_t*)scratch(8);
+      compact_step(slot_hit, cap, (const uint64_t*)builds[rep_src].n_slots, gidx, gcnt, false);
+      std::vector<FinalOut> fo;
+      for (size_t i = 0; i < plan.outputs.size(); ++i) {
+        const BOut& o = plan.outputs[i];
+        dense[i].ptype = storage_ptype(o.type);
+        dense[i].width = ptype_width(dense[i].ptype);
+        dense[i].dev = scratch(cap * dense[i].width);
+        if (o.agg_idx >= 0) {
+          fo.push_back(agg_final((int)i, dense[i].dev));
+        } else {
+          FinalOut f;
+          memset(&f, 0, sizeof(f));
+          f.kind = F_GATHER_COL;
+          f.width = dense[i].width;
+          Column* c = rep_column(*plan.group_keys[o.group_idx]);
+          f.col = column_device(ctx, *c);
+          pinned_cols.insert(c);
+          f.rid = builds[rep_src].payload[rep_src];
+          f.out = dense[i].dev;
+          fo.push_back(f);
+        }
+      }
+      finalize_step(upload_finals(fo), (int)fo.size(), gidx, gcnt, cap);
+      order_and_limit(gcnt, cap, tie);
+      return;
+    }
+
+    // hash aggregation (shared-memory tables when the group count is small)
+    const uint64_t cap = groups;
+    pb.d.table.capacity = cap;
+    pb.d.table.n_keys = (int)plan.group_keys.size();
+    pb.d.table.state = (uint32_t*)scratch(cap * 4);
+    memset_step(pb.d.table.state, 0, cap * 4);
+    for (size_t k = 0; k < plan.group_keys.size(); ++k) {
+      pb.d.table.keys[k] = (uint64_t*)scratch(cap * 8);
+      pb.d.key_prog[k] = add_prog(pb, *plan.group_keys[k]);
+    }
+    fill_aggs(pb, true);
+    pb.d.sink = SK_AGG_HASH;
+    if (est_groups <= 1536) {
+      pb.d.sink = SK_AGG_SMEM;
+      pb.d.smem_capacity = (int)std::max<uint64_t>(256, est_groups * 4 / 3 + 64);
+      size_t smem = pipeline_smem_bytes(pb.d);
+      if (smem > 200 * 1024) {
+        pb.d.sink = SK_AGG_HASH;
+        pb.d.smem_capacity = 0;
+      }
+    }
+    push_pipeline(pb, root_rows);
+    uint32_t* gidx = (uint32_t*)scratch(cap * 4);
+    uint64_t* gcnt = (uint64_t*)scratch(8);
+    compact_step(pb.d.table.state, cap, nullptr, gidx, gcnt, true);
+    std::vector<FinalOut> fo;
+    for (size_t i = 0; i < plan.outputs.size(); ++i) {
+      const BOut& o = plan.outputs[i];
+      dense[i].ptype = storage_ptype(o.type);
+      dense[i].width = ptype_width(dense[i].ptype);
+      dense[i].dev = scratch(cap * dense[i].width);
+      if (o.agg_idx >= 0) {
+        fo.push_back(agg_final((int)i, dense[i].dev));
+      } else {
+        FinalOut f;
+        memset(&f, 0, sizeof(f));
+        const int32_t pt = dense[i].ptype;
+        f.kind = pt == P_I32 ? F_COPY_I32 : pt == P_F32 ? F_COPY_F32 : F_COPY_I64;
+        f.a = pb.d.table.keys[o.group_idx];
+        f.out = dense[i].dev;
+        fo.push_back(f);
+      }
+    }
+    finalize_step(upload_finals(fo), (int)fo.size(), gidx, gcnt, cap);
+    order_and_limit(gcnt, cap, tie);
+  }
+
+  void compact_step(const void* flag, uint64_t n, const uint64_t* n_dev, uint32_t* out_idx, uint64_t* out_count,
+                    bool ready) {
+    const uint64_t tiles = (n + compact_tile_rows() - 1) / compact_tile_rows();
+    Step s;
+    s.k = ready ? Step::COMPACT_READY : Step::COMPACT_FLAGS;
+    s.flag = flag;
+    s.n = n;
+    s.n_dev = n_dev;
+    s.out_idx = out_idx;
+    s.out_count = out_count;
+    s.tstatus = (uint64_t*)scratch(std::max<uint64_t>(tiles, 1) * 8);
+    s.tcounter = (uint32_t*)scratch(8);
+    memset_step(s.tstatus, 0, std::max<uint64_t>(tiles, 1) * 8);
+    memset_step(s.tcounter, 0, 8);
+    P.steps.push_back(s);
+    P.kernels += 1;
+  }
+
+  // ---- representative-row grouping
+  // Union-find over (source, column) joined by equality.
+  std::map<std::pair<int, const Column*>, std::pair<int, const Column*>> uf;
+  std::pair<int, const Column*> findc(std::pair<int, const Column*> x) {
+    auto it = uf.find(x);
+    if (it == uf.end() || it->second == x) return x;
+    auto r = findc(it->second);
+    uf[x] = r;
+    return r;
+  }
+  void unite(std::pair<int, const Column*> a, std::pair<int, const Column*> b) {
+    auto ra = findc(a), rb = findc(b);
+    if (ra != rb) uf[ra] = rb;
+  }
+
+  // The key column of the representative build equal to group key `e`.
+  Column* rep_column(const BExpr& e) {
+    if (e.src == rep_src) return e.col;
+    auto cls = findc({e.src, e.col});
+    for (auto& c : plan.sources[rep_src].table->cols)
+      if (findc({rep_src, c.get()}) == cls) return c.get();
+    fail(MTL_DEVICE_ERROR, "representative column not found");
+  }
+
+  int find_rep() {
+    if (plan.group_keys.empty() || plan.sources.size() < 2) return -1;
+    for (const BJoin& j : plan.joins) unite({j.ls, j.lc}, {j.rs, j.rc});
+    for (int b : children[root]) {
+      bool all = true;
+      for (auto& k : plan.group_keys) {
+        if (k->src == b) continue;
+        auto cls = findc({k->src, k->col});
+        bool found = false;
+        for (auto& c : plan.sources[b].table->cols)
+          if (findc({b, c.get()}) == cls) found = true;
+        if (!found) all = false;
+      }
+      if (!all) continue;
+      // the build key of b must be (equal to) a group key: one group per build row
+      auto kcls = findc({b, up_col[b]});
+      bool has_key = false;
+      for (auto& k : plan.group_keys)
+        if (findc({k->src, k->col}) == kcls) has_key = true;
+      if (has_key) return b;
+    }
+    return -1;
+  }
+
+  uint64_t estimate_groups() {
+    const uint64_t rows = plan.sources[root].table->rows;
+    __int128 est = 1;
+    for (auto& k : plan.group_keys) {
+      Table& t = *plan.sources[k->src].table;
+      column_distinct(ctx, t, *k->col);
+      est *= (__int128)std::max<uint64_t>(1, k->col->distinct);
+      if (est > (__int128)rows) break;
+    }
+    uint64_t e = est > (__int128)rows ? rows : (uint64_t)est;
+    return std::max<uint64_t>(1, e);
+  }
+};
+
+}  // namespace
+
+std::unique_ptr<Program> compile(Ctx& ctx, const BoundPlan& plan) {
+  auto P = std::make_unique<Program>();
+  Compiler c{ctx, plan, *P};
+  try {
+    c.compile();
+  } catch (...) {
+    for (void* b : P->blocks) ctx.arena.free(b);
+    P->blocks.clear();
+    throw;
+  }
+  {
+    std::lock_guard<std::recursive_mutex> g(ctx.mu);
+    for (Column* col : c.pinned_cols) {
+      col->pins++;
+      P->pinned_cols.push_back(col);
+    }
+  }
+  return P;
+}
+
+void free_program(Ctx& ctx, Program& p) {
+  for (void* b : p.blocks) ctx.arena.free(b);
+  p.blocks.clear();
+  std::lock_guard<std::recursive_mutex> g(ctx.mu);
+  for (Column* c : p.pinned_cols) c->pins--;
+  p.pinned_cols.clear();
+}
+
+// ------------------------------------------------------------ run
+Program::~Program() {
+  for (cudaEvent_t e : prof_ev) cudaEventDestroy(e);
+}
+
+static const char* step_kind_name(Step::Kind k) {
+  switch (k) {
+    case Step::MEMSET: return "memset";
+    case Step::FILL: return "fill";
+    case Step::PIPELINE: return "pipeline";
+    case Step::COMPACT_FLAGS: return "compact_flags";
+    case Step::COMPACT_READY: return "compact_ready";
+    case Step::FINALIZE: return "finalize";
+    case Step::ENCODE: return "encode_keys";
+    case Step::RADIX: return "radix_sort";
+    case Step::TOPK: return "topk";
+    case Step::GATHER: return "gather";
+  }
+  return "step";
+}
+
+void run_program(Ctx& ctx, Program& p, cudaStream_t s) {
+  (void)ctx;
+  if (p.profile && p.prof_ev.size() != 2 * p.steps.size()) {
+    for (cudaEvent_t e : p.prof_ev) cudaEventDestroy(e);
+    p.prof_ev.assign(2 * p.steps.size(), nullptr);
+    for (auto& e : p.prof_ev) CK(cudaEventCreate(&e));
+  }
+  for (size_t i = 0; i < p.steps.size(); ++i) {
+    Step& st = p.steps[i];
+    if (st.name.empty()) st.name = step_kind_name(st.k);
+    if (p.profile) CK(cudaEventRecord(p.prof_ev[2 * i], s));
+    switch (st.k) {
+      case Step::MEMSET: CK(cudaMemsetAsync(st.ptr, st.byte, st.bytes, s)); break;
+      case Step::FILL: CK(launch_fill_u64((uint64_t*)st.ptr, st.bytes, st.fill, s)); break;
+      case Step::PIPELINE: CK(launch_pipeline(st.pipe, st.n_hint, s)); break;
+      case Step::COMPACT_FLAGS:
+        CK(launch_compact_flags((const uint8_t*)st.flag, st.n, st.n_dev, st.out_idx, st.out_count, st.tstatus,
+                                st.tcounter, 1, p.status, s));
+        break;
+      case Step::COMPACT_READY:
+        CK(launch_compact_ready((const uint32_t*)st.flag, st.n, st.out_idx, st.out_count, st.tstatus, st.tcounter, 1,
+                                p.status, s));
+        break;
+      case Step::FINALIZE: CK(launch_finalize(st.fin_dev, st.n_fin, st.idx, st.count, st.n_max, s)); break;
+      case Step::ENCODE: CK(launch_encode_keys(st.spec, st.count, st.n_max, st.keys, st.kidx, s)); break;
+      case Step::RADIX: {
+        int in_tmp = 0;
+        CK(launch_radix_sort(st.keys, st.kidx, st.keys_tmp, st.kidx_tmp, st.count, st.n_max, st.key_bytes, st.temp,
+                             s, &in_tmp));
+        break;
+      }
+      case Step::TOPK:
+        CK(launch_topk(st.keys, st.kidx, st.count, st.n_max, st.topk, st.out_idx, st.out_count, st.temp, p.status,
+                       s));
+        break;
+      case Step::GATHER: CK(launch_gather_width(st.gin, st.width, st.idx, st.count, st.n_max, st.gout, s)); break;
+    }
+    if (p.profile) CK(cudaEventRecord(p.prof_ev[2 * i + 1], s));
+  }
+}
+
+static void check_status(uint32_t st) {
+  if (!st) return;
+  if (st & ST_OVERFLOW) fail(MTL_OVERFLOW, "Overflow in integer arithmetic (out of range for the result type)");
+  if (st & ST_SPIN_LIMIT) fail(MTL_DEVICE_ERROR, "a device wait exceeded its iteration limit");
+  if (st & ST_TABLE_FULL) fail(MTL_DEVICE_ERROR, "a device hash table ran out of slots");
+  if (st & ST_DUP_BUILD_KEY) fail(MTL_DEVICE_ERROR, "duplicate key on a unique join build side");
+  if (st & ST_CAPACITY) fail(MTL_DEVICE_ERROR, "a device output buffer was too small");
+}
+
+std::shared_ptr<Result> fetch_program(Ctx& ctx, Program& p, cudaStream_t s) {
+  (void)ctx;
+  uint32_t st = 0;
+  uint64_t count = 0;
+  CK(cudaMemcpyAsync(&st, p.status, 4, cudaMemcpyDeviceToHost, s));
+  if (p.out_count) CK(cudaMemcpyAsync(&count, p.out_count, 8, cudaMemcpyDeviceToHost, s));
+  uint64_t empty = 1;
+  if (p.empty_count) CK(cudaMemcpyAsync(&empty, p.empty_count, 8, cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  check_status(st);
+  if (!p.out_count) count = p.fixed_count == UINT64_MAX ? 0 : p.fixed_count;
+  if (count > p.n_max) count = p.n_max;
+  if (p.limit >= 0 && count > (uint64_t)p.limit) count = (uint64_t)p.limit;
+  auto r = std::make_shared<Result>();
+  r->rows = (int64_t)count;
+  for (const OutBuf& o : p.outs) {
+    ResultCol c;
+    c.name = o.name;
+    c.type = o.type;
+    c.width = o.width;
+    c.data.resize(count * o.width);
+    if (count) CK(cudaMemcpyAsync(c.data.data(), o.dev, count * o.width, cudaMemcpyDeviceToHost, s));
+    if (o.dict) c.dict = *o.dict;
+    r->cols.push_back(std::move(c));
+  }
+  CK(cudaStreamSynchronize(s));
+  if (p.empty_count && empty == 0) {
+    // ungrouped aggregate over no rows: everything but COUNT is NULL
+    for (ResultCol& c : r->cols) {
+      if (c.type.t == MTL_T_BIGINT && c.name.find("count") != std::string::npos) continue;
+      c.valid.assign(count, 0);
+    }
+  }
+  return r;
+}
+
+// ------------------------------------------------------------ constants
+std::shared_ptr<Result> constant_result(const BoundPlan& plan) {
+  auto r = std::make_shared<Result>();
+  r->rows = plan.limit == 0 ? 0 : 1;
+  for (const BOut& o : plan.outputs) {
+    ResultCol c;
+    c.name = o.name;
+    c.type = o.type;
+    c.width = ptype_width(storage_ptype(o.type));
+    c.data.resize(r->rows * c.width);
+    if (r->rows) {
+      int64_t v[2] = {o.expr->lo, o.expr->hi};
+      memcpy(c.data.data(), v, c.width);
+    }
+    r->cols.push_back(std::move(c));
+  }
+  return r;
+}
+
+// ------------------------------------------------------------ gpu_processing
+static bool query_cache_enabled() { return std::getenv("METTLE_DISABLE_QUERY_CACHE") == nullptr; }
+static const size_t kQueryCacheEntries = 32;  // src/source_cache.rs:230-233
+
+static std::string trim(const std::string& s) {
+  size_t b = s.find_first_not_of(" \t\r\n"), e = s.find_last_not_of(" \t\r\n;");
+  if (b == std::string::npos) return "";
+  return s.substr(b, e - b + 1);
+}
+
+std::shared_ptr<Result> processing(Ctx& ctx, const std::string& sql_in) {
+  const std::string sql = trim(sql_in);
+  if (sql.empty()) fail(MTL_INVALID, "gpu_processing requires a non-empty SQL string");
+  {
+    std::lock_guard<std::recursive_mutex> g(ctx.mu);
+    ctx.last_mode.clear();
+  }
+  const std::string key = std::to_string(ctx.table_version) + "\x1f" + sql;
+  if (query_cache_enabled()) {
+    std::lock_guard<std::recursive_mutex> g(ctx.mu);
+    for (auto it = ctx.qcache.begin(); it != ctx.qcache.end(); ++it) {
+      if (it->first == key) {
+        ctx.qcache.splice(ctx.qcache.begin(), ctx.qcache, it);
+        ctx.last_mode = "cuda_hot_query_cache";
+        return ctx.qcache.front().second;
+      }
+    }
+  }
+  SelectStmt st;
+  try {
+    st = parse_sql(sql);
+  } catch (const SqlError& e) {
+    fail(MTL_UNSUPPORTED, std::string("SQL outside the offloaded subset: ") + e.what());
+  }
+  BoundPlan plan = bind_select(ctx, st);
+  std::shared_ptr<Result> r;
+  std::string mode;
+  if (plan.constant_only) {
+    r = constant_result(plan);
+    mode = "host_constant";
+  } else {
+    auto prog = compile(ctx, plan);
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    try {
+      CK(cudaEventRecord(e0, ctx.stream));
+      run_program(ctx, *prog, ctx.stream);
+      CK(cudaEventRecord(e1, ctx.stream));
+      r = fetch_program(ctx, *prog, ctx.stream);
+      float ms = 0;
+      cudaEventElapsedTime(&ms, e0, e1);
+      r->device_ms = ms;
+    } catch (...) {
+      cudaStreamSynchronize(ctx.stream);
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
+      free_program(ctx, *prog);
+      throw;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    free_program(ctx, *prog);
+    mode = "cuda_generic_plan";
+  }
+  std::lock_guard<std::recursive_mutex> g(ctx.mu);
+  ctx.last_mode = mode;
+  if (query_cache_enabled() && mode != "host_constant") {
+    ctx.qcache.emplace_front(key, r);
+    if (plan.grouped_topk) ctx.grouped_topk_entries++;
+    while (ctx.qcache.size() > kQueryCacheEntries) ctx.qcache.pop_back();
+  }
+  return r;
+}
+
+}  // namespace mtl

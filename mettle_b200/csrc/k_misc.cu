@@ -1,0 +1,384 @@
+// k_misc.cu — compaction of aggregate tables, final aggregate outputs,
+// gathers, the scalar SQL hooks and column statistics (sm_100a).
+#include "kern_common.cuh"
+#include "kernels.h"
+
+namespace mtl {
+
+namespace {
+constexpr int kCThreads = 256;
+constexpr int kCItems = 16;
+constexpr int kCTile = kCThreads * kCItems;
+
+int sms() {
+  static int n = 0;
+  if (!n) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    if (n <= 0) n = 148;
+  }
+  return n;
+}
+unsigned grid_for(uint64_t n, int threads, int per_sm = 8) {
+  uint64_t b = (n + threads - 1) / threads;
+  uint64_t cap = (uint64_t)sms() * per_sm;
+  if (b > cap) b = cap;
+  return b ? (unsigned)b : 1u;
+}
+}  // namespace
+
+size_t compact_tile_rows() { return kCTile; }
+
+// ------------------------------------------------------------ compaction
+// Order-preserving index compaction with decoupled look-back; the reference
+// compacts with a global atomic per element (compact_grouped_rows,
+// kernels.metal:1120), which loses the order.
+template <typename Flag>
+__global__ void __launch_bounds__(kCThreads) k_compact(Flag flag, uint64_t n_static, const uint64_t* n_dev,
+                                                       uint32_t* out_idx, uint64_t* out_count, uint64_t* tstatus,
+                                                       uint32_t* counter, uint32_t epoch, uint32_t* status) {
+  __shared__ uint32_t s_warp[kCThreads / 32 + 1];
+  __shared__ uint64_t s_tile, s_base;
+  const uint64_t n = n_dev ? *n_dev : n_static;
+  const uint64_t n_tiles = (n + kCTile - 1) / kCTile;
+  const int tid = threadIdx.x;
+  for (;;) {
+    if (tid == 0) s_tile = atomicAdd(counter, 1u);
+    __syncthreads();
+    const uint64_t tile = s_tile;
+    if (tile >= n_tiles) break;
+    const uint64_t base_i = tile * kCTile + (uint64_t)tid * kCItems;
+    uint32_t bits = 0;
+#pragma unroll
+    for (int i = 0; i < kCItems; ++i) {
+      uint64_t g = base_i + i;
+      bits |= (g < n && flag(g)) ? (1u << i) : 0u;
+    }
+    uint32_t total;
+    uint32_t pos = block_excl_sum<kCThreads>(__popc(bits), s_warp, &total);
+    if (tid == 0) {
+      uint64_t excl = lb_exclusive(tstatus, tile, total, epoch, status);
+      s_base = excl;
+      if (tile == n_tiles - 1) *out_count = excl + total;
+    }
+    __syncthreads();
+    const uint64_t base = s_base;
+#pragma unroll
+    for (int i = 0; i < kCItems; ++i)
+      if ((bits >> i) & 1u) out_idx[base + pos++] = (uint32_t)(base_i + i);
+    __syncthreads();
+  }
+  if (tid == 0) {
+    if (n == 0 && blockIdx.x == 0) *out_count = 0;
+    __threadfence();
+    if (atomicAdd(counter + 1, 1u) == gridDim.x - 1) {
+      counter[0] = 0;
+      counter[1] = 0;
+    }
+  }
+}
+
+struct ReadyFlag {
+  const uint32_t* state;
+  __device__ bool operator()(uint64_t i) const { return state[i] == 2u; }
+};
+struct ByteFlag {
+  const uint8_t* f;
+  __device__ bool operator()(uint64_t i) const { return f[i] != 0; }
+};
+
+cudaError_t launch_compact_ready(const uint32_t* state, uint64_t capacity, uint32_t* out_idx, uint64_t* out_count,
+                                 uint64_t* tile_status, uint32_t* tile_counter, uint32_t epoch, uint32_t* status,
+                                 cudaStream_t s) {
+  uint64_t tiles = (capacity + kCTile - 1) / kCTile;
+  unsigned grid = (unsigned)(tiles < (uint64_t)sms() * 8 ? (tiles ? tiles : 1) : sms() * 8);
+  k_compact<ReadyFlag><<<grid, kCThreads, 0, s>>>(ReadyFlag{state}, capacity, nullptr, out_idx, out_count,
+                                                  tile_status, tile_counter, epoch, status);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_compact_flags(const uint8_t* flag, uint64_t n, const uint64_t* n_dev, uint32_t* out_idx,
+                                 uint64_t* out_count, uint64_t* tile_status, uint32_t* tile_counter, uint32_t epoch,
+                                 uint32_t* status, cudaStream_t s) {
+  uint64_t tiles = (n + kCTile - 1) / kCTile;
+  unsigned grid = (unsigned)(tiles < (uint64_t)sms() * 8 ? (tiles ? tiles : 1) : sms() * 8);
+  k_compact<ByteFlag><<<grid, kCThreads, 0, s>>>(ByteFlag{flag}, n, n_dev, out_idx, out_count, tile_status,
+                                                 tile_counter, epoch, status);
+  return cudaGetLastError();
+}
+
+// ------------------------------------------------------------ gathers
+template <typename T>
+__global__ void k_gather(const T* __restrict__ in, const uint32_t* __restrict__ idx, const uint64_t* count,
+                         uint64_t n_max, T* __restrict__ out) {
+  const uint64_t n = count ? *count : n_max;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+    out[i] = in[idx[i]];
+}
+
+cudaError_t launch_gather_u64(const uint64_t* in, const uint32_t* idx, const uint64_t* count, uint64_t n_max,
+                              uint64_t* out, cudaStream_t s) {
+  k_gather<uint64_t><<<grid_for(n_max, 256), 256, 0, s>>>(in, idx, count, n_max, out);
+  return cudaGetLastError();
+}
+cudaError_t launch_gather_u32(const uint32_t* in, const uint32_t* idx, const uint64_t* count, uint64_t n_max,
+                              uint32_t* out, cudaStream_t s) {
+  k_gather<uint32_t><<<grid_for(n_max, 256), 256, 0, s>>>(in, idx, count, n_max, out);
+  return cudaGetLastError();
+}
+cudaError_t launch_gather_width(const void* in, int width, const uint32_t* idx, const uint64_t* count, uint64_t n_max,
+                                void* out, cudaStream_t s) {
+  unsigned g = grid_for(n_max, 256);
+  switch (width) {
+    case 4: k_gather<uint32_t><<<g, 256, 0, s>>>((const uint32_t*)in, idx, count, n_max, (uint32_t*)out); break;
+    case 8: k_gather<uint64_t><<<g, 256, 0, s>>>((const uint64_t*)in, idx, count, n_max, (uint64_t*)out); break;
+    case 16: k_gather<longlong2><<<g, 256, 0, s>>>((const longlong2*)in, idx, count, n_max, (longlong2*)out); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
+// ------------------------------------------------------------ finalize
+// AVG of a 128-bit integer sum as DuckDB computes it on x86-64
+// (IntegerAverageOperationHugeint): the quotient is formed in x87 extended
+// precision (64-bit significand, round to nearest even) and then stored as
+// a double (a second rounding to 53 bits). Emulated exactly with integer
+// arithmetic; the sum is assumed below 2^64 in magnitude (the long double
+// image of larger sums is rounded, and this emulation rounds it the same
+// way only when the discarded bits are not a tie).
+__device__ double avg_extended(__int128 sum, unsigned long long count) {
+  if (sum == 0 || count == 0) return 0.0;
+  const bool neg = sum < 0;
+  unsigned __int128 S = neg ? (unsigned __int128)(-sum) : (unsigned __int128)sum;
+  const unsigned __int128 C = count;
+  int lenS = 0;
+  {
+    uint64_t hi = (uint64_t)(S >> 64), lo = (uint64_t)S;
+    lenS = hi ? 128 - __clzll((long long)hi) : 64 - __clzll((long long)lo);
+  }
+  // Round S itself to a 64-bit significand if it is wider.
+  int sexp = 0;
+  if (lenS > 64) {
+    int drop = lenS - 64;
+    unsigned __int128 q = S >> drop, rem = S & ((((unsigned __int128)1) << drop) - 1);
+    unsigned __int128 half = ((unsigned __int128)1) << (drop - 1);
+    if (rem > half || (rem == half && (q & 1))) q += 1;
+    if (q >> 64) { q >>= 1; drop += 1; }
+    S = q;
+    sexp = drop;
+    lenS = 64;
+  }
+  const int lenC = 64 - __clzll((long long)count);
+  // Quotient with a 64-bit significand: Q = floor(S * 2^k / C).
+  int k = 64 - (lenS - lenC);
+  unsigned __int128 Q, R, D;
+  for (int attempt = 0; attempt < 3; ++attempt) {
+    if (k >= 0) {
+      unsigned __int128 N = S << k;
+      D = C;
+      Q = N / D;
+      R = N % D;
+    } else {
+      D = C << (-k);
+      Q = S / D;
+      R = S % D;
+    }
+    if (Q >> 64) { --k; continue; }
+    if (!(Q >> 63)) { ++k; continue; }
+    break;
+  }
+  // Round to 64 bits (nearest even) on the exact remainder.
+  unsigned __int128 twoR = R << 1;
+  if (twoR > D || (twoR == D && (Q & 1))) Q += 1;
+  if (Q >> 64) { Q >>= 1; --k; }
+  // Second rounding, 64 -> 53 bits, on the 11 dropped bits alone.
+  uint64_t q64 = (uint64_t)Q;
+  uint64_t low = q64 & 0x7FFULL, m = q64 >> 11;
+  if (low > 0x400ULL || (low == 0x400ULL && (m & 1))) m += 1;
+  int e = 11 - k + sexp;
+  if (m >> 53) { m >>= 1; e += 1; }
+  double r = ldexp((double)m, e);
+  return neg ? -r : r;
+}
+
+__global__ void k_finalize(const FinalOut* __restrict__ outs, int n_outs, const uint32_t* __restrict__ idx,
+                           const uint64_t* count, uint64_t n_max) {
+  const uint64_t n = count ? *count : n_max;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t g = idx ? idx[i] : i;
+    for (int o = 0; o < n_outs; ++o) {
+      const FinalOut f = outs[o];
+      switch (f.kind) {
+        case F_COPY_I32:
+        case F_COPY_F32: ((uint32_t*)f.out)[i] = (uint32_t)f.a[g]; break;
+        case F_COPY_I64:
+        case F_COPY_F64: ((uint64_t*)f.out)[i] = f.a[g]; break;
+        case F_SUM_I128: ((longlong2*)f.out)[i] = make_longlong2((long long)f.a[g], (long long)f.a_hi[g]); break;
+        case F_SUM_I64_AS_I128: {
+          long long v = (long long)f.a[g];
+          ((longlong2*)f.out)[i] = make_longlong2(v, v < 0 ? -1LL : 0LL);
+          break;
+        }
+        case F_MINMAX_F32: ((float*)f.out)[i] = (float)unord_f64(f.a[g]); break;
+        case F_MINMAX_F64: ((double*)f.out)[i] = unord_f64(f.a[g]); break;
+        case F_AVG_I128_LD: {
+          __int128 s = f.a_hi ? (__int128)(((unsigned __int128)(uint64_t)f.a_hi[g] << 64) | f.a[g])
+                              : (__int128)(long long)f.a[g];
+          ((double*)f.out)[i] = avg_extended(s, f.cnt[g]);
+          break;
+        }
+        case F_AVG_I64_D:
+          ((double*)f.out)[i] = __ddiv_rn(__ll2double_rn((long long)f.a[g]), __ull2double_rn(f.cnt[g]));
+          break;
+        case F_AVG_F64:
+          ((double*)f.out)[i] = __ddiv_rn(__longlong_as_double((long long)f.a[g]), __ull2double_rn(f.cnt[g]));
+          break;
+        case F_AVG_DEC: {
+          __int128 s = f.a_hi ? (__int128)(((unsigned __int128)(uint64_t)f.a_hi[g] << 64) | f.a[g])
+                              : (__int128)(long long)f.a[g];
+          ((double*)f.out)[i] = avg_extended(s, f.cnt[g] * (unsigned long long)f.scale);
+          break;
+        }
+        case F_GATHER_COL: {
+          const uint32_t r = f.rid[g];
+          if (f.width == 4) ((uint32_t*)f.out)[i] = ((const uint32_t*)f.col)[r];
+          else ((uint64_t*)f.out)[i] = ((const uint64_t*)f.col)[r];
+          break;
+        }
+        default: break;
+      }
+    }
+  }
+}
+
+cudaError_t launch_finalize(const FinalOut* outs, int n_outs, const uint32_t* idx, const uint64_t* count,
+                            uint64_t n_max, cudaStream_t s) {
+  k_finalize<<<grid_for(n_max, 256), 256, 0, s>>>(outs, n_outs, idx, count, n_max);
+  return cudaGetLastError();
+}
+
+// ------------------------------------------------------------ scalar hooks
+// gpu_add_scalar / gpu_mul_scalar: out = in op k with DuckDB result types
+// and overflow errors; the reference's project_*_scalar kernels
+// (kernels.metal:4-68) compute the same element-wise op.
+__global__ void k_scalar_arith(int op, int ptype, const void* __restrict__ in, uint64_t n, int64_t ilit, double flit,
+                               void* __restrict__ out, uint32_t* status) {
+  uint32_t st = 0;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    switch (ptype) {
+      case P_I32: {
+        int64_t x = ((const int32_t*)in)[i];
+        int64_t r = op == 0 ? x + ilit : x * ilit;
+        ((int32_t*)out)[i] = (int32_t)fit32(r, st);
+        break;
+      }
+      case P_I64: {
+        int64_t x = ((const int64_t*)in)[i];
+        ((int64_t*)out)[i] = op == 0 ? add64(x, ilit, st) : mul64(x, ilit, st);
+        break;
+      }
+      case P_F32: {
+        float x = ((const float*)in)[i], k = (float)flit;
+        ((float*)out)[i] = op == 0 ? __fadd_rn(x, k) : __fmul_rn(x, k);
+        break;
+      }
+      default: {
+        double x = ((const double*)in)[i];
+        ((double*)out)[i] = op == 0 ? __dadd_rn(x, flit) : __dmul_rn(x, flit);
+        break;
+      }
+    }
+  }
+  if (st) atomicOr(status, st);
+}
+
+// gpu_{eq,lt,le,gt,ge}_scalar: u8 mask with the reference's op codes
+// (compare_*_scalar, kernels.metal:70-173).
+__global__ void k_scalar_compare(int op, int ptype, const void* __restrict__ in, uint64_t n, int64_t ilit, double flit,
+                                 uint8_t* __restrict__ out) {
+  DPred p;
+  p.col = 0;
+  p.op = op;
+  p.ilit = ilit;
+  p.flit = flit;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+    out[i] = eval_pred_bits(load_bits(in, ptype, i), ptype, p) ? 1 : 0;
+}
+
+cudaError_t launch_scalar_arith(int op, int ptype, const void* in, uint64_t n, int64_t ilit, double flit, void* out,
+                                uint32_t* status, cudaStream_t s) {
+  k_scalar_arith<<<grid_for(n, 256), 256, 0, s>>>(op, ptype, in, n, ilit, flit, out, status);
+  return cudaGetLastError();
+}
+cudaError_t launch_scalar_compare(int op, int ptype, const void* in, uint64_t n, int64_t ilit, double flit, uint8_t* out,
+                                  cudaStream_t s) {
+  k_scalar_compare<<<grid_for(n, 256), 256, 0, s>>>(op, ptype, in, n, ilit, flit, out);
+  return cudaGetLastError();
+}
+
+// ------------------------------------------------------------ statistics
+__global__ void k_minmax(const void* __restrict__ col, int ptype, uint64_t n, int64_t* out) {
+  int64_t mn = 0x7FFFFFFFFFFFFFFFLL, mx = (int64_t)0x8000000000000000ULL;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    int64_t v = load_bits(col, ptype, i);
+    mn = v < mn ? v : mn;
+    mx = v > mx ? v : mx;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    int64_t a = __shfl_down_sync(0xFFFFFFFFu, mn, o), b = __shfl_down_sync(0xFFFFFFFFu, mx, o);
+    mn = a < mn ? a : mn;
+    mx = b > mx ? b : mx;
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicMin((long long*)out, (long long)mn);
+    atomicMax((long long*)out + 1, (long long)mx);
+  }
+}
+
+cudaError_t launch_minmax_i(const void* col, int ptype, uint64_t n, int64_t* out, cudaStream_t s) {
+  k_minmax<<<grid_for(n, 256, 4), 256, 0, s>>>(col, ptype, n, out);
+  return cudaGetLastError();
+}
+
+__global__ void k_count_dups(const void* __restrict__ col, int ptype, uint64_t n, int64_t* table, uint64_t cap,
+                             uint32_t* special, unsigned long long* out) {
+  unsigned long long dups = 0;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    int64_t key = load_bits(col, ptype, i);
+    if (key == kEmptyKey) {
+      if (atomicAdd(special, 1u) != 0u) ++dups;
+      continue;
+    }
+    uint64_t h = hash_slot(hash64((uint64_t)key), cap);
+    for (uint64_t p = 0; p < cap; ++p) {
+      unsigned long long prev =
+          atomicCAS((unsigned long long*)(table + h), (unsigned long long)kEmptyKey, (unsigned long long)key);
+      if (prev == (unsigned long long)kEmptyKey) break;
+      if ((int64_t)prev == key) {
+        ++dups;
+        break;
+      }
+      if (++h == cap) h = 0;
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) dups += __shfl_down_sync(0xFFFFFFFFu, dups, o);
+  if ((threadIdx.x & 31) == 0 && dups) atomicAdd(out, dups);
+}
+
+cudaError_t launch_count_dups(const void* col, int ptype, uint64_t n, int64_t* table, uint64_t cap, uint32_t* special,
+                              unsigned long long* out, cudaStream_t s) {
+  k_count_dups<<<grid_for(n, 256), 256, 0, s>>>(col, ptype, n, table, cap, special, out);
+  return cudaGetLastError();
+}
+
+__global__ void k_fill_u64(uint64_t* p, uint64_t n, uint64_t v) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+    p[i] = v;
+}
+cudaError_t launch_fill_u64(uint64_t* p, uint64_t n, uint64_t v, cudaStream_t s) {
+  k_fill_u64<<<grid_for(n, 256), 256, 0, s>>>(p, n, v);
+  return cudaGetLastError();
+}
+
+}  // namespace mtl

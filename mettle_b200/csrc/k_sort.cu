@@ -1,0 +1,405 @@
+// k_sort.cu — ORDER BY on sm_100a: order-preserving key encoding, a stable
+// LSD radix sort (8-bit digits, warp match-based stable ranking), and a
+// block-local top-K with threshold pruning and bitonic merges in shared
+// memory. The reference sorts the final batch on the CPU
+// (src/plan/helpers.rs:627-667) and runs its grouped top-K with a single
+// thread for K > 20 (topk_dense_grouped_rows, kernels.metal:1162) or one
+// 128-thread group with a serial merge (kernels.metal:1249); its tie order
+// (sum DESC, secondary ASC, row id ASC, kernels.metal:1102-1118) is kept by
+// encoding every ORDER BY part, then the tie-break parts, into one key.
+#include "kern_common.cuh"
+#include "kernels.h"
+
+namespace mtl {
+
+namespace {
+int sms() {
+  static int n = 0;
+  if (!n) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    if (n <= 0) n = 148;
+  }
+  return n;
+}
+}  // namespace
+
+// ------------------------------------------------------------ key encoding
+struct U256 {
+  uint64_t w[4];  // w[0] most significant
+};
+
+__device__ __forceinline__ void shl_or(U256& k, int bits, uint64_t lo, uint64_t hi) {
+  // k = (k << bits) | value, value given as (hi, lo) with `bits` significant bits.
+  while (bits > 0) {
+    int b = bits > 64 ? 64 : bits;
+    uint64_t part = bits > 64 ? hi : lo;
+    if (bits > 64) bits -= 64; else bits = 0;
+    if (b == 64) {
+      k.w[0] = k.w[1]; k.w[1] = k.w[2]; k.w[2] = k.w[3]; k.w[3] = part;
+    } else {
+      k.w[0] = (k.w[0] << b) | (k.w[1] >> (64 - b));
+      k.w[1] = (k.w[1] << b) | (k.w[2] >> (64 - b));
+      k.w[2] = (k.w[2] << b) | (k.w[3] >> (64 - b));
+      k.w[3] = (k.w[3] << b) | (part & ((1ULL << b) - 1));
+    }
+  }
+}
+
+__global__ void k_encode(const __grid_constant__ SortKeySpec spec, const uint64_t* count, uint64_t n_max,
+                         SortItem* __restrict__ keys, uint32_t* __restrict__ idx) {
+  const uint64_t n = count ? *count : n_max;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    U256 k{{0, 0, 0, 0}};
+    for (int p = 0; p < spec.n_parts; ++p) {
+      const int pt = spec.ptype[p];
+      uint64_t lo = 0, hi = 0;
+      int bits = 64;
+      switch (pt) {
+        case P_I32:
+          lo = (uint64_t)(uint32_t)(((const int32_t*)spec.col[p])[i] ^ (int32_t)0x80000000);
+          bits = 32;
+          break;
+        case P_F32: {
+          uint32_t b = ((const uint32_t*)spec.col[p])[i];
+          lo = (b & 0x80000000u) ? (uint64_t)(~b) : (uint64_t)(b | 0x80000000u);
+          lo &= 0xFFFFFFFFULL;
+          bits = 32;
+          break;
+        }
+        case P_I64: lo = ord_i64(((const int64_t*)spec.col[p])[i]); break;
+        case P_F64: lo = ord_f64_bits(((const uint64_t*)spec.col[p])[i]); break;
+        case P_I128: {
+          // longlong2 {lo, hi}: flip the sign bit of hi for an unsigned image.
+          longlong2 v = ((const longlong2*)spec.col[p])[i];
+          lo = (uint64_t)v.x;
+          hi = (uint64_t)v.y ^ 0x8000000000000000ULL;
+          bits = 128;
+          break;
+        }
+        default: break;
+      }
+      if (spec.desc[p]) {
+        lo = ~lo;
+        hi = ~hi;
+        if (bits == 32) lo &= 0xFFFFFFFFULL;
+      }
+      shl_or(k, bits, lo, hi);
+    }
+    SortItem it;
+    it.w[0] = k.w[0]; it.w[1] = k.w[1]; it.w[2] = k.w[2]; it.w[3] = k.w[3];
+    keys[i] = it;
+    idx[i] = (uint32_t)i;
+  }
+}
+
+cudaError_t launch_encode_keys(const SortKeySpec& spec, const uint64_t* count, uint64_t n_max, SortItem* keys,
+                               uint32_t* idx, cudaStream_t s) {
+  uint64_t b = (n_max + 255) / 256;
+  uint64_t cap = (uint64_t)sms() * 8;
+  if (b > cap) b = cap;
+  if (!b) b = 1;
+  k_encode<<<(unsigned)b, 256, 0, s>>>(spec, count, n_max, keys, idx);
+  return cudaGetLastError();
+}
+
+// ------------------------------------------------------------ radix sort
+constexpr int kRThreads = 256;
+constexpr int kRItems = 16;
+constexpr int kRTile = kRThreads * kRItems;
+constexpr int kRWarps = kRThreads / 32;
+
+__device__ __forceinline__ uint32_t digit_of(const SortItem& k, int byte) {
+  return (uint32_t)(k.w[3 - (byte >> 3)] >> ((byte & 7) * 8)) & 0xFFu;
+}
+
+__global__ void __launch_bounds__(kRThreads) k_radix_hist(const SortItem* __restrict__ keys, const uint64_t* count,
+                                                          uint64_t n_tiles_max, int byte, uint32_t* __restrict__ hist) {
+  __shared__ uint32_t s_h[256];
+  const uint64_t n = *count;
+  for (uint64_t tile = blockIdx.x; tile < n_tiles_max; tile += gridDim.x) {
+    for (int i = threadIdx.x; i < 256; i += kRThreads) s_h[i] = 0;
+    __syncthreads();
+    const uint64_t base = tile * kRTile;
+    for (int r = 0; r < kRItems; ++r) {
+      uint64_t g = base + (uint64_t)r * kRThreads + threadIdx.x;
+      if (g < n) atomicAdd(&s_h[digit_of(keys[g], byte)], 1u);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < 256; i += kRThreads) hist[(uint64_t)i * n_tiles_max + tile] = s_h[i];
+    __syncthreads();
+  }
+}
+
+// In-place exclusive scan of a u32 array in chunks: chunk sums first.
+constexpr int kSChunk = 4096;
+__global__ void k_scan_chunks(uint32_t* __restrict__ a, uint64_t n, uint32_t* __restrict__ sums) {
+  __shared__ uint32_t s_warp[kRThreads / 32 + 1];
+  const uint64_t base = (uint64_t)blockIdx.x * kSChunk;
+  constexpr int per = kSChunk / kRThreads;
+  uint32_t v[per];
+  uint32_t tot = 0;
+#pragma unroll
+  for (int i = 0; i < per; ++i) {
+    uint64_t g = base + (uint64_t)threadIdx.x * per + i;
+    v[i] = g < n ? a[g] : 0;
+    tot += v[i];
+  }
+  uint32_t total;
+  uint32_t pre = block_excl_sum<kRThreads>(tot, s_warp, &total);
+#pragma unroll
+  for (int i = 0; i < per; ++i) {
+    uint64_t g = base + (uint64_t)threadIdx.x * per + i;
+    if (g < n) a[g] = pre;
+    pre += v[i];
+  }
+  if (threadIdx.x == 0) sums[blockIdx.x] = total;
+}
+__global__ void k_scan_small(uint32_t* __restrict__ a, uint64_t n) {
+  // One CTA: exclusive scan of up to a few hundred thousand entries.
+  __shared__ uint32_t s_warp[kRThreads / 32 + 1];
+  uint32_t carry = 0;
+  for (uint64_t base = 0; base < n; base += kRThreads) {
+    uint64_t g = base + threadIdx.x;
+    uint32_t v = g < n ? a[g] : 0;
+    uint32_t total;
+    uint32_t pre = block_excl_sum<kRThreads>(v, s_warp, &total);
+    if (g < n) a[g] = carry + pre;
+    carry += total;
+  }
+}
+__global__ void k_scan_add(uint32_t* __restrict__ a, uint64_t n, const uint32_t* __restrict__ sums) {
+  const uint64_t base = (uint64_t)blockIdx.x * kSChunk;
+  const uint32_t add = sums[blockIdx.x];
+  for (int i = threadIdx.x; i < kSChunk; i += kRThreads) {
+    uint64_t g = base + i;
+    if (g < n) a[g] += add;
+  }
+}
+
+// Stable scatter: elements are ranked in index order within the tile using
+// warp match masks and per-warp digit counts in shared memory.
+__global__ void __launch_bounds__(kRThreads) k_radix_scatter(const SortItem* __restrict__ keys,
+                                                             const uint32_t* __restrict__ idx, const uint64_t* count,
+                                                             uint64_t n_tiles_max, int byte,
+                                                             const uint32_t* __restrict__ hist,
+                                                             SortItem* __restrict__ okeys, uint32_t* __restrict__ oidx) {
+  __shared__ uint32_t s_base[256];
+  __shared__ uint16_t s_wc[kRWarps][256];
+  const uint64_t n = *count;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint32_t lt = (1u << lane) - 1u;
+  for (uint64_t tile = blockIdx.x; tile < n_tiles_max; tile += gridDim.x) {
+    const uint64_t base = tile * kRTile;
+    if (base >= n) break;
+    for (int i = threadIdx.x; i < 256; i += kRThreads) s_base[i] = hist[(uint64_t)i * n_tiles_max + tile];
+    __syncthreads();
+    for (int r = 0; r < kRItems; ++r) {
+      const uint64_t g = base + (uint64_t)r * kRThreads + threadIdx.x;
+      const bool valid = g < n;
+      SortItem k;
+      uint32_t ix = 0, d = 256;
+      if (valid) {
+        k = keys[g];
+        ix = idx[g];
+        d = digit_of(k, byte);
+      }
+      for (int i = threadIdx.x; i < kRWarps * 256; i += kRThreads) (&s_wc[0][0])[i] = 0;
+      __syncthreads();
+      const uint32_t peers = __match_any_sync(0xFFFFFFFFu, d);
+      const uint32_t rank = __popc(peers & lt);
+      if (valid && rank == 0) s_wc[warp][d] = (uint16_t)__popc(peers);
+      __syncthreads();
+      uint32_t off = 0;
+      if (valid) {
+        off = s_base[d];
+        for (int w = 0; w < warp; ++w) off += s_wc[w][d];
+        off += rank;
+        okeys[off] = k;
+        oidx[off] = ix;
+      }
+      __syncthreads();
+      // advance the running per-digit base by this round's counts
+      for (int dd = threadIdx.x; dd < 256; dd += kRThreads) {
+        uint32_t t = 0;
+        for (int w = 0; w < kRWarps; ++w) t += s_wc[w][dd];
+        s_base[dd] += t;
+      }
+      __syncthreads();
+    }
+  }
+}
+
+size_t radix_sort_temp_bytes(uint64_t n_max) {
+  uint64_t tiles = (n_max + kRTile - 1) / kRTile;
+  if (!tiles) tiles = 1;
+  uint64_t hist = tiles * 256;
+  uint64_t chunks = (hist + kSChunk - 1) / kSChunk;
+  return (hist + chunks + 64) * sizeof(uint32_t);
+}
+
+cudaError_t launch_radix_sort(SortItem* keys, uint32_t* idx, SortItem* keys_tmp, uint32_t* idx_tmp,
+                              const uint64_t* count, uint64_t n_max, int key_bytes, void* temp, cudaStream_t s,
+                              int* result_in_tmp) {
+  uint64_t tiles = (n_max + kRTile - 1) / kRTile;
+  if (!tiles) tiles = 1;
+  const uint64_t hn = tiles * 256;
+  uint32_t* hist = (uint32_t*)temp;
+  uint32_t* sums = hist + hn;
+  const uint64_t chunks = (hn + kSChunk - 1) / kSChunk;
+  unsigned grid = (unsigned)(tiles < (uint64_t)sms() * 4 ? tiles : (uint64_t)sms() * 4);
+  SortItem* src_k = keys;
+  uint32_t* src_i = idx;
+  SortItem* dst_k = keys_tmp;
+  uint32_t* dst_i = idx_tmp;
+  for (int b = 0; b < key_bytes; ++b) {
+    k_radix_hist<<<grid, kRThreads, 0, s>>>(src_k, count, tiles, b, hist);
+    if (chunks == 1) {
+      k_scan_small<<<1, kRThreads, 0, s>>>(hist, hn);
+    } else {
+      k_scan_chunks<<<(unsigned)chunks, kRThreads, 0, s>>>(hist, hn, sums);
+      k_scan_small<<<1, kRThreads, 0, s>>>(sums, chunks);
+      k_scan_add<<<(unsigned)chunks, kRThreads, 0, s>>>(hist, hn, sums);
+    }
+    k_radix_scatter<<<grid, kRThreads, 0, s>>>(src_k, src_i, count, tiles, b, hist, dst_k, dst_i);
+    SortItem* tk = src_k; src_k = dst_k; dst_k = tk;
+    uint32_t* ti = src_i; src_i = dst_i; dst_i = ti;
+  }
+  *result_in_tmp = (key_bytes & 1) ? 1 : 0;
+  return cudaGetLastError();
+}
+
+// ------------------------------------------------------------ top-K
+__device__ __forceinline__ bool item_less(const SortItem& a, uint32_t ia, const SortItem& b, uint32_t ib) {
+#pragma unroll
+  for (int w = 0; w < 4; ++w)
+    if (a.w[w] != b.w[w]) return a.w[w] < b.w[w];
+  return ia < ib;
+}
+
+// Bitonic sort of B (SortItem, idx) pairs in shared memory, ascending.
+template <int B, int THREADS>
+__device__ void bitonic_sort(SortItem* sk, uint32_t* si) {
+  for (int size = 2; size <= B; size <<= 1) {
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+      for (int t = threadIdx.x; t < B / 2; t += THREADS) {
+        int lo = 2 * t - (t & (stride - 1));
+        int hi = lo + stride;
+        bool up = ((lo & size) == 0);
+        SortItem a = sk[lo], b = sk[hi];
+        uint32_t ia = si[lo], ib = si[hi];
+        bool sw = up ? item_less(b, ib, a, ia) : item_less(a, ia, b, ib);
+        if (sw) {
+          sk[lo] = b; sk[hi] = a;
+          si[lo] = ib; si[hi] = ia;
+        }
+      }
+      __syncthreads();
+    }
+  }
+}
+
+// Per-CTA top-K. Rows are taken in rounds of THREADS; a row enters the
+// candidate buffer only if it beats the current K-th best, and the buffer is
+// merged (bitonic sort of best-K + candidates) whenever it could overflow.
+template <int B, int THREADS>
+__global__ void __launch_bounds__(THREADS) k_topk(const SortItem* __restrict__ keys, const uint32_t* __restrict__ idx,
+                                                  const uint64_t* count, uint64_t n_max, int K,
+                                                  SortItem* __restrict__ out_keys, uint32_t* __restrict__ out_idx,
+                                                  uint64_t* out_count, int final_pass) {
+  extern __shared__ __align__(16) uint8_t smem[];
+  SortItem* sk = (SortItem*)smem;
+  uint32_t* si = (uint32_t*)(sk + B);
+  __shared__ int s_n;         // entries in [0, B): [0, K) best so far, then candidates
+  __shared__ int s_have;      // best entries valid (<= K)
+  const uint64_t n = count ? *count : n_max;
+  const SortItem inf{{~0ULL, ~0ULL, ~0ULL, ~0ULL}};
+  if (threadIdx.x == 0) {
+    s_n = 0;
+    s_have = 0;
+  }
+  __syncthreads();
+  // Rows handled by this CTA: a contiguous range.
+  const uint64_t per = (n + gridDim.x - 1) / gridDim.x;
+  const uint64_t lo = (uint64_t)blockIdx.x * per;
+  uint64_t hi = lo + per;
+  if (hi > n) hi = n;
+  auto merge = [&]() {
+    // pad, sort, keep the first K
+    for (int i = s_n + threadIdx.x; i < B; i += THREADS) {
+      sk[i] = inf;
+      si[i] = 0xFFFFFFFFu;
+    }
+    __syncthreads();
+    bitonic_sort<B, THREADS>(sk, si);
+    if (threadIdx.x == 0) {
+      int valid = s_n < K ? s_n : K;
+      s_have = valid;
+      s_n = valid;
+    }
+    __syncthreads();
+  };
+  for (uint64_t base = lo; base < hi; base += THREADS) {
+    const uint64_t g = base + threadIdx.x;
+    if (g < hi) {
+      SortItem k = keys[g];
+      uint32_t ix = idx ? idx[g] : (uint32_t)g;
+      // 0xFFFFFFFF marks padding from the per-CTA pass.
+      bool take = ix != 0xFFFFFFFFu && (s_have < K || item_less(k, ix, sk[K - 1], si[K - 1]));
+      if (take) {
+        int p = atomicAdd(&s_n, 1);
+        sk[p] = k;
+        si[p] = ix;
+      }
+    }
+    __syncthreads();
+    if (s_n > B - THREADS) merge();
+  }
+  if (s_n > s_have || s_have < K) merge();
+  const int m = s_have;
+  if (final_pass) {
+    for (int i = threadIdx.x; i < m; i += THREADS) out_idx[i] = si[i];
+    if (threadIdx.x == 0) *out_count = (uint64_t)m;
+  } else {
+    for (int i = threadIdx.x; i < K; i += THREADS) {
+      out_keys[(uint64_t)blockIdx.x * K + i] = i < m ? sk[i] : inf;
+      out_idx[(uint64_t)blockIdx.x * K + i] = i < m ? si[i] : 0xFFFFFFFFu;
+    }
+  }
+}
+
+size_t topk_temp_bytes(uint64_t n_max, int k) {
+  uint64_t ctas = (uint64_t)sms();
+  const uint64_t want = (n_max + 4095) / 4096;
+  if (want < ctas) ctas = want ? want : 1;
+  return ctas * (uint64_t)k * (sizeof(SortItem) + sizeof(uint32_t)) + 256;
+}
+
+template <int B>
+static cudaError_t topk_b(const SortItem* keys, const uint32_t* idx, const uint64_t* count, uint64_t n_max, int k,
+                          uint32_t* out_idx, uint64_t* out_count, void* temp, cudaStream_t s) {
+  constexpr int T = 256;
+  const size_t smem = (size_t)B * (sizeof(SortItem) + sizeof(uint32_t));
+  auto k1 = k_topk<B, T>;
+  cudaError_t e = cudaFuncSetAttribute(k1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  unsigned ctas = (unsigned)sms();
+  uint64_t want = (n_max + 4095) / 4096;
+  if (want < ctas) ctas = (unsigned)(want ? want : 1);
+  SortItem* pk = (SortItem*)temp;
+  uint32_t* pi = (uint32_t*)(pk + (uint64_t)ctas * k);
+  k1<<<ctas, T, smem, s>>>(keys, idx, count, n_max, k, pk, pi, nullptr, 0);
+  // Second pass over the per-CTA winners; the padding entries sort last.
+  k1<<<1, T, smem, s>>>(pk, pi, nullptr, (uint64_t)ctas * k, k, nullptr, out_idx, out_count, 1);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_topk(const SortItem* keys, const uint32_t* idx, const uint64_t* count, uint64_t n_max, int k,
+                        uint32_t* out_idx, uint64_t* out_count, void* temp, uint32_t* status, cudaStream_t s) {
+  if (k <= 0 || k > 1024) return cudaErrorInvalidValue;
+  if (k <= 128) return topk_b<512>(keys, idx, count, n_max, k, out_idx, out_count, temp, s);
+  return topk_b<2048>(keys, idx, count, n_max, k, out_idx, out_count, temp, s);
+}
+
+}  // namespace mtl

@@ -1,0 +1,108 @@
+// kernels.h — host-callable launchers for the sm_100a kernels. All take a
+// stream and enqueue asynchronously; none synchronizes.
+#pragma once
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+
+#include "dev_types.h"
+
+namespace mtl {
+
+// ---- pipeline (k_pipeline.cu)
+size_t pipeline_tile_rows();
+size_t pipeline_smem_bytes(const PipeDesc& d);
+// n_hint bounds the tuples (grid sizing when the count lives on the device).
+cudaError_t launch_pipeline(const PipeDesc& d, uint64_t n_hint, cudaStream_t s);
+
+// ---- aggregate finalize (k_misc.cu)
+// Order-preserving list of READY slots of a hash aggregate table.
+cudaError_t launch_compact_ready(const uint32_t* state, uint64_t capacity, uint32_t* out_idx,
+                                 uint64_t* out_count, uint64_t* tile_status, uint32_t* tile_counter,
+                                 uint32_t epoch, uint32_t* status, cudaStream_t s);
+// Order-preserving list of indices i < n with flag[i] != 0 (u8 flags).
+cudaError_t launch_compact_flags(const uint8_t* flag, uint64_t n, const uint64_t* n_dev, uint32_t* out_idx,
+                                 uint64_t* out_count, uint64_t* tile_status, uint32_t* tile_counter,
+                                 uint32_t epoch, uint32_t* status, cudaStream_t s);
+size_t compact_tile_rows();
+
+// Gather one u64 state array / key array through an index list into a
+// dense array (out[i] = in[idx[i]]), for i < *count.
+cudaError_t launch_gather_u64(const uint64_t* in, const uint32_t* idx, const uint64_t* count, uint64_t n_max,
+                              uint64_t* out, cudaStream_t s);
+cudaError_t launch_gather_u32(const uint32_t* in, const uint32_t* idx, const uint64_t* count, uint64_t n_max,
+                              uint32_t* out, cudaStream_t s);
+
+// Final aggregate outputs. kind: see FinalKind in k_misc.cu.
+enum FinalKind : int32_t {
+  F_COPY_I32 = 1,   // low 32 bits of a u64 state/key word
+  F_COPY_I64 = 2,
+  F_COPY_F32 = 3,   // key word holding f32 bits
+  F_COPY_F64 = 4,
+  F_SUM_I128 = 5,   // (lo, hi) -> i128
+  F_SUM_I64_AS_I128 = 6,
+  F_MINMAX_F32 = 7,  // ordered image -> f32
+  F_MINMAX_F64 = 8,  // ordered image -> f64
+  F_AVG_I128_LD = 9,  // (long double)sum / count -> double (DuckDB BIGINT AVG)
+  F_AVG_I64_D = 10,   // (double)sum / (double)count (DuckDB INTEGER AVG)
+  F_AVG_F64 = 11,     // double sum / count
+  F_AVG_DEC = 12,     // decimal: (long double)sum / count / 10^scale
+  F_GATHER_COL = 13,  // out[i] = col[rid[g]] (group key of a representative row), width 4/8
+};
+struct FinalOut {
+  int32_t kind;
+  int32_t width;         // F_GATHER_COL element width
+  const uint64_t* a;     // state or key words, indexed by group g
+  const int64_t* a_hi;   // high words
+  const uint64_t* cnt;   // counts (AVG)
+  void* out;
+  double scale;          // AVG of DECIMAL: 10^scale
+  const void* col;       // F_GATHER_COL column
+  const uint32_t* rid;   // F_GATHER_COL row id per group
+};
+// For i < *count (or n_max): g = idx ? idx[i] : i; writes out[i] per FinalOut.
+cudaError_t launch_finalize(const FinalOut* outs, int n_outs, const uint32_t* idx, const uint64_t* count,
+                            uint64_t n_max, cudaStream_t s);
+
+// ---- order by / top-K (k_sort.cu)
+// Encodes ORDER BY keys of rows [0, *count) into 32-byte order-preserving
+// images (most significant word first) plus a row index.
+struct SortItem {
+  uint64_t w[4];
+};
+cudaError_t launch_encode_keys(const SortKeySpec& spec, const uint64_t* count, uint64_t n_max, SortItem* keys,
+                               uint32_t* idx, cudaStream_t s);
+// Stable LSD radix sort of (keys, idx) on the given number of significant
+// key bytes (from the least significant), count on the device.
+size_t radix_sort_temp_bytes(uint64_t n_max);
+cudaError_t launch_radix_sort(SortItem* keys, uint32_t* idx, SortItem* keys_tmp, uint32_t* idx_tmp,
+                              const uint64_t* count, uint64_t n_max, int key_bytes, void* temp,
+                              cudaStream_t s, int* result_in_tmp);
+// Top-K of (keys, idx): smallest K images first. Writes K (or fewer) indices.
+size_t topk_temp_bytes(uint64_t n_max, int k);
+cudaError_t launch_topk(const SortItem* keys, const uint32_t* idx, const uint64_t* count, uint64_t n_max, int k,
+                        uint32_t* out_idx, uint64_t* out_count, void* temp, uint32_t* status, cudaStream_t s);
+
+// ---- gathers for final materialization (k_misc.cu)
+// out[i] = in[idx[i]] for fixed width elements (4, 8 or 16 bytes).
+cudaError_t launch_gather_width(const void* in, int width, const uint32_t* idx, const uint64_t* count,
+                                uint64_t n_max, void* out, cudaStream_t s);
+
+// ---- scalar hooks (k_misc.cu): gpu_{add,mul}_scalar, gpu_{eq,lt,le,gt,ge}_scalar
+cudaError_t launch_scalar_arith(int op, int ptype, const void* in, uint64_t n, int64_t ilit, double flit, void* out,
+                                uint32_t* status, cudaStream_t s);
+cudaError_t launch_scalar_compare(int op, int ptype, const void* in, uint64_t n, int64_t ilit, double flit,
+                                  uint8_t* out, cudaStream_t s);
+
+// ---- column statistics (k_misc.cu)
+// min/max of an integer-like column as i64 (out[0] = min, out[1] = max).
+cudaError_t launch_minmax_i(const void* col, int ptype, uint64_t n, int64_t* out, cudaStream_t s);
+// Counts keys that occur more than once by inserting into an open-addressing
+// table of `cap` i64 slots (all bits set = empty); out[0] = duplicates.
+cudaError_t launch_count_dups(const void* col, int ptype, uint64_t n, int64_t* table, uint64_t cap,
+                              uint32_t* special, unsigned long long* out, cudaStream_t s);
+
+// ---- utility
+cudaError_t launch_fill_u64(uint64_t* p, uint64_t n, uint64_t v, cudaStream_t s);
+
+}  // namespace mtl

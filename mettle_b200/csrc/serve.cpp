@@ -1,0 +1,324 @@
+// serve.cpp — the serving loop behind gpu_processing.
+//
+// The reference executes one query at a time at DuckDB bind time with
+// set_max_threads(1) (src/processing.rs:59-75). Here requests are queued and
+// run by `slots` workers, each with its own CUDA stream, so requests that
+// arrive while others are on the GPU overlap on the device. A request is
+// admitted when its device scratch fits in the processing region next to
+// the requests already running (its compile step allocates from the region
+// arena; on a shortfall it waits for running requests to release memory, and
+// is rejected only if it cannot fit even alone). Small requests (root table
+// at most kSmallRows rows) that are queued together are compiled together
+// and launched as one captured CUDA graph, which removes the per-kernel
+// launch cost that dominates small queries.
+#include <chrono>
+#include <cstring>
+
+#include "engine.h"
+
+namespace mtl {
+
+constexpr uint64_t kSmallRows = 1ull << 20;
+constexpr int kBatchMax = 16;
+
+struct Request {
+  std::string sql;
+  std::mutex mu;
+  std::condition_variable cv;
+  bool done = false;
+  int status = MTL_OK;
+  std::string err;
+  std::shared_ptr<Result> result;
+  std::chrono::steady_clock::time_point t_submit, t_done;
+  bool small = false;
+  // compiled state while running
+  BoundPlan plan;
+  std::unique_ptr<Program> prog;
+};
+
+struct ServeState {
+  std::mutex mu;
+  std::condition_variable cv;       // queue and memory
+  std::deque<Request*> queue;
+  std::vector<std::thread> workers;
+  std::vector<cudaStream_t> streams;
+  bool stop = false;
+  int slots = 4;
+  std::atomic<int64_t> submitted{0}, completed{0}, rejected{0}, in_flight{0}, admitted_bytes{0}, batched{0};
+};
+
+static void finish(ServeState& S, Request* r, int status, const std::string& err) {
+  {
+    std::lock_guard<std::mutex> g(r->mu);
+    r->status = status;
+    r->err = err;
+    r->done = true;
+    r->t_done = std::chrono::steady_clock::now();
+  }
+  r->cv.notify_all();
+  S.completed++;
+  if (status == MTL_BUDGET_EXCEEDED) S.rejected++;
+}
+
+// Binds and compiles; waits for memory when other requests hold it.
+// Returns false (request finished) on error.
+static bool prepare(Ctx& ctx, ServeState& S, Request* r) {
+  try {
+    SelectStmt st;
+    try {
+      st = parse_sql(r->sql);
+    } catch (const SqlError& e) {
+      fail(MTL_UNSUPPORTED, std::string("SQL outside the offloaded subset: ") + e.what());
+    }
+    r->plan = bind_select(ctx, st);
+    if (r->plan.constant_only) {
+      r->result = constant_result(r->plan);
+      finish(S, r, MTL_OK, "");
+      return false;
+    }
+    for (;;) {
+      try {
+        r->prog = compile(ctx, r->plan);
+        S.admitted_bytes += (int64_t)r->prog->scratch_bytes;
+        return true;
+      } catch (const EngineError& e) {
+        if (e.code != MTL_BUDGET_EXCEEDED) throw;
+        std::unique_lock<std::mutex> lk(S.mu);
+        // Only this request holds no memory: it can never fit.
+        if (S.admitted_bytes.load() == 0) throw;
+        S.cv.wait_for(lk, std::chrono::milliseconds(20));
+        if (S.stop) throw;
+      }
+    }
+  } catch (const EngineError& e) {
+    finish(S, r, e.code, e.what());
+  } catch (const std::exception& e) {
+    finish(S, r, MTL_DEVICE_ERROR, e.what());
+  }
+  return false;
+}
+
+static void release(Ctx& ctx, ServeState& S, Request* r) {
+  if (r->prog) {
+    S.admitted_bytes -= (int64_t)r->prog->scratch_bytes;
+    free_program(ctx, *r->prog);
+    r->prog.reset();
+  }
+  S.cv.notify_all();
+}
+
+static void run_batch(Ctx& ctx, ServeState& S, std::vector<Request*>& batch, cudaStream_t s) {
+  std::vector<Request*> ready;
+  for (Request* r : batch)
+    if (prepare(ctx, S, r)) ready.push_back(r);
+  if (ready.empty()) return;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  bool graphed = false;
+  try {
+    if (ready.size() > 1) {
+      // One captured graph for the whole batch.
+      cudaGraph_t graph = nullptr;
+      cudaGraphExec_t exec = nullptr;
+      if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+        bool ok = true;
+        try {
+          for (Request* r : ready) run_program(ctx, *r->prog, s);
+        } catch (...) {
+          ok = false;
+        }
+        if (cudaStreamEndCapture(s, &graph) != cudaSuccess) ok = false;
+        if (ok && cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess) {
+          cudaEventRecord(e0, s);
+          if (cudaGraphLaunch(exec, s) == cudaSuccess) graphed = true;
+          cudaEventRecord(e1, s);
+        }
+        cudaGetLastError();
+        if (graph) cudaGraphDestroy(graph);
+        if (exec) {
+          cudaStreamSynchronize(s);
+          cudaGraphExecDestroy(exec);
+        }
+      } else {
+        cudaGetLastError();
+      }
+      if (graphed) S.batched++;
+    }
+    if (!graphed) {
+      cudaEventRecord(e0, s);
+      for (Request* r : ready) run_program(ctx, *r->prog, s);
+      cudaEventRecord(e1, s);
+    }
+  } catch (const EngineError& e) {
+    cudaStreamSynchronize(s);
+    for (Request* r : ready) {
+      release(ctx, S, r);
+      finish(S, r, e.code, e.what());
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return;
+  }
+  float ms = 0;
+  for (Request* r : ready) {
+    try {
+      r->result = fetch_program(ctx, *r->prog, s);
+      if (ms == 0) {
+        cudaEventElapsedTime(&ms, e0, e1);
+      }
+      r->result->device_ms = ms / (float)ready.size();
+      release(ctx, S, r);
+      finish(S, r, MTL_OK, "");
+    } catch (const EngineError& e) {
+      release(ctx, S, r);
+      finish(S, r, e.code, e.what());
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+}
+
+static void worker(Ctx* ctx, ServeState* S, int slot) {
+  cudaSetDevice(ctx->device);
+  cudaStream_t s = S->streams[slot];
+  for (;;) {
+    std::vector<Request*> batch;
+    {
+      std::unique_lock<std::mutex> lk(S->mu);
+      S->cv.wait(lk, [&] { return S->stop || !S->queue.empty(); });
+      if (S->stop && S->queue.empty()) return;
+      Request* r = S->queue.front();
+      S->queue.pop_front();
+      batch.push_back(r);
+      if (r->small) {
+        while (!S->queue.empty() && (int)batch.size() < kBatchMax && S->queue.front()->small) {
+          batch.push_back(S->queue.front());
+          S->queue.pop_front();
+        }
+      }
+    }
+    S->in_flight += (int64_t)batch.size();
+    run_batch(*ctx, *S, batch, s);
+    S->in_flight -= (int64_t)batch.size();
+  }
+}
+
+void serve_init(Ctx& ctx) {
+  std::lock_guard<std::recursive_mutex> g(ctx.mu);
+  if (ctx.serve) return;
+  ctx.serve = new ServeState();
+  ServeState& S = *ctx.serve;
+  S.streams.resize(S.slots);
+  for (int i = 0; i < S.slots; ++i) cudaStreamCreateWithFlags(&S.streams[i], cudaStreamNonBlocking);
+  for (int i = 0; i < S.slots; ++i) S.workers.emplace_back(worker, &ctx, &S, i);
+}
+
+void serve_shutdown(Ctx& ctx) {
+  if (!ctx.serve) return;
+  ServeState& S = *ctx.serve;
+  {
+    std::lock_guard<std::mutex> g(S.mu);
+    S.stop = true;
+  }
+  S.cv.notify_all();
+  for (auto& t : S.workers) t.join();
+  for (cudaStream_t s : S.streams) cudaStreamDestroy(s);
+  delete ctx.serve;
+  ctx.serve = nullptr;
+}
+
+static bool is_small(Ctx& ctx, const std::string& sql) {
+  try {
+    SelectStmt st = parse_sql(sql);
+    std::lock_guard<std::recursive_mutex> g(ctx.mu);
+    uint64_t rows = 0;
+    for (auto& f : st.from) {
+      auto it = ctx.tables.find(f.name);
+      if (it != ctx.tables.end()) rows = std::max(rows, it->second->rows);
+    }
+    for (auto& js : st.joins)
+      for (auto& j : js) {
+        auto it = ctx.tables.find(j.right.name);
+        if (it != ctx.tables.end()) rows = std::max(rows, it->second->rows);
+      }
+    return rows <= kSmallRows;
+  } catch (...) {
+    return false;
+  }
+}
+
+Request* serve_submit(Ctx& ctx, const std::string& sql) {
+  serve_init(ctx);
+  ServeState& S = *ctx.serve;
+  Request* r = new Request();
+  r->sql = sql;
+  r->t_submit = std::chrono::steady_clock::now();
+  r->small = is_small(ctx, sql);
+  S.submitted++;
+  {
+    std::lock_guard<std::mutex> g(S.mu);
+    S.queue.push_back(r);
+  }
+  S.cv.notify_all();
+  return r;
+}
+
+// ------------------------------------------------------------ C ABI helpers
+int serve_wait(Request* r, int64_t timeout_ns, std::shared_ptr<Result>* out, std::string* err) {
+  std::unique_lock<std::mutex> lk(r->mu);
+  if (timeout_ns < 0) {
+    r->cv.wait(lk, [&] { return r->done; });
+  } else if (!r->cv.wait_for(lk, std::chrono::nanoseconds(timeout_ns), [&] { return r->done; })) {
+    *err = "request did not finish within the timeout";
+    return MTL_TIMEOUT;
+  }
+  *err = r->err;
+  if (r->status == MTL_OK) *out = r->result;
+  return r->status;
+}
+
+double serve_latency_ms(Request* r) {
+  std::lock_guard<std::mutex> g(r->mu);
+  if (!r->done) return -1.0;
+  return std::chrono::duration<double, std::milli>(r->t_done - r->t_submit).count();
+}
+
+void serve_free(Request* r) {
+  {
+    std::unique_lock<std::mutex> lk(r->mu);
+    r->cv.wait(lk, [&] { return r->done; });
+  }
+  delete r;
+}
+
+void serve_stats(Ctx& ctx, mtl_serve_stats* out) {
+  memset(out, 0, sizeof(*out));
+  if (!ctx.serve) return;
+  ServeState& S = *ctx.serve;
+  out->submitted = S.submitted;
+  out->completed = S.completed;
+  out->rejected = S.rejected;
+  out->in_flight = S.in_flight;
+  {
+    std::lock_guard<std::mutex> g(S.mu);
+    out->queued = (int64_t)S.queue.size();
+  }
+  out->admitted_bytes = S.admitted_bytes;
+  out->batched_launches = S.batched;
+}
+
+int serve_set_slots(Ctx& ctx, int slots) {
+  if (slots < 1 || slots > 64) return MTL_INVALID;
+  serve_shutdown(ctx);
+  std::lock_guard<std::recursive_mutex> g(ctx.mu);
+  ctx.serve = new ServeState();
+  ServeState& S = *ctx.serve;
+  S.slots = slots;
+  S.streams.resize(slots);
+  for (int i = 0; i < slots; ++i) cudaStreamCreateWithFlags(&S.streams[i], cudaStreamNonBlocking);
+  for (int i = 0; i < slots; ++i) S.workers.emplace_back(worker, &ctx, &S, i);
+  return MTL_OK;
+}
+
+}  // namespace mtl

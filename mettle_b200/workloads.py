@@ -1,0 +1,185 @@
+"""Seeded synthetic workloads with the shapes of the benchmark configurations.
+
+The reference benchmarks on TPC-H data produced by DuckDB's dbgen
+(test/generate_tpch.py); neither DuckDB nor the network is available, so
+these generators stand in, with the table shapes, sizes and value
+distributions of the five configurations (numpy PCG64, fixed seeds):
+
+* ``numbers``   — one INTEGER column uniform in [0, 10^6) (the plain small query);
+* ``scan``      — a INTEGER U[0, 2^31), b BIGINT U[-2^62, 2^62), c FLOAT U[0,1),
+                  d DATE and e TIMESTAMP uniform over seven years (filter scan);
+* ``groupby``   — k BIGINT with G distinct keys, uniform or Zipf(s), key ids
+                  hashed over int64; v BIGINT U[0, 10^6); f FLOAT U[0,1);
+* ``q3``        — customer / orders / lineitem of the join -> filter -> group
+                  -> top-K pipeline, DECIMAL(15,2) money as int64 cents.
+"""
+from __future__ import annotations
+
+import datetime as _dt
+from dataclasses import dataclass
+
+import numpy as np
+
+SEED_BASE = 0x4D45_54544C45
+DAY0 = (_dt.date(1992, 1, 1) - _dt.date(1970, 1, 1)).days  # 1992-01-01 as days since epoch
+SPAN_DAYS = (_dt.date(1999, 1, 1) - _dt.date(1992, 1, 1)).days  # seven years = 2557 days
+SEGMENTS = ["AUTOMOBILE", "BUILDING", "FURNITURE", "HOUSEHOLD", "MACHINERY"]  # sorted: code 1 = BUILDING
+
+
+def rng(config: int, salt: int = 0) -> np.random.Generator:
+    return np.random.Generator(np.random.PCG64(SEED_BASE + config + 1000 * salt))
+
+
+def day_to_iso(days: int) -> str:
+    return (_dt.date(1970, 1, 1) + _dt.timedelta(days=int(days))).isoformat()
+
+
+# ------------------------------------------------------------------ config 1
+def numbers(n: int = 1_000_000, seed_salt: int = 0) -> dict[str, np.ndarray]:
+    r = rng(1, seed_salt)
+    return {"value": r.integers(0, 1_000_000, n, dtype=np.int32)}
+
+
+C1_SQL = "SELECT value, value * 10 AS scaled FROM numbers WHERE value > 500000 ORDER BY value"
+
+
+# ------------------------------------------------------------------ config 2
+def scan(n: int = 100_000_000, seed_salt: int = 0) -> dict[str, np.ndarray]:
+    r = rng(2, seed_salt)
+    us_day = 86_400_000_000
+    return {
+        "a": r.integers(0, 2**31, n, dtype=np.int64).astype(np.int32),
+        "b": r.integers(-(2**62), 2**62, n, dtype=np.int64),
+        "c": r.random(n, dtype=np.float32),
+        "d": (DAY0 + r.integers(0, SPAN_DAYS, n, dtype=np.int32)).astype(np.int32),
+        "e": DAY0 * us_day + r.integers(0, SPAN_DAYS * us_day, n, dtype=np.int64),
+    }
+
+
+def scan_literal(col: str, sel: float) -> str:
+    """Literal k so that `col < k` keeps about `sel` of the rows."""
+    if col == "a":
+        return str(int(sel * 2**31))
+    if col == "b":
+        return str(int(-(2**62) + sel * 2**63))
+    if col == "c":
+        return repr(float(sel))
+    if col == "d":
+        return f"DATE '{day_to_iso(DAY0 + int(sel * SPAN_DAYS))}'"
+    if col == "e":
+        us = int(sel * SPAN_DAYS * 86_400_000_000)
+        t = _dt.datetime(1992, 1, 1) + _dt.timedelta(microseconds=us)
+        return f"TIMESTAMP '{t.strftime('%Y-%m-%d %H:%M:%S')}'"
+    raise ValueError(col)
+
+
+def scan_sql(col: str = "a", op: str = "<", sel: float = 0.5) -> str:
+    """Filter/projection template: SELECT a, b + 5, c * 10, d, e FROM t WHERE <col> <op> <k>."""
+    lit = scan_literal(col, sel if op in ("<", "<=") else 1.0 - sel)
+    return f"SELECT a, b + 5 AS b5, c * 10 AS c10, d, e FROM t WHERE {col} {op} {lit}"
+
+
+# ------------------------------------------------------------------ config 3
+def _mix64(x: np.ndarray) -> np.ndarray:
+    x = x.astype(np.uint64)
+    x ^= x >> np.uint64(33)
+    x *= np.uint64(0xFF51AFD7ED558CCD)
+    x ^= x >> np.uint64(33)
+    x *= np.uint64(0xC4CEB9FE1A85EC53)
+    x ^= x >> np.uint64(33)
+    return x.view(np.int64)
+
+
+def groupby(n: int = 200_000_000, groups: int = 1000, dist: str = "uniform", s: float = 1.1,
+            seed_salt: int = 0) -> dict[str, np.ndarray]:
+    r = rng(3, seed_salt)
+    if dist == "uniform":
+        ids = r.integers(0, groups, n, dtype=np.int64)
+    elif dist == "zipf":
+        # exact bounded Zipf(s) over `groups` ranks: multinomial counts, then a shuffle
+        w = 1.0 / np.power(np.arange(1, groups + 1, dtype=np.float64), s)
+        counts = r.multinomial(n, w / w.sum())
+        ids = np.repeat(np.arange(groups, dtype=np.int64), counts)
+        r.shuffle(ids)
+    else:
+        raise ValueError(dist)
+    return {
+        "k": _mix64(ids),
+        "v": r.integers(0, 1_000_000, n, dtype=np.int64),
+        "f": r.random(n, dtype=np.float32),
+    }
+
+
+C3_SQL = ("SELECT k, SUM(v) AS sum_v, COUNT(*) AS cnt, MIN(v) AS min_v, MAX(v) AS max_v, AVG(v) AS avg_v, "
+          "SUM(f) AS sum_f, MIN(f) AS min_f, MAX(f) AS max_f, AVG(f) AS avg_f FROM t GROUP BY k "
+          "ORDER BY sum_v DESC, k LIMIT 100")
+
+
+# ------------------------------------------------------------------ config 4
+@dataclass
+class Q3Tables:
+    customer: dict
+    orders: dict
+    lineitem: dict
+    date: int
+
+    @property
+    def lineitem_rows(self) -> int:
+        return len(self.lineitem["l_orderkey"])
+
+
+def q3(n_cust: int = 1_500_000, n_ord: int = 15_000_000, seed_salt: int = 0) -> Q3Tables:
+    r = rng(4, seed_salt)
+    customer = {
+        "c_custkey": np.arange(1, n_cust + 1, dtype=np.int32),
+        "c_mktsegment": r.integers(0, len(SEGMENTS), n_cust, dtype=np.int32),
+    }
+    orderdate = (DAY0 + r.integers(0, SPAN_DAYS, n_ord, dtype=np.int32)).astype(np.int32)
+    orders = {
+        "o_orderkey": np.arange(1, n_ord + 1, dtype=np.int32),
+        "o_custkey": r.integers(1, n_cust + 1, n_ord, dtype=np.int32),
+        "o_orderdate": orderdate,
+        "o_shippriority": np.zeros(n_ord, dtype=np.int32),
+    }
+    lines = r.integers(1, 8, n_ord, dtype=np.int32)  # 1..7 lines per order, drawn first
+    n_li = int(lines.sum())
+    li_order = np.repeat(np.arange(n_ord, dtype=np.int64), lines)
+    lineitem = {
+        "l_orderkey": orders["o_orderkey"][li_order],
+        "l_extendedprice": r.integers(90_000, 10_500_001, n_li, dtype=np.int64),
+        "l_discount": r.integers(0, 11, n_li, dtype=np.int64),
+        "l_shipdate": (orderdate[li_order] + r.integers(1, 122, n_li, dtype=np.int32)).astype(np.int32),
+    }
+    return Q3Tables(customer, orders, lineitem, DAY0 + SPAN_DAYS // 2)
+
+
+def q3_sql(date: int, segment: str = "BUILDING", limit: int = 10) -> str:
+    d = day_to_iso(date)
+    return ("SELECT l_orderkey, SUM(l_extendedprice * (1 - l_discount)) AS revenue, o_orderdate, o_shippriority "
+            "FROM customer, orders, lineitem "
+            f"WHERE c_mktsegment = '{segment}' AND c_custkey = o_custkey AND l_orderkey = o_orderkey "
+            f"AND o_orderdate < DATE '{d}' AND l_shipdate > DATE '{d}' "
+            "GROUP BY l_orderkey, o_orderdate, o_shippriority "
+            f"ORDER BY revenue DESC, o_orderdate LIMIT {limit}")
+
+
+def q3_bytes(t: Q3Tables) -> int:
+    """Algorithmic bytes of one config-4 query: every column the query names, read once."""
+    return (len(t.customer["c_custkey"]) * (4 + 4) + len(t.orders["o_orderkey"]) * (4 + 4 + 4 + 4)
+            + t.lineitem_rows * (4 + 8 + 8 + 4))
+
+
+def register_q3(conn, t: Q3Tables, upload: bool = True, borrow: bool = False):
+    from . import _lib as L
+    conn.create_table("customer", {"c_custkey": (L.T_INTEGER, t.customer["c_custkey"]),
+                                   "c_mktsegment": (L.T_VARCHAR, t.customer["c_mktsegment"], SEGMENTS)})
+    conn.create_table("orders", {"o_orderkey": (L.T_INTEGER, t.orders["o_orderkey"]),
+                                 "o_custkey": (L.T_INTEGER, t.orders["o_custkey"]),
+                                 "o_orderdate": (L.T_DATE, t.orders["o_orderdate"]),
+                                 "o_shippriority": (L.T_INTEGER, t.orders["o_shippriority"])})
+    conn.create_table("lineitem", {"l_orderkey": (L.T_INTEGER, t.lineitem["l_orderkey"]),
+                                   "l_extendedprice": (L.T_DECIMAL, t.lineitem["l_extendedprice"], 2),
+                                   "l_discount": (L.T_DECIMAL, t.lineitem["l_discount"], 2),
+                                   "l_shipdate": (L.T_DATE, t.lineitem["l_shipdate"])})
+    for name in ("customer", "orders", "lineitem"):
+        conn.gpu_register_table(name, upload=upload, borrow=borrow)

@@ -1,0 +1,233 @@
+"""Parity of the GPU path with the CPU oracle on the benchmark workloads
+through the C ABI. Integer, DECIMAL, DATE and
+TIMESTAMP results must be bit-exact; FLOAT aggregates within 1e-6 relative
+of an extended-precision sum."""
+import numpy as np
+import pytest
+
+import oracle as orc
+from mettle_b200 import MettleError
+from mettle_b200 import _lib as L
+from mettle_b200 import workloads as W
+
+FLOAT_RTOL = 1e-6
+
+
+def init(conn, cache="8 GB", processing="8 GB"):
+    conn.execute(f"CALL gpu_buffer_init('{cache}', '{processing}')")
+
+
+# ------------------------------------------------------------------ config 1
+@pytest.mark.gpu
+@pytest.mark.parametrize("n", [0, 1, 1000, 1_000_000])
+def test_c1_plain_small_query(conn, oracle_lib, n):
+    init(conn)
+    d = W.numbers(n)
+    conn.create_table("numbers", {"value": (L.T_INTEGER, d["value"])})
+    conn.gpu_register_table("numbers")
+    r = conn.gpu_processing(W.C1_SQL)
+    rows = orc.filter_rows([(d["value"], ">", 500000)])
+    rows = orc.sort_rows(d["value"], rows)
+    want_v = orc.gather(d["value"], rows)
+    want_s = orc.gather(d["value"], rows, "*", 10)
+    assert r.names == ["value", "scaled"]
+    assert np.array_equal(r.columns[0], want_v)
+    assert np.array_equal(r.columns[1], want_s)
+
+
+# ------------------------------------------------------------------ config 2
+def scan_expect(d, col, op, lit_value):
+    rows = orc.filter_rows([(d[col], op, lit_value)])
+    return {
+        "a": orc.gather(d["a"], rows), "b5": orc.gather(d["b"], rows, "+", 5),
+        "c10": orc.gather(d["c"], rows, "*", np.float32(10)), "d": orc.gather(d["d"], rows),
+        "e": orc.gather(d["e"], rows),
+    }
+
+
+def literal_value(col, sel):
+    if col == "a":
+        return int(sel * 2**31)
+    if col == "b":
+        return int(-(2**62) + sel * 2**63)
+    if col == "c":
+        return float(sel)
+    if col == "d":
+        return W.DAY0 + int(sel * W.SPAN_DAYS)
+    us = int(sel * W.SPAN_DAYS * 86_400_000_000)
+    return W.DAY0 * 86_400_000_000 + (us // 1_000_000) * 1_000_000
+
+
+@pytest.fixture(scope="module")
+def scan_conn(built_lib):
+    from mettle_b200 import Connection
+    c = Connection()
+    init(c)
+    d = W.scan(2_000_000)
+    c.create_table("t", {"a": (L.T_INTEGER, d["a"]), "b": (L.T_BIGINT, d["b"]), "c": (L.T_FLOAT, d["c"]),
+                         "d": (L.T_DATE, d["d"]), "e": (L.T_TIMESTAMP, d["e"])})
+    c.gpu_register_table("t", upload=True)
+    yield c, d
+    c.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("col", ["a", "b", "c", "d", "e"])
+@pytest.mark.parametrize("op", ["=", "<", "<=", ">", ">="])
+@pytest.mark.parametrize("sel", [0.01, 0.1, 0.5])
+def test_c2_filter_projection(scan_conn, col, op, sel):
+    conn, d = scan_conn
+    s = sel if op in ("<", "<=") else 1.0 - sel
+    if op == "=":
+        # equality: a value that occurs in the column
+        v = d[col][12345]
+        lit = {"a": str(int(v)), "b": str(int(v)), "c": repr(float(v)),
+               "d": f"DATE '{W.day_to_iso(int(v))}'"}.get(col)
+        if col == "e":
+            import datetime as dt
+            t = dt.datetime(1970, 1, 1) + dt.timedelta(microseconds=int(v))
+            lit = f"TIMESTAMP '{t.strftime('%Y-%m-%d %H:%M:%S.%f')}'"
+        value = v.item()
+    else:
+        lit = W.scan_literal(col, s)
+        value = literal_value(col, s)
+    sql = f"SELECT a, b + 5 AS b5, c * 10 AS c10, d, e FROM t WHERE {col} {op} {lit}"
+    r = conn.gpu_processing(sql)
+    want = scan_expect(d, col, op, value)
+    assert r.rows == len(want["a"])
+    for i, name in enumerate(["a", "b5", "c10", "d", "e"]):
+        assert np.array_equal(r.columns[i], want[name]), (sql, name)
+
+
+@pytest.mark.gpu
+def test_c2_multi_predicate_and_empty(scan_conn):
+    conn, d = scan_conn
+    r = conn.gpu_processing("SELECT a, d FROM t WHERE a < 1000000000 AND d >= DATE '1995-01-01' AND c < 0.25")
+    rows = orc.filter_rows([(d["a"], "<", 1_000_000_000), (d["d"], ">=", W.day_to_iso and
+                            (np.datetime64('1995-01-01') - np.datetime64('1970-01-01')).astype(int)),
+                            (d["c"], "<", 0.25)])
+    assert np.array_equal(r.columns[0], d["a"][rows])
+    r = conn.gpu_processing("SELECT a FROM t WHERE a < 0")
+    assert r.rows == 0
+
+
+# ------------------------------------------------------------------ config 3
+@pytest.mark.gpu
+@pytest.mark.parametrize("groups,dist", [(1000, "uniform"), (1000, "zipf"), (100_000, "uniform"),
+                                         (100_000, "zipf"), (1_500_000, "uniform")])
+def test_c3_groupby_topk(conn, groups, dist):
+    init(conn)
+    d = W.groupby(n=3_000_000, groups=groups, dist=dist, seed_salt=groups)
+    conn.create_table("t", {"k": (L.T_BIGINT, d["k"]), "v": (L.T_BIGINT, d["v"]), "f": (L.T_FLOAT, d["f"])})
+    conn.gpu_register_table("t")
+    r = conn.gpu_processing(W.C3_SQL)
+    want = orc.groupby_c3(d["k"], d["v"], d["f"], limit=100)
+    rows = r.fetchall()
+    assert len(rows) == len(want["k"])
+    for i, row in enumerate(rows):
+        k, sum_v, cnt, min_v, max_v, avg_v, sum_f, min_f, max_f, avg_f = row
+        assert k == want["k"][i]
+        assert sum_v == want["sum_v"][i]
+        assert cnt == want["cnt"][i] and min_v == want["min_v"][i] and max_v == want["max_v"][i]
+        assert avg_v == want["avg_v"][i]  # exact: DuckDB's extended-precision quotient
+        assert abs(sum_f - want["sum_f"][i]) <= FLOAT_RTOL * abs(want["sum_f"][i])
+        assert np.float32(min_f) == want["min_f"][i] and np.float32(max_f) == want["max_f"][i]
+        assert abs(avg_f - want["avg_f"][i]) <= FLOAT_RTOL * abs(want["avg_f"][i])
+
+
+@pytest.mark.gpu
+def test_c3_all_groups_exact(conn):
+    init(conn)
+    d = W.groupby(n=500_000, groups=5000, dist="zipf", seed_salt=9)
+    conn.create_table("t", {"k": (L.T_BIGINT, d["k"]), "v": (L.T_BIGINT, d["v"]), "f": (L.T_FLOAT, d["f"])})
+    conn.gpu_register_table("t")
+    r = conn.gpu_processing("SELECT k, SUM(v), COUNT(*), MIN(v), MAX(v) FROM t GROUP BY k ORDER BY k")
+    want = orc.groupby_c3(d["k"], d["v"], d["f"], limit=-1)
+    assert r.rows == want["groups"]
+    assert np.array_equal(r.columns[0], want["k"])
+    assert [int(x[0]) for x in r.columns[1]] == [int(s) for s in want["sum_v"]]
+    assert np.array_equal(r.columns[2], want["cnt"])
+    assert np.array_equal(r.columns[3], want["min_v"]) and np.array_equal(r.columns[4], want["max_v"])
+
+
+# ------------------------------------------------------------------ config 4
+def q3_check(conn, t, limit=10):
+    r = conn.gpu_processing(W.q3_sql(t.date, limit=limit))
+    want = orc.q3(t, segment_code=1, limit=limit)
+    rows = r.fetchall()
+    assert len(rows) == len(want["key"])
+    for i, (k, rev, date, prio) in enumerate(rows):
+        assert k == want["key"][i]
+        assert int(rev.scaleb(4)) == want["revenue"][i]  # DECIMAL(38,4), exact
+        assert (date - __import__("datetime").date(1970, 1, 1)).days == want["date"][i]
+        assert prio == want["prio"][i]
+    return r
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("scale", [0.001, 0.01])
+def test_c4_pipeline_small(conn, scale):
+    init(conn)
+    t = W.q3(n_cust=int(1_500_000 * scale), n_ord=int(15_000_000 * scale), seed_salt=int(scale * 1000))
+    W.register_q3(conn, t)
+    q3_check(conn, t, limit=10)
+    q3_check(conn, t, limit=1000)
+
+
+@pytest.mark.gpu
+def test_c4_pipeline_full_size(conn):
+    init(conn, "16 GB", "16 GB")
+    t = W.q3()
+    W.register_q3(conn, t, upload=True)
+    q3_check(conn, t, limit=10)
+
+
+@pytest.mark.gpu
+def test_prepared_statement_replays(conn):
+    init(conn)
+    t = W.q3(n_cust=15000, n_ord=150000, seed_salt=3)
+    W.register_q3(conn, t)
+    st = conn.prepare(W.q3_sql(t.date))
+    assert st.kernel_count() >= 3
+    outs = []
+    for _ in range(3):
+        st.launch()
+        outs.append(st.fetch().fetchall())
+    assert outs[0] == outs[1] == outs[2]
+    assert outs[0] == conn.gpu_processing(W.q3_sql(t.date)).fetchall()
+    st.close()
+
+
+# ------------------------------------------------------------------ errors
+@pytest.mark.gpu
+def test_integer_overflow_is_an_error(conn):
+    init(conn)
+    conn.create_table("n", {"x": (L.T_INTEGER, np.array([1, 2, 2_000_000_000], np.int32))})
+    conn.gpu_register_table("n")
+    with pytest.raises(MettleError) as e:
+        conn.gpu_processing("SELECT x * 10 FROM n")
+    assert e.value.code == L.OVERFLOW
+    assert conn.gpu_processing("SELECT x * 10 FROM n WHERE x < 10").fetchall() == [(10,), (20,)]
+
+
+@pytest.mark.gpu
+def test_unsupported_shapes(conn):
+    init(conn)
+    conn.create_table("n", {"x": (L.T_INTEGER, np.arange(10, dtype=np.int32))})
+    conn.gpu_register_table("n")
+    for sql in ["SELECT x FROM n WHERE x > 1 OR x < 0", "SELECT DISTINCT x FROM n",
+                "SELECT x FROM n WHERE x IN (1, 2)", "WITH a AS (SELECT x FROM n) SELECT x FROM a",
+                "SELECT x FROM missing_table"]:
+        with pytest.raises(MettleError) as e:
+            conn.gpu_processing(sql)
+        assert e.value.code == L.UNSUPPORTED, sql
+
+
+@pytest.mark.gpu
+def test_budget_exceeded(conn):
+    conn.execute("CALL gpu_buffer_init('64 KB', '64 KB', pinned_memory_size = '64 MB')")
+    conn.create_table("big", {"x": (L.T_BIGINT, np.arange(100_000, dtype=np.int64))})
+    conn.gpu_register_table("big")
+    with pytest.raises(MettleError) as e:
+        conn.gpu_processing("SELECT x FROM big WHERE x > 5")
+    assert e.value.code == L.BUDGET_EXCEEDED

@@ -1,0 +1,108 @@
+"""The serving loop: concurrent requests overlap on the device, are admitted
+against the processing-region budget, and each result is the same alone and
+in the mix."""
+import threading
+
+import numpy as np
+import pytest
+
+from mettle_b200 import MettleError
+from mettle_b200 import _lib as L
+from mettle_b200 import workloads as W
+
+
+def setup_tables(conn):
+    conn.execute("CALL gpu_buffer_init('4 GB', '2 GB')")
+    d1 = W.numbers(200_000, seed_salt=1)
+    conn.create_table("numbers", {"value": (L.T_INTEGER, d1["value"])})
+    d2 = W.scan(300_000, seed_salt=1)
+    conn.create_table("t", {"a": (L.T_INTEGER, d2["a"]), "b": (L.T_BIGINT, d2["b"]), "c": (L.T_FLOAT, d2["c"]),
+                            "d": (L.T_DATE, d2["d"]), "e": (L.T_TIMESTAMP, d2["e"])})
+    d3 = W.groupby(n=400_000, groups=2000, dist="zipf", seed_salt=1)
+    conn.create_table("g", {"k": (L.T_BIGINT, d3["k"]), "v": (L.T_BIGINT, d3["v"]), "f": (L.T_FLOAT, d3["f"])})
+    for n in ("numbers", "t", "g"):
+        conn.gpu_register_table(n, upload=True)
+
+
+def mixed_queries(n, seed=0):
+    r = np.random.default_rng(seed)
+    out = []
+    for i in range(n):
+        kind = i % 3
+        if kind == 0:
+            k = int(r.integers(0, 1_000_000))
+            out.append(f"SELECT value, value * 10 AS scaled FROM numbers WHERE value > {k} ORDER BY value LIMIT 50")
+        elif kind == 1:
+            out.append(W.scan_sql("abcde"[int(r.integers(0, 5))], "<", float(r.choice([0.01, 0.1, 0.5]))))
+        else:
+            lim = int(r.integers(5, 100))
+            out.append(W.C3_SQL.replace("FROM t", "FROM g").replace("LIMIT 100", f"LIMIT {lim}"))
+    return out
+
+
+@pytest.mark.gpu
+def test_results_identical_alone_and_in_mix(conn):
+    setup_tables(conn)
+    qs = mixed_queries(36)
+    alone = [conn.gpu_processing(q).fetchall() for q in qs]
+    reqs = [conn.submit(q) for q in qs]
+    mixed = [r.wait(timeout_s=120).fetchall() for r in reqs]
+    for q, a, m in zip(qs, alone, mixed):
+        if "sum_f" in q:
+            # FLOAT sums: same within the stated tolerance (atomic order differs)
+            for ra, rm in zip(a, m):
+                assert ra[:6] == rm[:6] and ra[7:9] == rm[7:9]
+                assert abs(ra[6] - rm[6]) <= 1e-6 * abs(ra[6]) and abs(ra[9] - rm[9]) <= 1e-6 * abs(ra[9])
+        else:
+            assert a == m, q
+    st = conn.serve_stats()
+    assert st["completed"] >= len(qs) and st["in_flight"] == 0
+    assert all(r.latency_ms() > 0 for r in reqs)
+
+
+@pytest.mark.gpu
+def test_concurrent_submitters(conn):
+    setup_tables(conn)
+    qs = mixed_queries(24, seed=5)
+    want = {q: conn.gpu_processing(q).fetchall() for q in qs if "sum_f" not in q}
+    errors = []
+
+    def client(part):
+        try:
+            for q in part:
+                got = conn.submit(q).wait(timeout_s=120).fetchall()
+                if q in want and got != want[q]:
+                    errors.append(q)
+        except Exception as e:  # pragma: no cover - reported below
+            errors.append(repr(e))
+
+    ths = [threading.Thread(target=client, args=(qs[i::4],)) for i in range(4)]
+    for t in ths:
+        t.start()
+    for t in ths:
+        t.join()
+    assert not errors, errors
+
+
+@pytest.mark.gpu
+def test_admission_rejects_what_never_fits(conn):
+    conn.execute("CALL gpu_buffer_init('64 MB', '1 MB', pinned_memory_size = '256 MB')")
+    d = W.groupby(n=2_000_000, groups=1_000_000, seed_salt=4)
+    conn.create_table("g", {"k": (L.T_BIGINT, d["k"]), "v": (L.T_BIGINT, d["v"]), "f": (L.T_FLOAT, d["f"])})
+    conn.gpu_register_table("g")
+    req = conn.submit("SELECT k, SUM(v) FROM g GROUP BY k ORDER BY k LIMIT 5")
+    with pytest.raises(MettleError) as e:
+        req.wait(timeout_s=60)
+    assert e.value.code == L.BUDGET_EXCEEDED
+    assert conn.serve_stats()["rejected"] >= 1
+
+
+@pytest.mark.gpu
+def test_small_queries_are_graph_batched(conn):
+    setup_tables(conn)
+    qs = [f"SELECT value FROM numbers WHERE value > {k} ORDER BY value LIMIT 10" for k in range(0, 64000, 1000)]
+    reqs = [conn.submit(q) for q in qs]
+    res = [r.wait(timeout_s=60).fetchall() for r in reqs]
+    for q, r in zip(qs, res):
+        assert r == conn.gpu_processing(q).fetchall()
+    assert conn.serve_stats()["batched_launches"] >= 1
