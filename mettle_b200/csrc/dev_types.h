@@ -176,6 +176,16 @@ struct PipeDesc {
   VmProg progs[kMaxProgs];
   DBuild builds[kMaxProbes + 1];
   int32_t first_col;                // column prefetched for every tuple (-1 none)
+  // Columns the sink reads for every surviving tuple (build key, group keys,
+  // aggregate inputs, outputs): fetched for a batch of tuples at once so
+  // their loads overlap, then served to the expression VM from registers.
+  int32_t n_sink_cols;
+  int32_t sink_cols[6];
+  // Columns of the driving table read for (nearly) every tuple: each tile of
+  // them is staged into shared memory with bulk (TMA) copies, double
+  // buffered, so their HBM traffic is in flight independently of registers.
+  int32_t n_stream;
+  int32_t stream_cols[4];
 
   // sink
   int32_t sink;

@@ -409,6 +409,7 @@ struct Compiler {
   struct PipeBuilder {
     PipeDesc d;
     std::map<std::pair<int, const Column*>, int> colmap;
+    std::vector<double> op_sel;  // estimated pass fraction of each op
     PipeBuilder() {
       memset(&d, 0, sizeof(d));
       d.first_col = -1;
@@ -559,7 +560,81 @@ struct Compiler {
       pb.d.ops[pb.d.n_ops].kind = OPK_FILTER;
       pb.d.ops[pb.d.n_ops].idx = pi;
       pb.d.n_ops++;
+      pb.op_sel.push_back(estimate_selectivity(f));
     }
+  }
+
+  // Pass fraction of a predicate from the column's min/max (uniform values
+  // assumed); used only to decide which columns to stream.
+  double estimate_selectivity(const BFilter& f) {
+    if (f.op == C_TRUE) return 1.0;
+    if (f.op == C_FALSE) return 0.0;
+    const int32_t pt = storage_ptype(f.col->type);
+    if (pt != P_I32 && pt != P_I64) return f.op == C_EQ ? 0.05 : 0.5;
+    column_minmax(ctx, *f.col);
+    if (!f.col->has_minmax) return 0.5;
+    const double lo = (double)f.col->vmin, hi = (double)f.col->vmax, span = hi - lo + 1.0, x = (double)f.ilit;
+    auto clamp = [](double v) { return v < 0 ? 0.0 : (v > 1 ? 1.0 : v); };
+    switch (f.op) {
+      case C_LT: return clamp((x - lo) / span);
+      case C_LE: return clamp((x - lo + 1) / span);
+      case C_GT: return clamp((hi - x) / span);
+      case C_GE: return clamp((hi - x + 1) / span);
+      case C_EQ: return clamp(1.0 / span);
+      case C_NE: return clamp(1.0 - 1.0 / span);
+      default: return 0.5;
+    }
+  }
+
+  static void prog_cols(const VmProg& p, std::vector<int>& out) {
+    for (int i = 0; i < p.n; ++i)
+      if (p.ins[i].op == VM_COL && std::find(out.begin(), out.end(), p.ins[i].arg) == out.end())
+        out.push_back(p.ins[i].arg);
+  }
+
+  // Chooses the sink's prefetched columns and the streamed (bulk-copied)
+  // columns of the driving table.
+  void plan_columns(PipeBuilder& pb) {
+    PipeDesc& d = pb.d;
+    std::vector<int> sink;
+    if (d.sink == SK_BUILD) sink.push_back(d.build_key_col);
+    if (d.sink == SK_AGG_HASH || d.sink == SK_AGG_SMEM)
+      for (int k = 0; k < d.table.n_keys; ++k) prog_cols(d.progs[d.key_prog[k]], sink);
+    if (d.sink == SK_AGG_HASH || d.sink == SK_AGG_SMEM || d.sink == SK_AGG_SLOT || d.sink == SK_AGG_SCALAR)
+      for (int a = 0; a < d.n_aggs; ++a)
+        if (d.aggs[a].prog >= 0) prog_cols(d.progs[d.aggs[a].prog], sink);
+    if (d.sink == SK_MATERIALIZE)
+      for (int q = 0; q < d.n_out; ++q) prog_cols(d.progs[d.out_prog[q]], sink);
+    d.n_sink_cols = (int)std::min<size_t>(sink.size(), 6);
+    for (int i = 0; i < d.n_sink_cols; ++i) d.sink_cols[i] = sink[i];
+
+    d.n_stream = 0;
+    if (d.tuple_input) return;
+    uint32_t budget = 16;  // bytes per tuple: 64 KB of double-buffered tiles
+    if (d.sink == SK_AGG_SMEM) {
+      size_t table = pipeline_smem_bytes(d);
+      budget = table >= 150 * 1024 ? 0 : (uint32_t)std::min<size_t>(16, (150 * 1024 - table) / (2 * 2048));
+    }
+    uint32_t used = 0;
+    auto try_stream = [&](int col) {
+      if (d.cols[col].src != d.drive_src || d.n_stream >= 4) return;
+      for (int i = 0; i < d.n_stream; ++i)
+        if (d.stream_cols[i] == col) return;
+      uint32_t w = (uint32_t)ptype_width(d.cols[col].ptype);
+      if (w > 8 || used + w > budget) return;
+      d.stream_cols[d.n_stream++] = col;
+      used += w;
+    };
+    double reach = 1.0;  // estimated fraction of tuples reaching the op
+    const double kStreamAbove = 0.25;
+    for (int o = 0; o < d.n_ops; ++o) {
+      const PipeOp& op = d.ops[o];
+      const int col = op.kind == OPK_FILTER ? d.preds[op.idx].col : d.probes[op.idx].key_col;
+      if (o == 0 || reach >= kStreamAbove) try_stream(col);
+      reach *= op.kind == OPK_FILTER ? (o < (int)pb.op_sel.size() ? pb.op_sel[o] : 0.5) : 0.25;
+    }
+    if (reach >= kStreamAbove)
+      for (int c : sink) try_stream(c);
   }
 
   // Probes into the children's builds; fill masks bring the row ids listed
@@ -590,6 +665,7 @@ struct Compiler {
 
   void push_pipeline(PipeBuilder& pb, uint64_t n_hint) {
     static const char* sinks[] = {"none", "build", "materialize", "agg_hash", "agg_smem", "agg_slot", "agg_scalar"};
+    plan_columns(pb);
     Step s;
     s.k = Step::PIPELINE;
     s.pipe = pb.d;

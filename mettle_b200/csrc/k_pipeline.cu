@@ -270,28 +270,70 @@ __device__ __forceinline__ int smem_agg_find(const PipeDesc& d, SmemAgg& s, cons
 }
 
 // ------------------------------------------------------------ the kernel
+constexpr int kThreads = 256;
+constexpr int kItems = 8;
+constexpr int kTile = kThreads * kItems;  // tuples per tile
+constexpr int kBatch = 4;                 // tuples a thread advances through the ops together
+constexpr int kAggCols = 4;               // sink columns fetched ahead in phase A
+constexpr int kOutCols = 6;               // output columns fetched ahead in the write phase
+
+struct StreamLayout {
+  int n;
+  int col[4];
+  int width[4];
+  uint32_t off[4];
+  uint32_t bytes;  // per buffer
+};
+
+__host__ __device__ inline uint32_t stream_bytes_per_row(const PipeDesc& d) {
+  uint32_t w = 0;
+  for (int i = 0; i < d.n_stream && i < 4; ++i) w += (uint32_t)ptype_width(d.cols[d.stream_cols[i]].ptype);
+  return w;
+}
+
 // SINK is a compile-time constant so each instantiation carries only its own
-// sink code (register pressure decides occupancy for this streaming kernel).
-template <int THREADS, int ITEMS, int VEC, int SINK>
-__global__ void __launch_bounds__(THREADS) k_pipeline(const __grid_constant__ PipeDesc d) {
-  constexpr int TILE = THREADS * ITEMS;
-  constexpr int CHUNKS = ITEMS / VEC;
-  extern __shared__ __align__(16) uint8_t smem[];
+// sink code. Tiles: tuple ti of a tile is handled by thread ti % 256 (striped),
+// which keeps shared-memory reads conflict free. The streamed columns of the
+// next tile are copied into the idle shared buffer by one thread with bulk
+// (TMA) copies while the CTA works on the current tile. Other columns are
+// read for a batch of kBatch tuples at once so their loads overlap.
+template <int SINK>
+__global__ void __launch_bounds__(kThreads) k_pipeline(const __grid_constant__ PipeDesc d) {
+  constexpr int THREADS = kThreads, ITEMS = kItems, TILE = kTile;
+  extern __shared__ __align__(128) uint8_t smem[];
+  __shared__ __align__(8) uint64_t s_mbar[2];
   __shared__ uint32_t s_warp[THREADS / 32 + 1];
   __shared__ uint64_t s_base;
-  __shared__ uint64_t s_tile;
-  __shared__ uint64_t s_red[kMaxAggs][THREADS / 32];
-  __shared__ int64_t s_redhi[kMaxAggs][THREADS / 32];
+  __shared__ uint64_t s_tile[2];
+  __shared__ uint64_t s_red[SINK == SK_AGG_SCALAR ? kMaxAggs : 1][THREADS / 32];
+  __shared__ int64_t s_redhi[SINK == SK_AGG_SCALAR ? kMaxAggs : 1][THREADS / 32];
 
   const int tid = threadIdx.x;
   const uint64_t n = d.in_count ? *d.in_count : d.n;
   const uint64_t n_tiles = (n + TILE - 1) / TILE;
   uint32_t st = 0;
 
-  // per-sink shared memory
-  uint8_t* s_keep = smem;                                   // MATERIALIZE
-  uint16_t* s_list = (uint16_t*)(smem + TILE);
-  uint32_t* s_rid = (uint32_t*)(smem + TILE + 2 * TILE);
+  StreamLayout S;
+  S.n = d.tuple_input ? 0 : (d.n_stream < 4 ? d.n_stream : 4);
+  {
+    uint32_t off = 0;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      S.col[i] = i < S.n ? d.stream_cols[i] : -1;
+      S.width[i] = i < S.n ? ptype_width(d.cols[S.col[i]].ptype) : 0;
+      S.off[i] = off;
+      off += (uint32_t)TILE * (uint32_t)S.width[i];
+    }
+    S.bytes = off;
+  }
+  uint8_t* const sbuf0 = smem;
+  uint8_t* const sbuf1 = smem + S.bytes;
+  uint8_t* const sink_smem = smem + 2 * S.bytes;
+
+  // MATERIALIZE shared memory: keep flags | compacted tile list | row ids
+  uint8_t* s_keep = sink_smem;
+  uint16_t* s_list = (uint16_t*)(sink_smem + TILE);
+  uint32_t* s_rid = (uint32_t*)(sink_smem + 3 * TILE);
   int rid_slot[kMaxSrc];
   {
     int q = 0;
@@ -302,13 +344,9 @@ __global__ void __launch_bounds__(THREADS) k_pipeline(const __grid_constant__ Pi
     }
   }
   SmemAgg sagg;
-  if (SINK == SK_AGG_SMEM) {
-    smem_agg_init(d, sagg, smem);
-    __syncthreads();
-  }
-  // scalar aggregate partials (registers)
-  uint64_t plo[kMaxAggs];
-  int64_t phi[kMaxAggs];
+  if (SINK == SK_AGG_SMEM) smem_agg_init(d, sagg, sink_smem);
+  uint64_t plo[SINK == SK_AGG_SCALAR ? kMaxAggs : 1];
+  int64_t phi[SINK == SK_AGG_SCALAR ? kMaxAggs : 1];
   if (SINK == SK_AGG_SCALAR) {
 #pragma unroll
     for (int a = 0; a < kMaxAggs; ++a) {
@@ -318,7 +356,6 @@ __global__ void __launch_bounds__(THREADS) k_pipeline(const __grid_constant__ Pi
           case A_MIN_I: init = 0x7FFFFFFFFFFFFFFFULL; break;
           case A_MAX_I: init = 0x8000000000000000ULL; break;
           case A_MIN_F: init = ~0ULL; break;
-          case A_SUM_F: init = (uint64_t)__double_as_longlong(0.0); break;
           default: init = 0; break;
         }
       }
@@ -326,204 +363,268 @@ __global__ void __launch_bounds__(THREADS) k_pipeline(const __grid_constant__ Pi
       phi[a] = 0;
     }
   }
+  if (tid == 0 && S.n) {
+    mbar_init(&s_mbar[0], 1);
+    mbar_init(&s_mbar[1], 1);
+    mbar_fence_init();
+  }
 
   const bool dynamic_tiles = SINK == SK_MATERIALIZE;
-  uint64_t iter = 0;
-  for (;;) {
-    uint64_t tile;
-    if (dynamic_tiles) {
-      if (tid == 0) s_tile = atomicAdd(d.tile_counter, 1u);
-      __syncthreads();
-      tile = s_tile;
-    } else {
-      tile = blockIdx.x + iter * gridDim.x;
-    }
-    ++iter;
-    if (tile >= n_tiles) break;
-    const uint64_t tile_base = tile * (uint64_t)TILE;
+  // Thread 0 stages the streamed columns of a full tile into buffer `b`.
+  auto issue = [&](uint64_t tile, int b) {
+    const uint64_t base = tile * (uint64_t)TILE;
+    if (base + TILE > n) return;  // the tail tile is loaded directly
+    uint8_t* dst = b ? sbuf1 : sbuf0;
+    fence_proxy_async();
+    mbar_arrive_expect_tx(&s_mbar[b], S.bytes);
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+      if (i < S.n)
+        bulk_g2s(dst + S.off[i], (const uint8_t*)d.cols[S.col[i]].ptr + base * (uint64_t)S.width[i],
+                 (uint32_t)TILE * (uint32_t)S.width[i], &s_mbar[b]);
+  };
 
-    // Stream the first column of every tuple with vector loads.
-    int64_t pre[ITEMS];
-    const bool have_pre = d.first_col >= 0 && !d.tuple_input;
-    if (have_pre) {
-      const DCol& c = d.cols[d.first_col];
-#pragma unroll
-      for (int j = 0; j < CHUNKS; ++j) {
-        const uint64_t i0 = tile_base + ((uint64_t)j * THREADS + tid) * VEC;
-        if (i0 + VEC <= n) {
-          if (VEC == 4) {
-            int4 v = __ldg((const int4*)((const int32_t*)c.ptr + i0));
-            if (c.ptype == P_I32) {
-              pre[j * VEC + 0] = v.x; pre[j * VEC + 1] = v.y; pre[j * VEC + 2] = v.z; pre[j * VEC + 3] = v.w;
-            } else {
-              pre[j * VEC + 0] = (uint32_t)v.x; pre[j * VEC + 1] = (uint32_t)v.y;
-              pre[j * VEC + 2] = (uint32_t)v.z; pre[j * VEC + 3] = (uint32_t)v.w;
-            }
-          } else if (VEC == 2) {
-            longlong2 v = __ldg((const longlong2*)((const int64_t*)c.ptr + i0));
-            pre[j * VEC + 0] = v.x;
-            pre[j * VEC + 1] = v.y;
-          } else {
-            pre[j * VEC] = load_bits(c.ptr, c.ptype, i0);
+  if (tid == 0) s_tile[0] = dynamic_tiles ? (uint64_t)atomicAdd(d.tile_counter, 1u) : (uint64_t)blockIdx.x;
+  __syncthreads();
+  uint64_t cur = s_tile[0];
+  if (tid == 0 && S.n && cur < n_tiles) issue(cur, 0);
+  uint32_t parity = 0;
+  int b = 0;
+  uint32_t k = 0;
+  while (cur < n_tiles) {
+    // Claim the next tile and start its copies before waiting on this one.
+    uint64_t nxt_static = cur + gridDim.x;
+    if (tid == 0) {
+      uint64_t nx = dynamic_tiles ? (uint64_t)atomicAdd(d.tile_counter, 1u) : nxt_static;
+      s_tile[(k + 1) & 1] = nx;
+      if (S.n && nx < n_tiles) issue(nx, b ^ 1);
+    }
+    const uint64_t tile = cur;
+    const uint64_t tile_base = tile * (uint64_t)TILE;
+    uint8_t* const buf = b ? sbuf1 : sbuf0;
+    if (S.n) {
+      bool ok = true;
+      if (tile_base + TILE <= n) {
+        ok = mbar_wait(&s_mbar[b], (parity >> b) & 1u);
+        parity ^= 1u << b;
+      } else {
+        for (int i = 0; i < S.n; ++i) {
+          const DCol& c = d.cols[S.col[i]];
+          for (int r = tid; r < TILE; r += THREADS) {
+            const uint64_t g = tile_base + r;
+            int64_t v = g < n ? load_bits(c.ptr, c.ptype, g) : 0;
+            if (S.width[i] == 4) ((uint32_t*)(buf + S.off[i]))[r] = (uint32_t)v;
+            else ((int64_t*)(buf + S.off[i]))[r] = v;
           }
-        } else {
-#pragma unroll
-          for (int k = 0; k < VEC; ++k) pre[j * VEC + k] = (i0 + k < n) ? load_bits(c.ptr, c.ptype, i0 + k) : 0;
         }
+      }
+      if (__syncthreads_or(!ok)) {
+        st |= ST_SPIN_LIMIT;
+        // give the copies still in flight a bounded chance to land, then stop
+        mbar_wait(&s_mbar[b ^ 1], (parity >> (b ^ 1)) & 1u);
+        break;
       }
     }
 
-    // The first op, when it filters the streamed column, runs for every
-    // tuple from registers; the survivors form a bit mask.
-    const bool first_filter = have_pre && d.n_ops > 0 && d.ops[0].kind == OPK_FILTER &&
-                              d.preds[d.ops[0].idx].col == d.first_col;
+    // Value of column `col` for a tuple: shared memory when it is a streamed
+    // column of the driving table, else a global load.
+    auto fetch = [&](int col, uint32_t rowid, uint32_t ti) -> int64_t {
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+        if (i < S.n && S.col[i] == col) {
+          if (S.width[i] == 4)
+            return d.cols[col].ptype == P_I32 ? (int64_t)((const int32_t*)(buf + S.off[i]))[ti]
+                                              : (int64_t)((const uint32_t*)(buf + S.off[i]))[ti];
+          return ((const int64_t*)(buf + S.off[i]))[ti];
+        }
+      const DCol& c = d.cols[col];
+      return load_bits(c.ptr, c.ptype, rowid);
+    };
+
     uint32_t alive = 0;
 #pragma unroll
-    for (int it = 0; it < ITEMS; ++it) {
-      const int j = it / VEC, k = it % VEC;
-      const uint64_t gi = tile_base + ((uint64_t)j * THREADS + tid) * VEC + k;
-      bool keep = gi < n;
-      if (keep && first_filter) {
-        const DPred& p = d.preds[d.ops[0].idx];
-        keep = eval_pred_bits(pre[it], d.cols[p.col].ptype, p);
-      }
-      alive |= (keep ? 1u : 0u) << it;
-    }
+    for (int it = 0; it < ITEMS; ++it) alive |= (tile_base + (uint64_t)it * THREADS + tid < n ? 1u : 0u) << it;
 
-    // Phase A: remaining filters, probes and the per-tuple sinks.
+    // Phase A: ops and sink, kBatch tuples at a time.
 #pragma unroll 1
-    for (int it = 0; it < ITEMS; ++it) {
-      const int j = it / VEC, k = it % VEC;
-      const uint32_t ti = (uint32_t)(((uint32_t)j * THREADS + tid) * VEC + k);
-      const uint64_t gi = tile_base + ti;
-      bool keep = (alive >> it) & 1u;
-      uint32_t rid[kMaxSrc];
-      uint32_t slots[kMaxProbes];
+    for (int h = 0; h < ITEMS / kBatch; ++h) {
+      uint32_t am = (alive >> (h * kBatch)) & ((1u << kBatch) - 1u);
+      uint32_t rid[kBatch][kMaxSrc];
+      uint32_t gslot[kBatch];
+      uint32_t ti[kBatch];
 #pragma unroll
-      for (int s = 0; s < kMaxSrc; ++s) rid[s] = 0;
+      for (int bb = 0; bb < kBatch; ++bb) {
+        ti[bb] = (uint32_t)((h * kBatch + bb) * THREADS + tid);
+        gslot[bb] = 0;
 #pragma unroll
-      for (int p = 0; p < kMaxProbes; ++p) slots[p] = 0;
-      if (keep) {
-        if (d.tuple_input) {
-#pragma unroll
-          for (int s = 0; s < kMaxSrc; ++s)
-            if ((d.src_mask >> s) & 1u) rid[s] = d.in_rids[s][gi];
-        } else {
-#pragma unroll
-          for (int s = 0; s < kMaxSrc; ++s)
-            if (s == d.drive_src) rid[s] = (uint32_t)gi;
-        }
+        for (int s = 0; s < kMaxSrc; ++s)
+          rid[bb][s] = (!d.tuple_input && s == d.drive_src) ? (uint32_t)(tile_base + ti[bb]) : 0u;
       }
-      for (int o = first_filter ? 1 : 0; o < d.n_ops && keep; ++o) {
+      if (d.tuple_input) {
+#pragma unroll
+        for (int s = 0; s < kMaxSrc; ++s)
+          if ((d.src_mask >> s) & 1u) {
+#pragma unroll
+            for (int bb = 0; bb < kBatch; ++bb)
+              if ((am >> bb) & 1u) rid[bb][s] = d.in_rids[s][tile_base + ti[bb]];
+          }
+      }
+      for (int o = 0; o < d.n_ops && am; ++o) {
         const PipeOp op = d.ops[o];
         if (op.kind == OPK_FILTER) {
           const DPred& p = d.preds[op.idx];
           const DCol& c = d.cols[p.col];
-          keep = eval_pred_bits(load_bits(c.ptr, c.ptype, pick(rid, c.src)), c.ptype, p);
+          int64_t v[kBatch];
+#pragma unroll
+          for (int bb = 0; bb < kBatch; ++bb)
+            v[bb] = ((am >> bb) & 1u) ? fetch(p.col, pick(rid[bb], c.src), ti[bb]) : 0;
+#pragma unroll
+          for (int bb = 0; bb < kBatch; ++bb)
+            if (((am >> bb) & 1u) && !eval_pred_bits(v[bb], c.ptype, p)) am &= ~(1u << bb);
         } else {
           const DProbe& pr = d.probes[op.idx];
           const DCol& c = d.cols[pr.key_col];
-          const int64_t key = load_bits(c.ptr, c.ptype, pick(rid, c.src));
-          uint32_t slot = 0;
-          const DBuild& b = d.builds[pr.build];
-          keep = build_lookup(b, key, slot, st);
-          if (keep) {
+          const DBuild& bd = d.builds[pr.build];
+          int64_t key[kBatch];
+          uint32_t sl[kBatch];
 #pragma unroll
-            for (int q = 0; q < kMaxProbes; ++q)
-              if (q == op.idx) slots[q] = slot;
+          for (int bb = 0; bb < kBatch; ++bb)
+            key[bb] = ((am >> bb) & 1u) ? fetch(pr.key_col, pick(rid[bb], c.src), ti[bb]) : 0;
+          if (bd.kind == B_DENSE) {
+            uint32_t m[kBatch];
 #pragma unroll
-            for (int s = 0; s < kMaxSrc; ++s)
-              if ((pr.fill_mask >> s) & 1u) rid[s] = b.payload[s][slot];
+            for (int bb = 0; bb < kBatch; ++bb) {
+              const uint64_t kk = (uint64_t)(key[bb] - bd.key_min);
+              m[bb] = (((am >> bb) & 1u) && kk < bd.capacity) ? bd.dense_map[kk] : 0u;
+            }
+#pragma unroll
+            for (int bb = 0; bb < kBatch; ++bb) {
+              if (m[bb] == 0u) am &= ~(1u << bb);
+              sl[bb] = m[bb] - 1u;
+            }
+          } else {
+#pragma unroll
+            for (int bb = 0; bb < kBatch; ++bb) {
+              uint32_t s_ = 0;
+              if (((am >> bb) & 1u) && !build_lookup(bd, key[bb], s_, st)) am &= ~(1u << bb);
+              sl[bb] = s_;
+            }
           }
+          if (op.idx == d.slot_probe) {
+#pragma unroll
+            for (int bb = 0; bb < kBatch; ++bb) gslot[bb] = sl[bb];
+          }
+#pragma unroll
+          for (int s = 0; s < kMaxSrc; ++s)
+            if ((pr.fill_mask >> s) & 1u) {
+#pragma unroll
+              for (int bb = 0; bb < kBatch; ++bb)
+                if ((am >> bb) & 1u) rid[bb][s] = bd.payload[s][sl[bb]];
+            }
         }
       }
 
-      switch (SINK) {
-        case SK_MATERIALIZE:
-          s_keep[ti] = keep ? 1 : 0;
+      if (SINK == SK_MATERIALIZE) {
+#pragma unroll
+        for (int bb = 0; bb < kBatch; ++bb) {
+          const bool keep = (am >> bb) & 1u;
+          s_keep[ti[bb]] = keep ? 1 : 0;
           if (keep) {
 #pragma unroll
             for (int s = 0; s < kMaxSrc; ++s)
-              if (rid_slot[s] >= 0) s_rid[(size_t)rid_slot[s] * TILE + ti] = rid[s];
+              if (rid_slot[s] >= 0) s_rid[(size_t)rid_slot[s] * TILE + ti[bb]] = rid[bb][s];
           }
-          break;
-        case SK_BUILD:
-          if (keep) {
-            const DBuild& b = d.builds[d.sink_build];
+        }
+        continue;
+      }
+      if (!am) continue;
+
+      // Fetch the sink's columns for the whole batch, then run the sink.
+      int64_t cv[kBatch][kAggCols];
+#pragma unroll
+      for (int jc = 0; jc < kAggCols; ++jc) {
+        const bool use = jc < d.n_sink_cols;
+        const int col = use ? d.sink_cols[jc] : 0;
+        const int src = d.cols[col].src;
+#pragma unroll
+        for (int bb = 0; bb < kBatch; ++bb)
+          cv[bb][jc] = (use && ((am >> bb) & 1u)) ? fetch(col, pick(rid[bb], src), ti[bb]) : 0;
+      }
+#pragma unroll
+      for (int bb = 0; bb < kBatch; ++bb) {
+        if (!((am >> bb) & 1u)) continue;
+        switch (SINK) {
+          case SK_BUILD: {
+            const DBuild& bd = d.builds[d.sink_build];
             cg::coalesced_group g = cg::coalesced_threads();
             uint32_t base = 0;
-            if (g.thread_rank() == 0) base = atomicAdd(b.n_slots, g.size());
+            if (g.thread_rank() == 0) base = atomicAdd(bd.n_slots, g.size());
             base = g.shfl(base, 0);
             const uint32_t slot = base + g.thread_rank();
-            const DCol& c = d.cols[d.build_key_col];
-            const int64_t key = load_bits(c.ptr, c.ptype, pick(rid, c.src));
+            const int64_t key = (d.n_sink_cols > 0 && d.sink_cols[0] == d.build_key_col)
+                                    ? cv[bb][0]
+                                    : fetch(d.build_key_col, pick(rid[bb], d.cols[d.build_key_col].src), ti[bb]);
 #pragma unroll
             for (int s = 0; s < kMaxSrc; ++s)
-              if ((d.build_payload_mask >> s) & 1u) b.payload[s][slot] = rid[s];
+              if ((d.build_payload_mask >> s) & 1u) bd.payload[s][slot] = rid[bb][s];
             // A representative-row aggregate downstream keeps its states by
             // this slot: initialize them here so no memset of the (build
             // table sized) state arrays is needed per query.
             for (int a = 0; a < d.n_aggs; ++a) agg_init_global(d.aggs[a], slot);
             if (d.slot_hit) d.slot_hit[slot] = 0;
-            build_insert(b, key, slot, st);
+            build_insert(bd, key, slot, st);
+            break;
           }
-          break;
-        case SK_AGG_SLOT:
-          if (keep) {
-            const uint32_t g = pick5(slots, d.slot_probe);
+          case SK_AGG_SLOT: {
+            const uint32_t g = gslot[bb];
             d.slot_hit[g] = 1;
             for (int a = 0; a < d.n_aggs; ++a) {
               const DAgg& ag = d.aggs[a];
               Val v{0, 0};
               int32_t vt = P_I64;
               if (ag.prog >= 0) {
-                v = vm_eval(d.progs[ag.prog], d.cols, rid, slots, st);
+                v = vm_eval_c<kAggCols>(d.progs[ag.prog], d.cols, rid[bb], d.sink_cols, d.n_sink_cols, cv[bb], st);
                 vt = d.progs[ag.prog].out_type;
               }
               agg_apply(ag.fn, (unsigned long long*)(ag.lo + g), (long long*)(ag.hi ? ag.hi + g : nullptr), v, vt);
             }
+            break;
           }
-          break;
-        case SK_AGG_HASH:
-        case SK_AGG_SMEM:
-          if (keep) {
+          case SK_AGG_HASH:
+          case SK_AGG_SMEM: {
             uint64_t kw[kMaxKeys];
 #pragma unroll
             for (int i = 0; i < kMaxKeys; ++i)
-              kw[i] = i < d.table.n_keys ? (uint64_t)vm_eval(d.progs[d.key_prog[i]], d.cols, rid, slots, st).lo : 0;
+              kw[i] = i < d.table.n_keys
+                          ? (uint64_t)vm_eval_c<kAggCols>(d.progs[d.key_prog[i]], d.cols, rid[bb], d.sink_cols,
+                                                          d.n_sink_cols, cv[bb], st).lo
+                          : 0;
             int sidx = -1;
             if (SINK == SK_AGG_SMEM) sidx = smem_agg_find(d, sagg, kw, st);
-            if (sidx >= 0) {
-              for (int a = 0; a < d.n_aggs; ++a) {
-                const DAgg& ag = d.aggs[a];
-                Val v{0, 0};
-                int32_t vt = P_I64;
-                if (ag.prog >= 0) {
-                  v = vm_eval(d.progs[ag.prog], d.cols, rid, slots, st);
-                  vt = d.progs[ag.prog].out_type;
-                }
-                long long* hp = sagg.hi_index[a] >= 0 ? (long long*)(sagg.hi + (size_t)sagg.hi_index[a] * sagg.cap + sidx) : nullptr;
-                agg_apply(ag.fn, (unsigned long long*)(sagg.lo + (size_t)a * sagg.cap + sidx), hp, v, vt);
+            uint64_t g = d.table.capacity;
+            if (sidx < 0) g = agg_find_global(d, kw, st);
+            if (sidx < 0 && g >= d.table.capacity) break;
+            for (int a = 0; a < d.n_aggs; ++a) {
+              const DAgg& ag = d.aggs[a];
+              Val v{0, 0};
+              int32_t vt = P_I64;
+              if (ag.prog >= 0) {
+                v = vm_eval_c<kAggCols>(d.progs[ag.prog], d.cols, rid[bb], d.sink_cols, d.n_sink_cols, cv[bb], st);
+                vt = d.progs[ag.prog].out_type;
               }
-            } else {
-              uint64_t g = agg_find_global(d, kw, st);
-              if (g < d.table.capacity) {
-                for (int a = 0; a < d.n_aggs; ++a) {
-                  const DAgg& ag = d.aggs[a];
-                  Val v{0, 0};
-                  int32_t vt = P_I64;
-                  if (ag.prog >= 0) {
-                    v = vm_eval(d.progs[ag.prog], d.cols, rid, slots, st);
-                    vt = d.progs[ag.prog].out_type;
-                  }
-                  agg_apply(ag.fn, (unsigned long long*)(ag.lo + g), (long long*)(ag.hi ? ag.hi + g : nullptr), v, vt);
-                }
+              if (sidx >= 0) {
+                long long* hp = sagg.hi_index[a] >= 0
+                                    ? (long long*)(sagg.hi + (size_t)sagg.hi_index[a] * sagg.cap + sidx)
+                                    : nullptr;
+                agg_apply(ag.fn, (unsigned long long*)(sagg.lo + (size_t)a * sagg.cap + sidx), hp, v, vt);
+              } else {
+                agg_apply(ag.fn, (unsigned long long*)(ag.lo + g), (long long*)(ag.hi ? ag.hi + g : nullptr), v,
+                          vt);
               }
             }
+            break;
           }
-          break;
-        case SK_AGG_SCALAR:
-          if (keep) {
+          case SK_AGG_SCALAR: {
 #pragma unroll
             for (int a = 0; a < kMaxAggs; ++a) {
               if (a >= d.n_aggs) break;
@@ -531,7 +632,7 @@ __global__ void __launch_bounds__(THREADS) k_pipeline(const __grid_constant__ Pi
               Val v{0, 0};
               int32_t vt = P_I64;
               if (ag.prog >= 0) {
-                v = vm_eval(d.progs[ag.prog], d.cols, rid, slots, st);
+                v = vm_eval_c<kAggCols>(d.progs[ag.prog], d.cols, rid[bb], d.sink_cols, d.n_sink_cols, cv[bb], st);
                 vt = d.progs[ag.prog].out_type;
               }
               switch (ag.fn) {
@@ -544,7 +645,8 @@ __global__ void __launch_bounds__(THREADS) k_pipeline(const __grid_constant__ Pi
                   break;
                 }
                 case A_SUM_F:
-                  plo[a] = (uint64_t)__double_as_longlong(__dadd_rn(__longlong_as_double((long long)plo[a]), val_as_f64(v, vt)));
+                  plo[a] = (uint64_t)__double_as_longlong(
+                      __dadd_rn(__longlong_as_double((long long)plo[a]), val_as_f64(v, vt)));
                   break;
                 case A_MIN_I: if ((int64_t)v.lo < (int64_t)plo[a]) plo[a] = (uint64_t)v.lo; break;
                 case A_MAX_I: if ((int64_t)v.lo > (int64_t)plo[a]) plo[a] = (uint64_t)v.lo; break;
@@ -553,9 +655,10 @@ __global__ void __launch_bounds__(THREADS) k_pipeline(const __grid_constant__ Pi
                 default: break;
               }
             }
+            break;
           }
-          break;
-        default: break;
+          default: break;
+        }
       }
     }
 
@@ -577,32 +680,58 @@ __global__ void __launch_bounds__(THREADS) k_pipeline(const __grid_constant__ Pi
       }
       __syncthreads();
       const uint64_t base = s_base;
-      for (uint32_t p = tid; p < total; p += THREADS) {
-        const uint32_t ti = s_list[p];
-        const uint64_t o = base + p;
-        if (o >= d.out_capacity) {
-          st |= ST_CAPACITY;
-          continue;
-        }
-        uint32_t rid[kMaxSrc];
+      // Write phase: kBatch compacted rows per thread, columns fetched first.
+      for (uint32_t p0 = tid; p0 < total; p0 += THREADS * kBatch) {
+        uint32_t rr[kBatch][kMaxSrc];
+        uint32_t tx[kBatch];
+        uint32_t okm = 0;
 #pragma unroll
-        for (int s = 0; s < kMaxSrc; ++s) rid[s] = rid_slot[s] >= 0 ? s_rid[(size_t)rid_slot[s] * TILE + ti] : 0;
-        if (!d.tuple_input) {
+        for (int bb = 0; bb < kBatch; ++bb) {
+          const uint32_t p = p0 + bb * THREADS;
+          const bool ok = p < total;
+          okm |= (ok ? 1u : 0u) << bb;
+          tx[bb] = ok ? s_list[p] : 0u;
+#pragma unroll
+          for (int s = 0; s < kMaxSrc; ++s) {
+            uint32_t r = (rid_slot[s] >= 0 && ok) ? s_rid[(size_t)rid_slot[s] * TILE + tx[bb]] : 0u;
+            if (!d.tuple_input && s == d.drive_src) r = (uint32_t)(tile_base + tx[bb]);
+            rr[bb][s] = r;
+          }
+        }
+        int64_t cv[kBatch][kOutCols];
+#pragma unroll
+        for (int jc = 0; jc < kOutCols; ++jc) {
+          const bool use = jc < d.n_sink_cols;
+          const int col = use ? d.sink_cols[jc] : 0;
+          const int src = d.cols[col].src;
+#pragma unroll
+          for (int bb = 0; bb < kBatch; ++bb)
+            cv[bb][jc] = (use && ((okm >> bb) & 1u)) ? fetch(col, pick(rr[bb], src), tx[bb]) : 0;
+        }
+#pragma unroll
+        for (int bb = 0; bb < kBatch; ++bb) {
+          if (!((okm >> bb) & 1u)) continue;
+          const uint64_t o = base + p0 + bb * THREADS;
+          if (o >= d.out_capacity) {
+            st |= ST_CAPACITY;
+            continue;
+          }
+          for (int q = 0; q < d.n_out; ++q) {
+            const VmProg& pg = d.progs[d.out_prog[q]];
+            Val v = vm_eval_c<kOutCols>(pg, d.cols, rr[bb], d.sink_cols, d.n_sink_cols, cv[bb], st);
+            store_val(d.out_ptr[q], pg.out_type, o, v);
+          }
 #pragma unroll
           for (int s = 0; s < kMaxSrc; ++s)
-            if (s == d.drive_src) rid[s] = (uint32_t)(tile_base + ti);
+            if ((d.out_rid_mask >> s) & 1u) d.out_rids[s][o] = rr[bb][s];
         }
-        for (int q = 0; q < d.n_out; ++q) {
-          const VmProg& pg = d.progs[d.out_prog[q]];
-          Val v = vm_eval(pg, d.cols, rid, rid /*unused*/, st);
-          store_val(d.out_ptr[q], pg.out_type, o, v);
-        }
-#pragma unroll
-        for (int s = 0; s < kMaxSrc; ++s)
-          if ((d.out_rid_mask >> s) & 1u) d.out_rids[s][o] = rid[s];
       }
-      __syncthreads();
     }
+    // Every thread is done with `buf` (and the sink scratch) before reuse.
+    __syncthreads();
+    cur = s_tile[(k + 1) & 1];
+    ++k;
+    b ^= 1;
   }
 
   // End-of-kernel work.
@@ -683,72 +812,62 @@ static int sm_count() {
   return g_sm_count;
 }
 
-template <int THREADS, int ITEMS, int VEC, int SINK>
-static cudaError_t launch_vec(const PipeDesc& d, size_t smem, uint64_t n_hint, cudaStream_t s) {
-  auto kern = k_pipeline<THREADS, ITEMS, VEC, SINK>;
+size_t pipeline_tile_rows() { return kTile; }
+
+size_t pipeline_stream_bytes(const PipeDesc& d) {
+  return d.tuple_input ? 0 : 2ull * kTile * stream_bytes_per_row(d);
+}
+
+size_t pipeline_smem_bytes(const PipeDesc& d) {
+  constexpr size_t TILE = kTile;
+  size_t s = pipeline_stream_bytes(d);
+  if (d.sink == SK_MATERIALIZE) {
+    size_t q = 0;
+    for (int i = 0; i < kMaxSrc; ++i) {
+      bool implicit = !d.tuple_input && i == d.drive_src;
+      if (((d.mat_src_mask >> i) & 1u) && !implicit) ++q;
+    }
+    s += TILE + 2 * TILE + 4 * TILE * q;
+  }
+  if (d.sink == SK_AGG_SMEM) {
+    size_t n128 = 0;
+    for (int a = 0; a < d.n_aggs; ++a) n128 += d.aggs[a].fn == A_SUM_I128;
+    s += (size_t)d.smem_capacity * (4 + 8 * d.table.n_keys + 8 * d.n_aggs + 8 * n128);
+  }
+  return s;
+}
+
+template <int SINK>
+static cudaError_t launch_sink(const PipeDesc& d, uint64_t n_hint, cudaStream_t s) {
+  auto kern = k_pipeline<SINK>;
+  const size_t smem = pipeline_smem_bytes(d);
   if (smem > 48 * 1024) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
   }
   // Grid = resident CTAs per SM x SM count (a persistent grid-stride grid).
   int blocks_per_sm = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, kern, THREADS, smem) != cudaSuccess ||
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, kern, kThreads, smem) != cudaSuccess ||
       blocks_per_sm < 1) {
     cudaGetLastError();
     blocks_per_sm = 1;
   }
-  constexpr int TILE = THREADS * ITEMS;
-  uint64_t tiles = (n_hint + TILE - 1) / TILE;
+  uint64_t tiles = (n_hint + kTile - 1) / kTile;
   uint64_t max_grid = (uint64_t)sm_count() * (uint64_t)blocks_per_sm;
   uint64_t grid = tiles < max_grid ? tiles : max_grid;
   if (grid == 0) grid = 1;
-  kern<<<(unsigned)grid, THREADS, smem, s>>>(d);
+  kern<<<(unsigned)grid, kThreads, smem, s>>>(d);
   return cudaGetLastError();
 }
 
-size_t pipeline_tile_rows() { return 256 * 8; }
-
-size_t pipeline_smem_bytes(const PipeDesc& d) {
-  constexpr size_t TILE = 256 * 8;
-  if (d.sink == SK_MATERIALIZE) {
-    size_t q = 0;
-    for (int s = 0; s < kMaxSrc; ++s) {
-      bool implicit = !d.tuple_input && s == d.drive_src;
-      if (((d.mat_src_mask >> s) & 1u) && !implicit) ++q;
-    }
-    return TILE + 2 * TILE + 4 * TILE * q;
-  }
-  if (d.sink == SK_AGG_SMEM) {
-    size_t n128 = 0;
-    for (int a = 0; a < d.n_aggs; ++a) n128 += d.aggs[a].fn == A_SUM_I128;
-    return (size_t)d.smem_capacity * (4 + 8 * d.table.n_keys + 8 * d.n_aggs + 8 * n128);
-  }
-  return 0;
-}
-
-template <int SINK>
-static cudaError_t launch_sink(const PipeDesc& d, size_t smem, uint64_t n_hint, int vec, cudaStream_t s) {
-  switch (vec) {
-    case 4: return launch_vec<256, 8, 4, SINK>(d, smem, n_hint, s);
-    case 2: return launch_vec<256, 8, 2, SINK>(d, smem, n_hint, s);
-    default: return launch_vec<256, 8, 1, SINK>(d, smem, n_hint, s);
-  }
-}
-
 cudaError_t launch_pipeline(const PipeDesc& d, uint64_t n_hint, cudaStream_t s) {
-  const size_t smem = pipeline_smem_bytes(d);
-  int vec = 1;
-  if (d.first_col >= 0 && !d.tuple_input) {
-    int w = ptype_width(d.cols[d.first_col].ptype);
-    vec = w == 4 ? 4 : (w == 8 ? 2 : 1);
-  }
   switch (d.sink) {
-    case SK_BUILD: return launch_sink<SK_BUILD>(d, smem, n_hint, vec, s);
-    case SK_MATERIALIZE: return launch_sink<SK_MATERIALIZE>(d, smem, n_hint, vec, s);
-    case SK_AGG_HASH: return launch_sink<SK_AGG_HASH>(d, smem, n_hint, vec, s);
-    case SK_AGG_SMEM: return launch_sink<SK_AGG_SMEM>(d, smem, n_hint, vec, s);
-    case SK_AGG_SLOT: return launch_sink<SK_AGG_SLOT>(d, smem, n_hint, vec, s);
-    case SK_AGG_SCALAR: return launch_sink<SK_AGG_SCALAR>(d, smem, n_hint, vec, s);
+    case SK_BUILD: return launch_sink<SK_BUILD>(d, n_hint, s);
+    case SK_MATERIALIZE: return launch_sink<SK_MATERIALIZE>(d, n_hint, s);
+    case SK_AGG_HASH: return launch_sink<SK_AGG_HASH>(d, n_hint, s);
+    case SK_AGG_SMEM: return launch_sink<SK_AGG_SMEM>(d, n_hint, s);
+    case SK_AGG_SLOT: return launch_sink<SK_AGG_SLOT>(d, n_hint, s);
+    case SK_AGG_SCALAR: return launch_sink<SK_AGG_SCALAR>(d, n_hint, s);
     default: return cudaErrorInvalidValue;
   }
 }

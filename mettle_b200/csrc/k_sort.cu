@@ -369,6 +369,109 @@ __global__ void __launch_bounds__(THREADS) k_topk(const SortItem* __restrict__ k
   }
 }
 
+// ------------------------------------------------------------ warp top-K
+// K <= 32: each warp keeps its best K as a sorted list in registers (lane i
+// holds rank i). A row enters only if it beats the warp's current K-th best
+// (one ballot per 32 rows); an insertion is one ballot plus a one-lane shift.
+// No block-wide barrier runs in the scan loop.
+struct Cand {
+  uint64_t w[4];
+  uint32_t ix;
+};
+
+__device__ __forceinline__ bool cand_less(const Cand& a, const Cand& b) {
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+    if (a.w[i] != b.w[i]) return a.w[i] < b.w[i];
+  return a.ix < b.ix;
+}
+__device__ __forceinline__ Cand cand_shfl(const Cand& c, int src) {
+  Cand r;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) r.w[i] = __shfl_sync(0xFFFFFFFFu, c.w[i], src);
+  r.ix = __shfl_sync(0xFFFFFFFFu, c.ix, src);
+  return r;
+}
+__device__ __forceinline__ Cand cand_shfl_up(const Cand& c) {
+  Cand r;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) r.w[i] = __shfl_up_sync(0xFFFFFFFFu, c.w[i], 1);
+  r.ix = __shfl_up_sync(0xFFFFFFFFu, c.ix, 1);
+  return r;
+}
+__device__ __forceinline__ Cand cand_inf() {
+  Cand c;
+  c.w[0] = c.w[1] = c.w[2] = c.w[3] = ~0ULL;
+  c.ix = 0xFFFFFFFFu;
+  return c;
+}
+
+// Offers each lane's candidate (when `valid`) to the warp list L.
+__device__ __forceinline__ void warp_offer(Cand& L, const Cand& c, bool valid, int K, int lane) {
+  Cand thr = cand_shfl(L, K - 1);
+  uint32_t m = __ballot_sync(0xFFFFFFFFu, valid && cand_less(c, thr));
+  while (m) {
+    const int src = __ffs(m) - 1;
+    m &= m - 1;
+    const Cand x = cand_shfl(c, src);
+    const uint32_t less = __ballot_sync(0xFFFFFFFFu, lane < K && cand_less(L, x));
+    const int pos = __popc(less);
+    if (pos < K) {
+      const Cand up = cand_shfl_up(L);
+      if (lane == pos) L = x;
+      else if (lane > pos && lane < K) L = up;
+      thr = cand_shfl(L, K - 1);
+      m &= __ballot_sync(0xFFFFFFFFu, valid && cand_less(c, thr));
+    }
+  }
+}
+
+template <int THREADS>
+__global__ void __launch_bounds__(THREADS) k_topk_warp(const SortItem* __restrict__ keys,
+                                                       const uint32_t* __restrict__ idx, const uint64_t* count,
+                                                       uint64_t n_max, int K, SortItem* __restrict__ out_keys,
+                                                       uint32_t* __restrict__ out_idx, uint64_t* out_count,
+                                                       int final_pass) {
+  constexpr int WARPS = THREADS / 32;
+  __shared__ Cand s_l[WARPS][32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint64_t n = count ? *count : n_max;
+  const uint64_t per = (n + gridDim.x - 1) / gridDim.x;
+  const uint64_t lo = (uint64_t)blockIdx.x * per;
+  const uint64_t hi = lo + per < n ? lo + per : n;
+  Cand L = cand_inf();
+  for (uint64_t base = lo + (uint64_t)warp * 32; base < hi; base += (uint64_t)THREADS) {
+    const uint64_t g = base + lane;
+    Cand c = cand_inf();
+    bool valid = g < hi;
+    if (valid) {
+      const SortItem k = keys[g];
+      c.w[0] = k.w[0]; c.w[1] = k.w[1]; c.w[2] = k.w[2]; c.w[3] = k.w[3];
+      c.ix = idx ? idx[g] : (uint32_t)g;
+      valid = c.ix != 0xFFFFFFFFu;  // padding of a previous pass
+    }
+    warp_offer(L, c, valid, K, lane);
+  }
+  s_l[warp][lane] = L;
+  __syncthreads();
+  if (warp == 0) {
+    for (int w = 1; w < WARPS; ++w) {
+      const Cand c = s_l[w][lane];
+      warp_offer(L, c, lane < K && c.ix != 0xFFFFFFFFu, K, lane);
+    }
+    if (final_pass) {
+      const uint32_t valid = __ballot_sync(0xFFFFFFFFu, lane < K && L.ix != 0xFFFFFFFFu);
+      if (lane < K && L.ix != 0xFFFFFFFFu) out_idx[lane] = L.ix;
+      if (lane == 0) *out_count = (uint64_t)__popc(valid);
+    } else if (lane < K) {
+      SortItem it;
+      it.w[0] = L.w[0]; it.w[1] = L.w[1]; it.w[2] = L.w[2]; it.w[3] = L.w[3];
+      out_keys[(uint64_t)blockIdx.x * K + lane] = it;
+      out_idx[(uint64_t)blockIdx.x * K + lane] = L.ix;
+    }
+  }
+}
+
 size_t topk_temp_bytes(uint64_t n_max, int k) {
   uint64_t ctas = (uint64_t)sms();
   const uint64_t want = (n_max + 4095) / 4096;
@@ -398,6 +501,16 @@ static cudaError_t topk_b(const SortItem* keys, const uint32_t* idx, const uint6
 cudaError_t launch_topk(const SortItem* keys, const uint32_t* idx, const uint64_t* count, uint64_t n_max, int k,
                         uint32_t* out_idx, uint64_t* out_count, void* temp, uint32_t* status, cudaStream_t s) {
   if (k <= 0 || k > 1024) return cudaErrorInvalidValue;
+  if (k <= 32) {
+    unsigned ctas = (unsigned)sms();
+    const uint64_t want = (n_max + 4095) / 4096;
+    if (want < ctas) ctas = (unsigned)(want ? want : 1);
+    SortItem* pk = (SortItem*)temp;
+    uint32_t* pi = (uint32_t*)(pk + (uint64_t)ctas * k);
+    k_topk_warp<256><<<ctas, 256, 0, s>>>(keys, idx, count, n_max, k, pk, pi, nullptr, 0);
+    k_topk_warp<256><<<1, 256, 0, s>>>(pk, pi, nullptr, (uint64_t)ctas * k, k, nullptr, out_idx, out_count, 1);
+    return cudaGetLastError();
+  }
   if (k <= 128) return topk_b<512>(keys, idx, count, n_max, k, out_idx, out_count, temp, s);
   return topk_b<2048>(keys, idx, count, n_max, k, out_idx, out_count, temp, s);
 }

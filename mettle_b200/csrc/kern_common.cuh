@@ -242,6 +242,67 @@ __device__ __forceinline__ Val vm_eval(const VmProg& p, const DCol* cols, const 
   return stack[0];
 }
 
+// vm_eval with column values prefetched in registers: cv[j] holds the value
+// of column sink_cols[j] for the current tuple (j < n_sink); columns outside
+// that set are loaded on demand.
+template <int NC>
+__device__ __forceinline__ Val vm_eval_c(const VmProg& p, const DCol* cols, const uint32_t* rid,
+                                         const int32_t* sink_cols, int n_sink, const int64_t* cv, uint32_t& st) {
+  Val stack[6];
+  int sp = 0;
+  for (int i = 0; i < p.n; ++i) {
+    const VmIns& in = p.ins[i];
+    switch (in.op) {
+      case VM_COL: {
+        const DCol& c = cols[in.arg];
+        int64_t bits = 0;
+        bool found = false;
+#pragma unroll
+        for (int j = 0; j < NC; ++j)
+          if (j < n_sink && sink_cols[j] == in.arg) {
+            bits = cv[j];
+            found = true;
+          }
+        if (!found) bits = load_bits(c.ptr, c.ptype, pick(rid, c.src));
+        Val v;
+        v.lo = bits;
+        v.hi = (c.ptype == P_I32 || c.ptype == P_I64) ? (bits >> 63) : 0;
+        stack[sp++] = v;
+        break;
+      }
+      case VM_CONST:
+        stack[sp].lo = in.k;
+        stack[sp].hi = in.k2;
+        ++sp;
+        break;
+      case VM_CAST:
+        stack[sp - 1] = vm_cast(stack[sp - 1], in.arg, in.type, in.k, in.k2, st);
+        break;
+      case VM_NEG: {
+        Val z{0, 0};
+        if (in.type == P_F32 || in.type == P_F64) {
+          stack[sp - 1].lo ^= (in.type == P_F32) ? (int64_t)0x80000000LL : (int64_t)0x8000000000000000ULL;
+        } else {
+          stack[sp - 1] = vm_arith(VM_SUB, in.type, z, stack[sp - 1], st);
+        }
+        break;
+      }
+      case VM_SLOT:
+        stack[sp].lo = 0;
+        stack[sp].hi = 0;
+        ++sp;
+        break;
+      default: {
+        Val b = stack[--sp];
+        Val a = stack[sp - 1];
+        stack[sp - 1] = vm_arith(in.op, in.type, a, b, st);
+        break;
+      }
+    }
+  }
+  return stack[0];
+}
+
 // Stores a VM result into a typed output array at index i.
 __device__ __forceinline__ void store_val(void* out, int32_t ptype, uint64_t i, Val v) {
   switch (ptype) {
@@ -353,6 +414,42 @@ __device__ __forceinline__ uint32_t block_excl_sum(uint32_t x, uint32_t* s_warp,
   *total = s_warp[THREADS / 32];
   __syncthreads();
   return r;
+}
+
+// ------------------------------------------------------------ bulk copies (TMA)
+// 1-D bulk global->shared copies completed on an mbarrier (no tensor map,
+// no multicast). Sizes and both addresses are multiples of 16 bytes.
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Bounded wait on an mbarrier phase; false when the limit is reached.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+  for (uint32_t i = 0; i < (1u << 20); ++i)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
 }
 
 // Multiplicative hash of a 64-bit word.

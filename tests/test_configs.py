@@ -81,9 +81,15 @@ def test_c2_filter_projection(scan_conn, col, op, sel):
     if op == "=":
         # equality: a value that occurs in the column
         v = d[col][12345]
-        lit = {"a": str(int(v)), "b": str(int(v)), "c": repr(float(v)),
-               "d": f"DATE '{W.day_to_iso(int(v))}'"}.get(col)
-        if col == "e":
+        if col in ("a", "b"):
+            lit = str(int(v))
+        elif col == "c":
+            # a DOUBLE literal (scientific notation) equal to the FLOAT value; a
+            # plain decimal literal is a DECIMAL, cast as (float)digits / (float)10^scale
+            lit = f"{float(v):.17e}"
+        elif col == "d":
+            lit = f"DATE '{W.day_to_iso(int(v))}'"
+        else:
             import datetime as dt
             t = dt.datetime(1970, 1, 1) + dt.timedelta(microseconds=int(v))
             lit = f"TIMESTAMP '{t.strftime('%Y-%m-%d %H:%M:%S.%f')}'"
