@@ -329,7 +329,10 @@ def run_mettle(args):
     conn.execute(f"CALL gpu_buffer_init('{gb} GB', '{gb} GB', pinned_memory_size = '{2 * gb} GB')")
     wl.register(conn, upload=True)
     stmt = conn.prepare(wl.sql)
-    stream = torch.cuda.current_stream()
+    # A dedicated (non-default) stream: the library enqueues on it and the
+    # CUDA events below are recorded on the same stream.
+    stream = torch.cuda.Stream(device=local)
+    torch.cuda.set_stream(stream)
     sp = stream.cuda_stream
 
     # parity of the measured statement (rank 0, once)

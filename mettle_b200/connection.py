@@ -340,7 +340,10 @@ class Connection:
                 raise MettleError(L.INVALID, "INSERT arity mismatch")
             for c, v in zip(t.columns, vals):
                 if c.array is not None:
-                    raise MettleError(L.INVALID, "INSERT into an array-backed table")
+                    # appending to a materialized column: back to python values
+                    c.values = ([c.dictionary[int(x)] for x in c.array] if c.type == L.T_VARCHAR
+                                else c.array.tolist())
+                    c.array = None
                 c.values.append(self._parse_value(v, c))
 
     # ------------------------------------------------------------ SQL surface

@@ -452,7 +452,7 @@ int mtl_stmt_launch(mtl_stmt* st, void* stream) {
     st->launched = true;
     if (st->constant) return;
     CKA(cudaEventRecord(st->e0, s));
-    run_program(st->ctx->c, *st->prog, s);
+    run_program_graph(st->ctx->c, *st->prog, s);
     CKA(cudaEventRecord(st->e1, s));
   });
 }

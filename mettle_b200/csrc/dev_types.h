@@ -99,7 +99,8 @@ struct DBuild {
   int32_t key_ptype;        // P_I32 or P_I64
   int64_t key_min;          // dense: first key
   uint64_t capacity;        // dense: key span; hash: slots
-  uint32_t* dense_map;      // dense: slot + 1, 0 = empty
+  uint32_t* dense_map;      // dense: slot + 1 (valid only where dense_bits is set)
+  uint32_t* dense_bits;     // dense: presence bitmap, one bit per key
   int64_t* hash_keys;       // hash: keys
   uint32_t* hash_slot;      // hash: slot + 1 per table entry
   uint32_t* hash_special;   // hash: slot + 1 of the key equal to kEmptyKey

@@ -248,6 +248,8 @@ struct Program {
   // per-step CUDA events (profiling on): ev[2i] before step i, ev[2i+1] after
   bool profile = false;
   std::vector<cudaEvent_t> prof_ev;
+  // the whole program captured once as a CUDA graph and replayed
+  cudaGraphExec_t graph = nullptr;
   ~Program();
 };
 
@@ -307,6 +309,7 @@ void column_distinct(Ctx& ctx, Table& t, Column& c);
 // planning / execution (exec.cpp)
 std::unique_ptr<Program> compile(Ctx& ctx, const BoundPlan& plan);
 void run_program(Ctx& ctx, Program& p, cudaStream_t s);
+void run_program_graph(Ctx& ctx, Program& p, cudaStream_t s);
 std::shared_ptr<Result> fetch_program(Ctx& ctx, Program& p, cudaStream_t s);
 void free_program(Ctx& ctx, Program& p);
 std::shared_ptr<Result> constant_result(const BoundPlan& plan);

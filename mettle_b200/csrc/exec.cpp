@@ -296,21 +296,37 @@ struct Compiler {
     P.scratch_bytes += (bytes + 255) & ~255ULL;
     return p;
   }
+  // Scratch initialization is collected and emitted as one fill launch at
+  // the start of the program (arena blocks are 256-byte aligned and sized in
+  // 256-byte units, so rounding a segment up to 16 bytes stays in its block).
+  std::vector<FillSeg> fills;
   void memset_step(void* p, int byte, uint64_t bytes) {
-    Step s;
-    s.k = Step::MEMSET;
-    s.ptr = p;
-    s.byte = byte;
-    s.bytes = bytes;
-    P.steps.push_back(s);
+    FillSeg f;
+    f.ptr = p;
+    f.bytes = (bytes + 15) & ~15ULL;
+    f.pattern = 0x0101010101010101ULL * (uint64_t)(byte & 0xFF);
+    fills.push_back(f);
   }
   void fill_step(void* p, uint64_t words, uint64_t v) {
+    FillSeg f;
+    f.ptr = p;
+    f.bytes = (words * 8 + 15) & ~15ULL;
+    f.pattern = v;
+    fills.push_back(f);
+  }
+  void emit_fills() {
+    if (fills.empty()) return;
+    FillSeg* dev = (FillSeg*)scratch(fills.size() * sizeof(FillSeg));
+    CK(cudaMemcpy(dev, fills.data(), fills.size() * sizeof(FillSeg), cudaMemcpyHostToDevice));
+    uint64_t mx = 0;
+    for (auto& f : fills) mx = std::max(mx, f.bytes);
     Step s;
     s.k = Step::FILL;
-    s.ptr = p;
-    s.bytes = words;
-    s.fill = v;
-    P.steps.push_back(s);
+    s.ptr = dev;
+    s.byte = (int)fills.size();
+    s.bytes = mx;
+    s.name = "init_scratch";
+    P.steps.insert(P.steps.begin(), s);
     P.kernels += 1;
   }
 
@@ -528,8 +544,11 @@ struct Compiler {
       b.kind = B_DENSE;
       if (rows) b.key_min = k.vmin;
       b.capacity = span;
+      // the slot map is read only where its presence bit is set, so only the
+      // bitmap (span / 8 bytes) is cleared per query
       b.dense_map = (uint32_t*)scratch(span * 4);
-      memset_step(b.dense_map, 0, span * 4);
+      b.dense_bits = (uint32_t*)scratch(((span + 31) / 32) * 4);
+      memset_step(b.dense_bits, 0, ((span + 31) / 32) * 4);
     } else {
       b.kind = B_HASH;
       b.capacity = std::max<uint64_t>(64, 2 * rows);
@@ -974,7 +993,7 @@ struct Compiler {
       else if (rep_src >= 0) groups = std::max<uint64_t>(1, plan.sources[rep_src].table->rows);
       else {
         est_groups = estimate_groups();
-        groups = std::max<uint64_t>(1024, est_groups * 2);
+        groups = std::max<uint64_t>(64, est_groups * 2);
       }
       plan_states(groups, root_rows, scalar);
     }
@@ -1271,6 +1290,7 @@ std::unique_ptr<Program> compile(Ctx& ctx, const BoundPlan& plan) {
   Compiler c{ctx, plan, *P};
   try {
     c.compile();
+    c.emit_fills();
   } catch (...) {
     for (void* b : P->blocks) ctx.arena.free(b);
     P->blocks.clear();
@@ -1297,6 +1317,44 @@ void free_program(Ctx& ctx, Program& p) {
 // ------------------------------------------------------------ run
 Program::~Program() {
   for (cudaEvent_t e : prof_ev) cudaEventDestroy(e);
+  if (graph) cudaGraphExecDestroy(graph);
+}
+
+// Replays the program as one CUDA graph (captured on first use). Falls back
+// to direct launches when the stream cannot be captured (the legacy default
+// stream) or when per-step profiling is on.
+void run_program_graph(Ctx& ctx, Program& p, cudaStream_t s) {
+  static const bool disabled = std::getenv("METTLE_NO_GRAPH") != nullptr;
+  if (p.profile || disabled || s == nullptr || s == cudaStreamLegacy || s == cudaStreamPerThread) {
+    run_program(ctx, p, s);
+    return;
+  }
+  if (!p.graph) {
+    cudaGraph_t g = nullptr;
+    if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+      cudaGetLastError();
+      run_program(ctx, p, s);
+      return;
+    }
+    try {
+      run_program(ctx, p, s);
+    } catch (...) {
+      cudaStreamEndCapture(s, &g);
+      if (g) cudaGraphDestroy(g);
+      cudaGetLastError();
+      throw;
+    }
+    CK(cudaStreamEndCapture(s, &g));
+    cudaError_t e = cudaGraphInstantiate(&p.graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      p.graph = nullptr;
+      run_program(ctx, p, s);
+      return;
+    }
+  }
+  CK(cudaGraphLaunch(p.graph, s));
 }
 
 static const char* step_kind_name(Step::Kind k) {
@@ -1328,7 +1386,7 @@ void run_program(Ctx& ctx, Program& p, cudaStream_t s) {
     if (p.profile) CK(cudaEventRecord(p.prof_ev[2 * i], s));
     switch (st.k) {
       case Step::MEMSET: CK(cudaMemsetAsync(st.ptr, st.byte, st.bytes, s)); break;
-      case Step::FILL: CK(launch_fill_u64((uint64_t*)st.ptr, st.bytes, st.fill, s)); break;
+      case Step::FILL: CK(launch_fill_segments((const FillSeg*)st.ptr, st.byte, st.bytes, s)); break;
       case Step::PIPELINE: CK(launch_pipeline(st.pipe, st.n_hint, s)); break;
       case Step::COMPACT_FLAGS:
         CK(launch_compact_flags((const uint8_t*)st.flag, st.n, st.n_dev, st.out_idx, st.out_count, st.tstatus,

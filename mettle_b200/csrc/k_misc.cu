@@ -381,4 +381,20 @@ cudaError_t launch_fill_u64(uint64_t* p, uint64_t n, uint64_t v, cudaStream_t s)
   return cudaGetLastError();
 }
 
+__global__ void k_fill_segments(const FillSeg* __restrict__ segs) {
+  const FillSeg sg = segs[blockIdx.y];
+  const uint64_t n16 = sg.bytes / 16;
+  const ulonglong2 v = make_ulonglong2(sg.pattern, sg.pattern);
+  ulonglong2* p = (ulonglong2*)sg.ptr;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n16; i += (uint64_t)gridDim.x * blockDim.x)
+    p[i] = v;
+}
+
+cudaError_t launch_fill_segments(const FillSeg* segs_dev, int n_segs, uint64_t max_bytes, cudaStream_t s) {
+  if (n_segs <= 0) return cudaSuccess;
+  dim3 grid(grid_for(max_bytes / 16, 256, 4), (unsigned)n_segs);
+  k_fill_segments<<<grid, 256, 0, s>>>(segs_dev);
+  return cudaGetLastError();
+}
+
 }  // namespace mtl

@@ -18,6 +18,9 @@
 //     shared-memory tables when the group count is small.
 #include <cooperative_groups.h>
 
+#include <map>
+#include <mutex>
+
 #include "kern_common.cuh"
 #include "kernels.h"
 
@@ -30,9 +33,8 @@ __device__ __forceinline__ bool build_lookup(const DBuild& b, int64_t key, uint3
   if (b.kind == B_DENSE) {
     uint64_t k = (uint64_t)(key - b.key_min);
     if (k >= b.capacity) return false;
-    uint32_t v = b.dense_map[k];
-    if (v == 0) return false;
-    slot = v - 1;
+    if (!((b.dense_bits[k >> 5] >> (k & 31)) & 1u)) return false;
+    slot = b.dense_map[k] - 1;
     return true;
   }
   if (key == kEmptyKey) {
@@ -62,7 +64,11 @@ __device__ __forceinline__ void build_insert(const DBuild& b, int64_t key, uint3
       st |= ST_CAPACITY;
       return;
     }
-    if (atomicCAS(b.dense_map + k, 0u, slot + 1) != 0u) st |= ST_DUP_BUILD_KEY;
+    // The map entry is written before its presence bit; probes run in a later
+    // launch, so the plain store is visible to them.
+    b.dense_map[k] = slot + 1;
+    const uint32_t bit = 1u << (k & 31);
+    if (atomicOr(b.dense_bits + (k >> 5), bit) & bit) st |= ST_DUP_BUILD_KEY;
     return;
   }
   if (key == kEmptyKey) {
@@ -271,11 +277,7 @@ __device__ __forceinline__ int smem_agg_find(const PipeDesc& d, SmemAgg& s, cons
 
 // ------------------------------------------------------------ the kernel
 constexpr int kThreads = 256;
-constexpr int kItems = 8;
-constexpr int kTile = kThreads * kItems;  // tuples per tile
-constexpr int kBatch = 4;                 // tuples a thread advances through the ops together
-constexpr int kAggCols = 4;               // sink columns fetched ahead in phase A
-constexpr int kOutCols = 6;               // output columns fetched ahead in the write phase
+constexpr int kTile = 2048;  // tuples per tile
 
 struct StreamLayout {
   int n;
@@ -291,20 +293,151 @@ __host__ __device__ inline uint32_t stream_bytes_per_row(const PipeDesc& d) {
   return w;
 }
 
-// SINK is a compile-time constant so each instantiation carries only its own
-// sink code. Tiles: tuple ti of a tile is handled by thread ti % 256 (striped),
-// which keeps shared-memory reads conflict free. The streamed columns of the
-// next tile are copied into the idle shared buffer by one thread with bulk
-// (TMA) copies while the CTA works on the current tile. Other columns are
-// read for a batch of kBatch tuples at once so their loads overlap.
+// Row ids of sources other than the driving one, per tile row, live in shared
+// arrays filled by the probes; `slot_of_src` packs each source's array index
+// (4 bits, 0xF = none).
+struct TileCtx {
+  const PipeDesc* d;
+  const StreamLayout* S;
+  const uint8_t* buf;  // streamed columns of this tile
+  uint64_t base;       // first row of the tile
+  uint32_t* srid;      // [nq][kTile] row ids of probed sources
+  uint32_t slot_of_src;
+};
+
+__device__ __forceinline__ uint32_t tc_rid(const TileCtx& t, int src, uint32_t r) {
+  if (src == t.d->drive_src) return (uint32_t)(t.base + r);
+  const uint32_t q = (t.slot_of_src >> (4 * src)) & 0xFu;
+  return t.srid[(size_t)q * kTile + r];
+}
+
+__device__ __forceinline__ int stream_index(const StreamLayout& S, int col) {
+  int k = -1;
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+    if (i < S.n && S.col[i] == col) k = i;
+  return k;
+}
+
+__device__ __forceinline__ int64_t stream_value(const StreamLayout& S, const uint8_t* buf, int k, int32_t ptype,
+                                                uint32_t r) {
+  if (S.width[k] == 4)
+    return ptype == P_I32 ? (int64_t)((const int32_t*)(buf + S.off[k]))[r]
+                          : (int64_t)((const uint32_t*)(buf + S.off[k]))[r];
+  return ((const int64_t*)(buf + S.off[k]))[r];
+}
+
+__device__ __forceinline__ int64_t tc_get(const TileCtx& t, int col, uint32_t r) {
+  const DCol& c = t.d->cols[col];
+  if (c.src == t.d->drive_src) {
+    const int k = stream_index(*t.S, col);
+    if (k >= 0) return stream_value(*t.S, t.buf, k, c.ptype, r);
+  }
+  return load_bits(c.ptr, c.ptype, tc_rid(t, c.src, r));
+}
+
+// Expression VM over one tile row.
+__device__ Val vm_eval_t(const VmProg& p, const TileCtx& t, uint32_t r, uint32_t& st) {
+  Val stack[6];
+  int sp = 0;
+  for (int i = 0; i < p.n; ++i) {
+    const VmIns& in = p.ins[i];
+    switch (in.op) {
+      case VM_COL: {
+        const int32_t pt = t.d->cols[in.arg].ptype;
+        Val v;
+        v.lo = tc_get(t, in.arg, r);
+        v.hi = (pt == P_I32 || pt == P_I64) ? (v.lo >> 63) : 0;
+        stack[sp++] = v;
+        break;
+      }
+      case VM_CONST:
+        stack[sp].lo = in.k;
+        stack[sp].hi = in.k2;
+        ++sp;
+        break;
+      case VM_CAST:
+        stack[sp - 1] = vm_cast(stack[sp - 1], in.arg, in.type, in.k, in.k2, st);
+        break;
+      case VM_NEG: {
+        Val z{0, 0};
+        if (in.type == P_F32 || in.type == P_F64)
+          stack[sp - 1].lo ^= (in.type == P_F32) ? (int64_t)0x80000000LL : (int64_t)0x8000000000000000ULL;
+        else
+          stack[sp - 1] = vm_arith(VM_SUB, in.type, z, stack[sp - 1], st);
+        break;
+      }
+      case VM_SLOT:
+        stack[sp].lo = 0;
+        stack[sp].hi = 0;
+        ++sp;
+        break;
+      default: {
+        Val b = stack[--sp];
+        Val a = stack[sp - 1];
+        stack[sp - 1] = vm_arith(in.op, in.type, a, b, st);
+        break;
+      }
+    }
+  }
+  return stack[0];
+}
+
+// Warp-aggregated append of tile row r to a shared selection list. Every
+// lane of the warp must call it (keep may be false).
+__device__ __forceinline__ void sel_push(bool keep, uint32_t r, uint16_t* out, uint32_t* cnt) {
+  const uint32_t m = __ballot_sync(0xFFFFFFFFu, keep);
+  const int lane = threadIdx.x & 31;
+  uint32_t base = 0;
+  if (lane == 0 && m) base = atomicAdd(cnt, (uint32_t)__popc(m));
+  base = __shfl_sync(0xFFFFFFFFu, base, 0);
+  if (keep) out[base + __popc(m & ((1u << lane) - 1u))] = (uint16_t)r;
+}
+
+// Integer predicates are evaluated as a closed interval [lo, hi] (negated for
+// <>), so the row loop carries no op dispatch.
+struct IntRange {
+  int64_t lo, hi;
+  bool neg, none;
+};
+__device__ __forceinline__ IntRange to_range(const DPred& p) {
+  IntRange r{INT64_MIN, INT64_MAX, false, false};
+  switch (p.op) {
+    case C_EQ: r.lo = r.hi = p.ilit; break;
+    case C_NE: r.lo = r.hi = p.ilit; r.neg = true; break;
+    case C_LT: if (p.ilit == INT64_MIN) r.none = true; else r.hi = p.ilit - 1; break;
+    case C_LE: r.hi = p.ilit; break;
+    case C_GT: if (p.ilit == INT64_MAX) r.none = true; else r.lo = p.ilit + 1; break;
+    case C_GE: r.lo = p.ilit; break;
+    case C_FALSE: r.none = true; break;
+    default: break;
+  }
+  return r;
+}
+
+// Filter op over the current selection: one loop per (column type, source),
+// chosen once per tile.
+template <typename GET>
+__device__ __forceinline__ void filter_loop(uint32_t n_sel, bool ident, const uint16_t* in, uint16_t* out,
+                                            uint32_t* cnt, GET get_keep) {
+  for (uint32_t i0 = 0; i0 < n_sel; i0 += kThreads) {
+    const uint32_t i = i0 + threadIdx.x;
+    const bool act = i < n_sel;
+    const uint32_t r = act ? (ident ? i : (uint32_t)in[i]) : 0u;
+    const bool keep = act && get_keep(r);
+    sel_push(keep, r, out, cnt);
+  }
+}
+
 template <int SINK>
 __global__ void __launch_bounds__(kThreads) k_pipeline(const __grid_constant__ PipeDesc d) {
-  constexpr int THREADS = kThreads, ITEMS = kItems, TILE = kTile;
+  constexpr int THREADS = kThreads, TILE = kTile;
   extern __shared__ __align__(128) uint8_t smem[];
   __shared__ __align__(8) uint64_t s_mbar[2];
   __shared__ uint32_t s_warp[THREADS / 32 + 1];
   __shared__ uint64_t s_base;
   __shared__ uint64_t s_tile[2];
+  __shared__ uint32_t s_cnt[3];
   __shared__ uint64_t s_red[SINK == SK_AGG_SCALAR ? kMaxAggs : 1][THREADS / 32];
   __shared__ int64_t s_redhi[SINK == SK_AGG_SCALAR ? kMaxAggs : 1][THREADS / 32];
 
@@ -314,7 +447,7 @@ __global__ void __launch_bounds__(kThreads) k_pipeline(const __grid_constant__ P
   uint32_t st = 0;
 
   StreamLayout S;
-  S.n = d.tuple_input ? 0 : (d.n_stream < 4 ? d.n_stream : 4);
+  S.n = d.n_stream < 4 ? d.n_stream : 4;
   {
     uint32_t off = 0;
 #pragma unroll
@@ -326,23 +459,29 @@ __global__ void __launch_bounds__(kThreads) k_pipeline(const __grid_constant__ P
     }
     S.bytes = off;
   }
-  uint8_t* const sbuf0 = smem;
-  uint8_t* const sbuf1 = smem + S.bytes;
-  uint8_t* const sink_smem = smem + 2 * S.bytes;
-
-  // MATERIALIZE shared memory: keep flags | compacted tile list | row ids
-  uint8_t* s_keep = sink_smem;
-  uint16_t* s_list = (uint16_t*)(sink_smem + TILE);
-  uint32_t* s_rid = (uint32_t*)(sink_smem + 3 * TILE);
-  int rid_slot[kMaxSrc];
-  {
-    int q = 0;
-#pragma unroll
-    for (int s = 0; s < kMaxSrc; ++s) {
-      bool implicit = !d.tuple_input && s == d.drive_src;
-      rid_slot[s] = ((d.mat_src_mask >> s) & 1u) && !implicit ? q++ : -1;
+  // probed sources whose row ids are kept per tile row
+  uint32_t slot_of_src = 0xFFFFFFFFu;
+  int nq = 0;
+  for (int s = 0; s < kMaxSrc; ++s) {
+    if (s == d.drive_src) continue;
+    bool used = false;
+    for (int p = 0; p < d.n_probes; ++p) used |= ((d.probes[p].fill_mask >> s) & 1u) != 0;
+    if (used) {
+      slot_of_src = (slot_of_src & ~(0xFu << (4 * s))) | ((uint32_t)nq << (4 * s));
+      ++nq;
     }
   }
+  // shared layout: stream buffers x2 | sel A | sel B | slot | rid arrays | sink
+  uint8_t* const sbuf0 = smem;
+  uint8_t* const sbuf1 = smem + S.bytes;
+  uint16_t* const selA = (uint16_t*)(smem + 2 * S.bytes);
+  uint16_t* const selB = selA + TILE;
+  uint32_t* const s_slot = (uint32_t*)(selB + TILE);
+  uint32_t* const s_srid = s_slot + TILE;
+  uint8_t* const sink_smem = (uint8_t*)(s_srid + (size_t)nq * TILE);
+  uint8_t* s_keep = sink_smem;                       // MATERIALIZE
+  uint16_t* s_list = (uint16_t*)(sink_smem + TILE);  // MATERIALIZE
+
   SmemAgg sagg;
   if (SINK == SK_AGG_SMEM) smem_agg_init(d, sagg, sink_smem);
   uint64_t plo[SINK == SK_AGG_SCALAR ? kMaxAggs : 1];
@@ -363,10 +502,13 @@ __global__ void __launch_bounds__(kThreads) k_pipeline(const __grid_constant__ P
       phi[a] = 0;
     }
   }
-  if (tid == 0 && S.n) {
-    mbar_init(&s_mbar[0], 1);
-    mbar_init(&s_mbar[1], 1);
-    mbar_fence_init();
+  if (tid == 0) {
+    if (S.n) {
+      mbar_init(&s_mbar[0], 1);
+      mbar_init(&s_mbar[1], 1);
+      mbar_fence_init();
+    }
+    s_cnt[0] = s_cnt[1] = s_cnt[2] = 0;
   }
 
   const bool dynamic_tiles = SINK == SK_MATERIALIZE;
@@ -377,11 +519,9 @@ __global__ void __launch_bounds__(kThreads) k_pipeline(const __grid_constant__ P
     uint8_t* dst = b ? sbuf1 : sbuf0;
     fence_proxy_async();
     mbar_arrive_expect_tx(&s_mbar[b], S.bytes);
-#pragma unroll
-    for (int i = 0; i < 4; ++i)
-      if (i < S.n)
-        bulk_g2s(dst + S.off[i], (const uint8_t*)d.cols[S.col[i]].ptr + base * (uint64_t)S.width[i],
-                 (uint32_t)TILE * (uint32_t)S.width[i], &s_mbar[b]);
+    for (int i = 0; i < S.n; ++i)
+      bulk_g2s(dst + S.off[i], (const uint8_t*)d.cols[S.col[i]].ptr + base * (uint64_t)S.width[i],
+               (uint32_t)TILE * (uint32_t)S.width[i], &s_mbar[b]);
   };
 
   if (tid == 0) s_tile[0] = dynamic_tiles ? (uint64_t)atomicAdd(d.tile_counter, 1u) : (uint64_t)blockIdx.x;
@@ -391,28 +531,27 @@ __global__ void __launch_bounds__(kThreads) k_pipeline(const __grid_constant__ P
   uint32_t parity = 0;
   int b = 0;
   uint32_t k = 0;
+  uint32_t cq = 0;  // selection-counter rotation
   while (cur < n_tiles) {
-    // Claim the next tile and start its copies before waiting on this one.
-    uint64_t nxt_static = cur + gridDim.x;
     if (tid == 0) {
-      uint64_t nx = dynamic_tiles ? (uint64_t)atomicAdd(d.tile_counter, 1u) : nxt_static;
+      const uint64_t nx = dynamic_tiles ? (uint64_t)atomicAdd(d.tile_counter, 1u) : cur + gridDim.x;
       s_tile[(k + 1) & 1] = nx;
       if (S.n && nx < n_tiles) issue(nx, b ^ 1);
     }
     const uint64_t tile = cur;
     const uint64_t tile_base = tile * (uint64_t)TILE;
+    const uint32_t nrow = (uint32_t)(n - tile_base < (uint64_t)TILE ? n - tile_base : (uint64_t)TILE);
     uint8_t* const buf = b ? sbuf1 : sbuf0;
     if (S.n) {
       bool ok = true;
-      if (tile_base + TILE <= n) {
+      if (nrow == TILE) {
         ok = mbar_wait(&s_mbar[b], (parity >> b) & 1u);
         parity ^= 1u << b;
       } else {
         for (int i = 0; i < S.n; ++i) {
           const DCol& c = d.cols[S.col[i]];
           for (int r = tid; r < TILE; r += THREADS) {
-            const uint64_t g = tile_base + r;
-            int64_t v = g < n ? load_bits(c.ptr, c.ptype, g) : 0;
+            int64_t v = (uint32_t)r < nrow ? load_bits(c.ptr, c.ptype, tile_base + r) : 0;
             if (S.width[i] == 4) ((uint32_t*)(buf + S.off[i]))[r] = (uint32_t)v;
             else ((int64_t*)(buf + S.off[i]))[r] = v;
           }
@@ -420,259 +559,112 @@ __global__ void __launch_bounds__(kThreads) k_pipeline(const __grid_constant__ P
       }
       if (__syncthreads_or(!ok)) {
         st |= ST_SPIN_LIMIT;
-        // give the copies still in flight a bounded chance to land, then stop
+        // give the copy still in flight a bounded chance to land, then stop
         mbar_wait(&s_mbar[b ^ 1], (parity >> (b ^ 1)) & 1u);
         break;
       }
     }
+    TileCtx tc{&d, &S, buf, tile_base, s_srid, slot_of_src};
 
-    // Value of column `col` for a tuple: shared memory when it is a streamed
-    // column of the driving table, else a global load.
-    auto fetch = [&](int col, uint32_t rowid, uint32_t ti) -> int64_t {
-#pragma unroll
-      for (int i = 0; i < 4; ++i)
-        if (i < S.n && S.col[i] == col) {
-          if (S.width[i] == 4)
-            return d.cols[col].ptype == P_I32 ? (int64_t)((const int32_t*)(buf + S.off[i]))[ti]
-                                              : (int64_t)((const uint32_t*)(buf + S.off[i]))[ti];
-          return ((const int64_t*)(buf + S.off[i]))[ti];
-        }
-      const DCol& c = d.cols[col];
-      return load_bits(c.ptr, c.ptype, rowid);
-    };
-
-    uint32_t alive = 0;
-#pragma unroll
-    for (int it = 0; it < ITEMS; ++it) alive |= (tile_base + (uint64_t)it * THREADS + tid < n ? 1u : 0u) << it;
-
-    // Phase A: ops and sink, kBatch tuples at a time.
-#pragma unroll 1
-    for (int h = 0; h < ITEMS / kBatch; ++h) {
-      uint32_t am = (alive >> (h * kBatch)) & ((1u << kBatch) - 1u);
-      uint32_t rid[kBatch][kMaxSrc];
-      uint32_t gslot[kBatch];
-      uint32_t ti[kBatch];
-#pragma unroll
-      for (int bb = 0; bb < kBatch; ++bb) {
-        ti[bb] = (uint32_t)((h * kBatch + bb) * THREADS + tid);
-        gslot[bb] = 0;
-#pragma unroll
-        for (int s = 0; s < kMaxSrc; ++s)
-          rid[bb][s] = (!d.tuple_input && s == d.drive_src) ? (uint32_t)(tile_base + ti[bb]) : 0u;
-      }
-      if (d.tuple_input) {
-#pragma unroll
-        for (int s = 0; s < kMaxSrc; ++s)
-          if ((d.src_mask >> s) & 1u) {
-#pragma unroll
-            for (int bb = 0; bb < kBatch; ++bb)
-              if ((am >> bb) & 1u) rid[bb][s] = d.in_rids[s][tile_base + ti[bb]];
-          }
-      }
-      for (int o = 0; o < d.n_ops && am; ++o) {
-        const PipeOp op = d.ops[o];
-        if (op.kind == OPK_FILTER) {
-          const DPred& p = d.preds[op.idx];
-          const DCol& c = d.cols[p.col];
-          int64_t v[kBatch];
-#pragma unroll
-          for (int bb = 0; bb < kBatch; ++bb)
-            v[bb] = ((am >> bb) & 1u) ? fetch(p.col, pick(rid[bb], c.src), ti[bb]) : 0;
-#pragma unroll
-          for (int bb = 0; bb < kBatch; ++bb)
-            if (((am >> bb) & 1u) && !eval_pred_bits(v[bb], c.ptype, p)) am &= ~(1u << bb);
-        } else {
-          const DProbe& pr = d.probes[op.idx];
-          const DCol& c = d.cols[pr.key_col];
-          const DBuild& bd = d.builds[pr.build];
-          int64_t key[kBatch];
-          uint32_t sl[kBatch];
-#pragma unroll
-          for (int bb = 0; bb < kBatch; ++bb)
-            key[bb] = ((am >> bb) & 1u) ? fetch(pr.key_col, pick(rid[bb], c.src), ti[bb]) : 0;
-          if (bd.kind == B_DENSE) {
-            uint32_t m[kBatch];
-#pragma unroll
-            for (int bb = 0; bb < kBatch; ++bb) {
-              const uint64_t kk = (uint64_t)(key[bb] - bd.key_min);
-              m[bb] = (((am >> bb) & 1u) && kk < bd.capacity) ? bd.dense_map[kk] : 0u;
-            }
-#pragma unroll
-            for (int bb = 0; bb < kBatch; ++bb) {
-              if (m[bb] == 0u) am &= ~(1u << bb);
-              sl[bb] = m[bb] - 1u;
-            }
+    // ---- ops over the selection vector
+    uint32_t n_sel = nrow;
+    bool ident = true;
+    uint16_t* sel_in = selA;
+    uint16_t* sel_out = selB;
+    for (int o = 0; o < d.n_ops && n_sel > 0; ++o) {
+      uint32_t* cnt = &s_cnt[cq];
+      if (tid == 0) s_cnt[(cq + 1) % 3] = 0;  // next op's counter (last read two barriers ago)
+      const PipeOp op = d.ops[o];
+      if (op.kind == OPK_FILTER) {
+        const DPred& p = d.preds[op.idx];
+        const DCol& c = d.cols[p.col];
+        const int si = (c.src == d.drive_src) ? stream_index(S, p.col) : -1;
+        if (c.ptype == P_I32 || c.ptype == P_I64) {
+          const IntRange rg = to_range(p);
+          if (rg.none) {
+            filter_loop(n_sel, ident, sel_in, sel_out, cnt, [&](uint32_t) { return false; });
+          } else if (si >= 0 && S.width[si] == 4) {
+            const int32_t* col = (const int32_t*)(buf + S.off[si]);
+            filter_loop(n_sel, ident, sel_in, sel_out, cnt, [&](uint32_t r) {
+              const int64_t x = col[r];
+              return (x >= rg.lo && x <= rg.hi) != rg.neg;
+            });
+          } else if (si >= 0) {
+            const int64_t* col = (const int64_t*)(buf + S.off[si]);
+            filter_loop(n_sel, ident, sel_in, sel_out, cnt, [&](uint32_t r) {
+              const int64_t x = col[r];
+              return (x >= rg.lo && x <= rg.hi) != rg.neg;
+            });
           } else {
-#pragma unroll
-            for (int bb = 0; bb < kBatch; ++bb) {
-              uint32_t s_ = 0;
-              if (((am >> bb) & 1u) && !build_lookup(bd, key[bb], s_, st)) am &= ~(1u << bb);
-              sl[bb] = s_;
+            filter_loop(n_sel, ident, sel_in, sel_out, cnt, [&](uint32_t r) {
+              const int64_t x = load_bits(c.ptr, c.ptype, tc_rid(tc, c.src, r));
+              return (x >= rg.lo && x <= rg.hi) != rg.neg;
+            });
+          }
+        } else {
+          filter_loop(n_sel, ident, sel_in, sel_out, cnt, [&](uint32_t r) {
+            return eval_pred_bits(tc_get(tc, p.col, r), c.ptype, p);
+          });
+        }
+      } else {
+        const DProbe& pr = d.probes[op.idx];
+        const DCol& c = d.cols[pr.key_col];
+        const DBuild& bd = d.builds[pr.build];
+        const bool want_slot = op.idx == d.slot_probe;
+        const uint32_t fill = pr.fill_mask & ~(1u << d.drive_src);
+        for (uint32_t i0 = 0; i0 < n_sel; i0 += THREADS) {
+          const uint32_t i = i0 + tid;
+          const bool act = i < n_sel;
+          const uint32_t r = act ? (ident ? i : (uint32_t)sel_in[i]) : 0u;
+          bool keep = false;
+          uint32_t slot = 0;
+          if (act) {
+            const int64_t key = tc_get(tc, pr.key_col, r);
+            if (bd.kind == B_DENSE) {
+              const uint64_t kk = (uint64_t)(key - bd.key_min);
+              if (kk < bd.capacity && ((bd.dense_bits[kk >> 5] >> (kk & 31)) & 1u)) {
+                keep = true;
+                slot = bd.dense_map[kk] - 1u;
+              }
+            } else {
+              keep = build_lookup(bd, key, slot, st);
+            }
+            if (keep) {
+              if (want_slot) s_slot[r] = slot;
+              for (int s = 0; s < kMaxSrc; ++s)
+                if ((fill >> s) & 1u)
+                  s_srid[(size_t)((slot_of_src >> (4 * s)) & 0xFu) * TILE + r] = bd.payload[s][slot];
             }
           }
-          if (op.idx == d.slot_probe) {
-#pragma unroll
-            for (int bb = 0; bb < kBatch; ++bb) gslot[bb] = sl[bb];
-          }
-#pragma unroll
-          for (int s = 0; s < kMaxSrc; ++s)
-            if ((pr.fill_mask >> s) & 1u) {
-#pragma unroll
-              for (int bb = 0; bb < kBatch; ++bb)
-                if ((am >> bb) & 1u) rid[bb][s] = bd.payload[s][sl[bb]];
-            }
+          (void)c;
+          sel_push(keep, r, sel_out, cnt);
         }
       }
-
-      if (SINK == SK_MATERIALIZE) {
-#pragma unroll
-        for (int bb = 0; bb < kBatch; ++bb) {
-          const bool keep = (am >> bb) & 1u;
-          s_keep[ti[bb]] = keep ? 1 : 0;
-          if (keep) {
-#pragma unroll
-            for (int s = 0; s < kMaxSrc; ++s)
-              if (rid_slot[s] >= 0) s_rid[(size_t)rid_slot[s] * TILE + ti[bb]] = rid[bb][s];
-          }
-        }
-        continue;
-      }
-      if (!am) continue;
-
-      // Fetch the sink's columns for the whole batch, then run the sink.
-      int64_t cv[kBatch][kAggCols];
-#pragma unroll
-      for (int jc = 0; jc < kAggCols; ++jc) {
-        const bool use = jc < d.n_sink_cols;
-        const int col = use ? d.sink_cols[jc] : 0;
-        const int src = d.cols[col].src;
-#pragma unroll
-        for (int bb = 0; bb < kBatch; ++bb)
-          cv[bb][jc] = (use && ((am >> bb) & 1u)) ? fetch(col, pick(rid[bb], src), ti[bb]) : 0;
-      }
-#pragma unroll
-      for (int bb = 0; bb < kBatch; ++bb) {
-        if (!((am >> bb) & 1u)) continue;
-        switch (SINK) {
-          case SK_BUILD: {
-            const DBuild& bd = d.builds[d.sink_build];
-            cg::coalesced_group g = cg::coalesced_threads();
-            uint32_t base = 0;
-            if (g.thread_rank() == 0) base = atomicAdd(bd.n_slots, g.size());
-            base = g.shfl(base, 0);
-            const uint32_t slot = base + g.thread_rank();
-            const int64_t key = (d.n_sink_cols > 0 && d.sink_cols[0] == d.build_key_col)
-                                    ? cv[bb][0]
-                                    : fetch(d.build_key_col, pick(rid[bb], d.cols[d.build_key_col].src), ti[bb]);
-#pragma unroll
-            for (int s = 0; s < kMaxSrc; ++s)
-              if ((d.build_payload_mask >> s) & 1u) bd.payload[s][slot] = rid[bb][s];
-            // A representative-row aggregate downstream keeps its states by
-            // this slot: initialize them here so no memset of the (build
-            // table sized) state arrays is needed per query.
-            for (int a = 0; a < d.n_aggs; ++a) agg_init_global(d.aggs[a], slot);
-            if (d.slot_hit) d.slot_hit[slot] = 0;
-            build_insert(bd, key, slot, st);
-            break;
-          }
-          case SK_AGG_SLOT: {
-            const uint32_t g = gslot[bb];
-            d.slot_hit[g] = 1;
-            for (int a = 0; a < d.n_aggs; ++a) {
-              const DAgg& ag = d.aggs[a];
-              Val v{0, 0};
-              int32_t vt = P_I64;
-              if (ag.prog >= 0) {
-                v = vm_eval_c<kAggCols>(d.progs[ag.prog], d.cols, rid[bb], d.sink_cols, d.n_sink_cols, cv[bb], st);
-                vt = d.progs[ag.prog].out_type;
-              }
-              agg_apply(ag.fn, (unsigned long long*)(ag.lo + g), (long long*)(ag.hi ? ag.hi + g : nullptr), v, vt);
-            }
-            break;
-          }
-          case SK_AGG_HASH:
-          case SK_AGG_SMEM: {
-            uint64_t kw[kMaxKeys];
-#pragma unroll
-            for (int i = 0; i < kMaxKeys; ++i)
-              kw[i] = i < d.table.n_keys
-                          ? (uint64_t)vm_eval_c<kAggCols>(d.progs[d.key_prog[i]], d.cols, rid[bb], d.sink_cols,
-                                                          d.n_sink_cols, cv[bb], st).lo
-                          : 0;
-            int sidx = -1;
-            if (SINK == SK_AGG_SMEM) sidx = smem_agg_find(d, sagg, kw, st);
-            uint64_t g = d.table.capacity;
-            if (sidx < 0) g = agg_find_global(d, kw, st);
-            if (sidx < 0 && g >= d.table.capacity) break;
-            for (int a = 0; a < d.n_aggs; ++a) {
-              const DAgg& ag = d.aggs[a];
-              Val v{0, 0};
-              int32_t vt = P_I64;
-              if (ag.prog >= 0) {
-                v = vm_eval_c<kAggCols>(d.progs[ag.prog], d.cols, rid[bb], d.sink_cols, d.n_sink_cols, cv[bb], st);
-                vt = d.progs[ag.prog].out_type;
-              }
-              if (sidx >= 0) {
-                long long* hp = sagg.hi_index[a] >= 0
-                                    ? (long long*)(sagg.hi + (size_t)sagg.hi_index[a] * sagg.cap + sidx)
-                                    : nullptr;
-                agg_apply(ag.fn, (unsigned long long*)(sagg.lo + (size_t)a * sagg.cap + sidx), hp, v, vt);
-              } else {
-                agg_apply(ag.fn, (unsigned long long*)(ag.lo + g), (long long*)(ag.hi ? ag.hi + g : nullptr), v,
-                          vt);
-              }
-            }
-            break;
-          }
-          case SK_AGG_SCALAR: {
-#pragma unroll
-            for (int a = 0; a < kMaxAggs; ++a) {
-              if (a >= d.n_aggs) break;
-              const DAgg& ag = d.aggs[a];
-              Val v{0, 0};
-              int32_t vt = P_I64;
-              if (ag.prog >= 0) {
-                v = vm_eval_c<kAggCols>(d.progs[ag.prog], d.cols, rid[bb], d.sink_cols, d.n_sink_cols, cv[bb], st);
-                vt = d.progs[ag.prog].out_type;
-              }
-              switch (ag.fn) {
-                case A_COUNT: plo[a] += 1; break;
-                case A_SUM_I: plo[a] += (uint64_t)v.lo; break;
-                case A_SUM_I128: {
-                  uint64_t o = plo[a];
-                  plo[a] += (uint64_t)v.lo;
-                  phi[a] += (vt == P_I128 ? v.hi : (v.lo >> 63)) + (plo[a] < o ? 1 : 0);
-                  break;
-                }
-                case A_SUM_F:
-                  plo[a] = (uint64_t)__double_as_longlong(
-                      __dadd_rn(__longlong_as_double((long long)plo[a]), val_as_f64(v, vt)));
-                  break;
-                case A_MIN_I: if ((int64_t)v.lo < (int64_t)plo[a]) plo[a] = (uint64_t)v.lo; break;
-                case A_MAX_I: if ((int64_t)v.lo > (int64_t)plo[a]) plo[a] = (uint64_t)v.lo; break;
-                case A_MIN_F: { uint64_t u = ord_f64(val_as_f64(v, vt)); if (u < plo[a]) plo[a] = u; break; }
-                case A_MAX_F: { uint64_t u = ord_f64(val_as_f64(v, vt)); if (u > plo[a]) plo[a] = u; break; }
-                default: break;
-              }
-            }
-            break;
-          }
-          default: break;
-        }
-      }
+      __syncthreads();
+      n_sel = *cnt;
+      ident = false;
+      uint16_t* t_ = sel_in;
+      sel_in = sel_out;
+      sel_out = t_;
+      cq = (cq + 1) % 3;
     }
 
+    // ---- sink over the surviving tile rows
     if (SINK == SK_MATERIALIZE) {
+      for (int r = tid; r < TILE; r += THREADS) s_keep[r] = 0;
       __syncthreads();
-      // Blocked arrangement for the scan: thread t owns tile rows [t*ITEMS, (t+1)*ITEMS).
-      uint32_t cnt = 0;
+      for (uint32_t i = tid; i < n_sel; i += THREADS) s_keep[ident ? i : sel_in[i]] = 1;
+      __syncthreads();
+      // Blocked arrangement for the scan: thread t owns tile rows [t*8, (t+1)*8).
+      constexpr int PER = TILE / THREADS;
+      uint32_t cntk = 0;
 #pragma unroll
-      for (int i = 0; i < ITEMS; ++i) cnt += s_keep[tid * ITEMS + i];
+      for (int i = 0; i < PER; ++i) cntk += s_keep[tid * PER + i];
       uint32_t total;
-      uint32_t pos = block_excl_sum<THREADS>(cnt, s_warp, &total);
+      uint32_t pos = block_excl_sum<THREADS>(cntk, s_warp, &total);
 #pragma unroll
-      for (int i = 0; i < ITEMS; ++i)
-        if (s_keep[tid * ITEMS + i]) s_list[pos++] = (uint16_t)(tid * ITEMS + i);
+      for (int i = 0; i < PER; ++i)
+        if (s_keep[tid * PER + i]) s_list[pos++] = (uint16_t)(tid * PER + i);
       if (tid == 0) {
         uint64_t excl = lb_exclusive(d.tile_status, tile, total, d.epoch, d.status);
         s_base = excl;
@@ -680,54 +672,137 @@ __global__ void __launch_bounds__(kThreads) k_pipeline(const __grid_constant__ P
       }
       __syncthreads();
       const uint64_t base = s_base;
-      // Write phase: kBatch compacted rows per thread, columns fetched first.
-      for (uint32_t p0 = tid; p0 < total; p0 += THREADS * kBatch) {
-        uint32_t rr[kBatch][kMaxSrc];
-        uint32_t tx[kBatch];
-        uint32_t okm = 0;
-#pragma unroll
-        for (int bb = 0; bb < kBatch; ++bb) {
-          const uint32_t p = p0 + bb * THREADS;
-          const bool ok = p < total;
-          okm |= (ok ? 1u : 0u) << bb;
-          tx[bb] = ok ? s_list[p] : 0u;
-#pragma unroll
-          for (int s = 0; s < kMaxSrc; ++s) {
-            uint32_t r = (rid_slot[s] >= 0 && ok) ? s_rid[(size_t)rid_slot[s] * TILE + tx[bb]] : 0u;
-            if (!d.tuple_input && s == d.drive_src) r = (uint32_t)(tile_base + tx[bb]);
-            rr[bb][s] = r;
+      // write phase: one output column at a time over the compacted rows
+      for (int q = 0; q < d.n_out; ++q) {
+        const VmProg& pg = d.progs[d.out_prog[q]];
+        void* out = d.out_ptr[q];
+        const int32_t ot = pg.out_type;
+        if (pg.n == 1 && pg.ins[0].op == VM_COL) {
+          // plain column: typed copy
+          const int col = pg.ins[0].arg;
+          for (uint32_t p = tid; p < total; p += THREADS) {
+            const uint64_t o = base + p;
+            if (o >= d.out_capacity) { st |= ST_CAPACITY; continue; }
+            Val v;
+            v.lo = tc_get(tc, col, s_list[p]);
+            v.hi = v.lo >> 63;
+            store_val(out, ot, o, v);
+          }
+        } else {
+          for (uint32_t p = tid; p < total; p += THREADS) {
+            const uint64_t o = base + p;
+            if (o >= d.out_capacity) { st |= ST_CAPACITY; continue; }
+            store_val(out, ot, o, vm_eval_t(pg, tc, s_list[p], st));
           }
         }
-        int64_t cv[kBatch][kOutCols];
-#pragma unroll
-        for (int jc = 0; jc < kOutCols; ++jc) {
-          const bool use = jc < d.n_sink_cols;
-          const int col = use ? d.sink_cols[jc] : 0;
-          const int src = d.cols[col].src;
-#pragma unroll
-          for (int bb = 0; bb < kBatch; ++bb)
-            cv[bb][jc] = (use && ((okm >> bb) & 1u)) ? fetch(col, pick(rr[bb], src), tx[bb]) : 0;
-        }
-#pragma unroll
-        for (int bb = 0; bb < kBatch; ++bb) {
-          if (!((okm >> bb) & 1u)) continue;
-          const uint64_t o = base + p0 + bb * THREADS;
-          if (o >= d.out_capacity) {
-            st |= ST_CAPACITY;
-            continue;
-          }
-          for (int q = 0; q < d.n_out; ++q) {
-            const VmProg& pg = d.progs[d.out_prog[q]];
-            Val v = vm_eval_c<kOutCols>(pg, d.cols, rr[bb], d.sink_cols, d.n_sink_cols, cv[bb], st);
-            store_val(d.out_ptr[q], pg.out_type, o, v);
-          }
-#pragma unroll
+      }
+      for (int s = 0; s < kMaxSrc; ++s)
+        if ((d.out_rid_mask >> s) & 1u)
+          for (uint32_t p = tid; p < total; p += THREADS)
+            if (base + p < d.out_capacity) d.out_rids[s][base + p] = tc_rid(tc, s, s_list[p]);
+    } else if (SINK == SK_BUILD) {
+      const DBuild& bd = d.builds[d.sink_build];
+      for (uint32_t i0 = 0; i0 < n_sel; i0 += THREADS) {
+        const uint32_t i = i0 + tid;
+        const bool act = i < n_sel;
+        const uint32_t r = act ? (ident ? i : (uint32_t)sel_in[i]) : 0u;
+        const uint32_t m = __ballot_sync(0xFFFFFFFFu, act);
+        const int lane = tid & 31;
+        uint32_t sbase = 0;
+        if (lane == 0 && m) sbase = atomicAdd(bd.n_slots, (uint32_t)__popc(m));
+        sbase = __shfl_sync(0xFFFFFFFFu, sbase, 0);
+        if (act) {
+          const uint32_t slot = sbase + __popc(m & ((1u << lane) - 1u));
+          const int64_t key = tc_get(tc, d.build_key_col, r);
           for (int s = 0; s < kMaxSrc; ++s)
-            if ((d.out_rid_mask >> s) & 1u) d.out_rids[s][o] = rr[bb][s];
+            if ((d.build_payload_mask >> s) & 1u) bd.payload[s][slot] = tc_rid(tc, s, r);
+          // A representative-row aggregate downstream keeps its states by
+          // this slot: initialize them here, so the (build-table sized)
+          // state arrays need no clearing per query.
+          for (int a = 0; a < d.n_aggs; ++a) agg_init_global(d.aggs[a], slot);
+          if (d.slot_hit) d.slot_hit[slot] = 0;
+          build_insert(bd, key, slot, st);
+        }
+      }
+    } else {
+      for (uint32_t i = tid; i < n_sel; i += THREADS) {
+        const uint32_t r = ident ? i : (uint32_t)sel_in[i];
+        if (SINK == SK_AGG_SLOT) {
+          const uint32_t g = s_slot[r];
+          d.slot_hit[g] = 1;
+          for (int a = 0; a < d.n_aggs; ++a) {
+            const DAgg& ag = d.aggs[a];
+            Val v{0, 0};
+            int32_t vt = P_I64;
+            if (ag.prog >= 0) {
+              v = vm_eval_t(d.progs[ag.prog], tc, r, st);
+              vt = d.progs[ag.prog].out_type;
+            }
+            agg_apply(ag.fn, (unsigned long long*)(ag.lo + g), (long long*)(ag.hi ? ag.hi + g : nullptr), v, vt);
+          }
+        } else if (SINK == SK_AGG_HASH || SINK == SK_AGG_SMEM) {
+          uint64_t kw[kMaxKeys];
+#pragma unroll
+          for (int q = 0; q < kMaxKeys; ++q)
+            kw[q] = q < d.table.n_keys ? (uint64_t)vm_eval_t(d.progs[d.key_prog[q]], tc, r, st).lo : 0;
+          int sidx = -1;
+          if (SINK == SK_AGG_SMEM) sidx = smem_agg_find(d, sagg, kw, st);
+          uint64_t g = d.table.capacity;
+          if (sidx < 0) g = agg_find_global(d, kw, st);
+          if (sidx < 0 && g >= d.table.capacity) continue;
+          for (int a = 0; a < d.n_aggs; ++a) {
+            const DAgg& ag = d.aggs[a];
+            Val v{0, 0};
+            int32_t vt = P_I64;
+            if (ag.prog >= 0) {
+              v = vm_eval_t(d.progs[ag.prog], tc, r, st);
+              vt = d.progs[ag.prog].out_type;
+            }
+            if (sidx >= 0) {
+              long long* hp = sagg.hi_index[a] >= 0
+                                  ? (long long*)(sagg.hi + (size_t)sagg.hi_index[a] * sagg.cap + sidx)
+                                  : nullptr;
+              agg_apply(ag.fn, (unsigned long long*)(sagg.lo + (size_t)a * sagg.cap + sidx), hp, v, vt);
+            } else {
+              agg_apply(ag.fn, (unsigned long long*)(ag.lo + g), (long long*)(ag.hi ? ag.hi + g : nullptr), v,
+                        vt);
+            }
+          }
+        } else if (SINK == SK_AGG_SCALAR) {
+#pragma unroll
+          for (int a = 0; a < kMaxAggs; ++a) {
+            if (a >= d.n_aggs) break;
+            const DAgg& ag = d.aggs[a];
+            Val v{0, 0};
+            int32_t vt = P_I64;
+            if (ag.prog >= 0) {
+              v = vm_eval_t(d.progs[ag.prog], tc, r, st);
+              vt = d.progs[ag.prog].out_type;
+            }
+            switch (ag.fn) {
+              case A_COUNT: plo[a] += 1; break;
+              case A_SUM_I: plo[a] += (uint64_t)v.lo; break;
+              case A_SUM_I128: {
+                uint64_t o = plo[a];
+                plo[a] += (uint64_t)v.lo;
+                phi[a] += (vt == P_I128 ? v.hi : (v.lo >> 63)) + (plo[a] < o ? 1 : 0);
+                break;
+              }
+              case A_SUM_F:
+                plo[a] = (uint64_t)__double_as_longlong(
+                    __dadd_rn(__longlong_as_double((long long)plo[a]), val_as_f64(v, vt)));
+                break;
+              case A_MIN_I: if ((int64_t)v.lo < (int64_t)plo[a]) plo[a] = (uint64_t)v.lo; break;
+              case A_MAX_I: if ((int64_t)v.lo > (int64_t)plo[a]) plo[a] = (uint64_t)v.lo; break;
+              case A_MIN_F: { uint64_t u = ord_f64(val_as_f64(v, vt)); if (u < plo[a]) plo[a] = u; break; }
+              case A_MAX_F: { uint64_t u = ord_f64(val_as_f64(v, vt)); if (u > plo[a]) plo[a] = u; break; }
+              default: break;
+            }
+          }
         }
       }
     }
-    // Every thread is done with `buf` (and the sink scratch) before reuse.
+    // Every thread is done with `buf`, the selection and the sink scratch.
     __syncthreads();
     cur = s_tile[(k + 1) & 1];
     ++k;
@@ -814,21 +889,24 @@ static int sm_count() {
 
 size_t pipeline_tile_rows() { return kTile; }
 
-size_t pipeline_stream_bytes(const PipeDesc& d) {
-  return d.tuple_input ? 0 : 2ull * kTile * stream_bytes_per_row(d);
+static int probed_sources(const PipeDesc& d) {
+  int nq = 0;
+  for (int s = 0; s < kMaxSrc; ++s) {
+    if (s == d.drive_src) continue;
+    bool used = false;
+    for (int p = 0; p < d.n_probes; ++p) used |= ((d.probes[p].fill_mask >> s) & 1u) != 0;
+    nq += used;
+  }
+  return nq;
 }
 
 size_t pipeline_smem_bytes(const PipeDesc& d) {
   constexpr size_t TILE = kTile;
-  size_t s = pipeline_stream_bytes(d);
-  if (d.sink == SK_MATERIALIZE) {
-    size_t q = 0;
-    for (int i = 0; i < kMaxSrc; ++i) {
-      bool implicit = !d.tuple_input && i == d.drive_src;
-      if (((d.mat_src_mask >> i) & 1u) && !implicit) ++q;
-    }
-    s += TILE + 2 * TILE + 4 * TILE * q;
-  }
+  size_t s = 2ull * TILE * stream_bytes_per_row(d);  // stream buffers
+  s += 2 * TILE * 2;                                  // selection vectors
+  s += TILE * 4;                                      // probe slots
+  s += (size_t)probed_sources(d) * TILE * 4;          // probed row ids
+  if (d.sink == SK_MATERIALIZE) s += TILE + 2 * TILE;  // keep flags + compacted list
   if (d.sink == SK_AGG_SMEM) {
     size_t n128 = 0;
     for (int a = 0; a < d.n_aggs; ++a) n128 += d.aggs[a].fn == A_SUM_I128;
@@ -837,21 +915,37 @@ size_t pipeline_smem_bytes(const PipeDesc& d) {
   return s;
 }
 
+// Occupancy per (sink, dynamic smem) is computed once and cached: these
+// queries cost host time on every launch otherwise.
+static std::mutex g_occ_mu;
+static std::map<std::pair<int, size_t>, int> g_occ;
+static size_t g_smem_set[8];
+
 template <int SINK>
 static cudaError_t launch_sink(const PipeDesc& d, uint64_t n_hint, cudaStream_t s) {
   auto kern = k_pipeline<SINK>;
   const size_t smem = pipeline_smem_bytes(d);
-  if (smem > 48 * 1024) {
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
+  int blocks_per_sm = 0;
+  {
+    std::lock_guard<std::mutex> g(g_occ_mu);
+    if (smem > 48 * 1024 && smem > g_smem_set[SINK]) {
+      cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      if (e != cudaSuccess) return e;
+      g_smem_set[SINK] = smem;
+    }
+    auto it = g_occ.find({SINK, smem});
+    if (it != g_occ.end()) {
+      blocks_per_sm = it->second;
+    } else {
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, kern, kThreads, smem) != cudaSuccess ||
+          blocks_per_sm < 1) {
+        cudaGetLastError();
+        blocks_per_sm = 1;
+      }
+      g_occ[{SINK, smem}] = blocks_per_sm;
+    }
   }
   // Grid = resident CTAs per SM x SM count (a persistent grid-stride grid).
-  int blocks_per_sm = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, kern, kThreads, smem) != cudaSuccess ||
-      blocks_per_sm < 1) {
-    cudaGetLastError();
-    blocks_per_sm = 1;
-  }
   uint64_t tiles = (n_hint + kTile - 1) / kTile;
   uint64_t max_grid = (uint64_t)sm_count() * (uint64_t)blocks_per_sm;
   uint64_t grid = tiles < max_grid ? tiles : max_grid;
@@ -861,6 +955,7 @@ static cudaError_t launch_sink(const PipeDesc& d, uint64_t n_hint, cudaStream_t 
 }
 
 cudaError_t launch_pipeline(const PipeDesc& d, uint64_t n_hint, cudaStream_t s) {
+  if (d.tuple_input) return cudaErrorInvalidValue;  // every pipeline scans a base table
   switch (d.sink) {
     case SK_BUILD: return launch_sink<SK_BUILD>(d, n_hint, s);
     case SK_MATERIALIZE: return launch_sink<SK_MATERIALIZE>(d, n_hint, s);

@@ -104,5 +104,14 @@ cudaError_t launch_count_dups(const void* col, int ptype, uint64_t n, int64_t* t
 
 // ---- utility
 cudaError_t launch_fill_u64(uint64_t* p, uint64_t n, uint64_t v, cudaStream_t s);
+// One launch that fills every segment with a repeated 64-bit pattern
+// (scratch initialization of a whole query). Segments are 16-byte aligned
+// and their sizes multiples of 16.
+struct FillSeg {
+  void* ptr;
+  uint64_t bytes;
+  uint64_t pattern;
+};
+cudaError_t launch_fill_segments(const FillSeg* segs_dev, int n_segs, uint64_t max_bytes, cudaStream_t s);
 
 }  // namespace mtl
