@@ -238,8 +238,18 @@ class Connection:
     # ------------------------------------------------------------ lifecycle
     def close(self):
         if self.ctx:
+            # requests and statements hold context resources: release them first
+            for obj in list(getattr(self, "_children", ())):
+                obj.close()
             self.lib.mtl_ctx_destroy(self.ctx)
             self.ctx = None
+
+    def _adopt(self, obj):
+        import weakref
+        if not hasattr(self, "_children"):
+            self._children = weakref.WeakSet()
+        self._children.add(obj)
+        return obj
 
     def __enter__(self):
         return self
@@ -526,13 +536,13 @@ class Connection:
     # ------------------------------------------------------------ prepared / serving
     def prepare(self, sql: str) -> "Statement":
         self._require_ctx()
-        return Statement(self, sql)
+        return self._adopt(Statement(self, sql))
 
     def submit(self, sql: str) -> "Request":
         self._require_ctx()
         h = C.c_void_p()
         self._check(self.lib.mtl_query_submit(self.ctx, sql.encode(), C.byref(h)))
-        return Request(self, h)
+        return self._adopt(Request(self, h))
 
     def serve_stats(self) -> dict:
         s = L.ServeStats()
@@ -575,9 +585,10 @@ class Statement:
                 for i in range(lib.mtl_stmt_step_count(self.h))]
 
     def close(self):
-        if self.h:
+        # after the connection closed, the context already released it
+        if self.h and self.conn.ctx:
             self.conn.lib.mtl_stmt_free(self.h)
-            self.h = None
+        self.h = None
 
     def __del__(self):
         try:
@@ -604,9 +615,9 @@ class Request:
         return float(self.conn.lib.mtl_request_latency_ms(self.h))
 
     def close(self):
-        if self.h:
+        if self.h and self.conn.ctx:
             self.conn.lib.mtl_request_free(self.h)
-            self.h = None
+        self.h = None
 
     def __del__(self):
         try:

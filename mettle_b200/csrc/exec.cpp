@@ -224,7 +224,7 @@ void column_minmax(Ctx& ctx, Column& c) {
   int64_t* buf = nullptr;
   CK(cudaMalloc(&buf, 16));
   int64_t init[2] = {INT64_MAX, INT64_MIN};
-  CK(cudaMemcpy(buf, init, 16, cudaMemcpyHostToDevice));
+  CK(cudaMemcpyAsync(buf, init, 16, cudaMemcpyHostToDevice, ctx.copy_stream));
   CK(launch_minmax_i(d, pt, rows, buf, ctx.copy_stream));
   int64_t out[2];
   CK(cudaMemcpyAsync(out, buf, 16, cudaMemcpyDeviceToHost, ctx.copy_stream));
@@ -296,6 +296,15 @@ struct Compiler {
     P.scratch_bytes += (bytes + 255) & ~255ULL;
     return p;
   }
+  // Descriptor uploads complete before compile() returns: the program may
+  // run on any stream, and a plain cudaMemcpy from pageable memory can
+  // return before its DMA lands.
+  void upload(void* dst, const void* src, size_t bytes) {
+    std::lock_guard<std::recursive_mutex> g(ctx.mu);
+    CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, ctx.copy_stream));
+    CK(cudaStreamSynchronize(ctx.copy_stream));
+  }
+
   // Scratch initialization is collected and emitted as one fill launch at
   // the start of the program (arena blocks are 256-byte aligned and sized in
   // 256-byte units, so rounding a segment up to 16 bytes stays in its block).
@@ -317,7 +326,7 @@ struct Compiler {
   void emit_fills() {
     if (fills.empty()) return;
     FillSeg* dev = (FillSeg*)scratch(fills.size() * sizeof(FillSeg));
-    CK(cudaMemcpy(dev, fills.data(), fills.size() * sizeof(FillSeg), cudaMemcpyHostToDevice));
+    upload(dev, fills.data(), fills.size() * sizeof(FillSeg));
     uint64_t mx = 0;
     for (auto& f : fills) mx = std::max(mx, f.bytes);
     Step s;
@@ -827,7 +836,7 @@ struct Compiler {
 
   FinalOut* upload_finals(const std::vector<FinalOut>& fo) {
     FinalOut* d = (FinalOut*)scratch(fo.size() * sizeof(FinalOut));
-    CK(cudaMemcpy(d, fo.data(), fo.size() * sizeof(FinalOut), cudaMemcpyHostToDevice));
+    upload(d, fo.data(), fo.size() * sizeof(FinalOut));
     return d;
   }
 

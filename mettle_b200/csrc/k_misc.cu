@@ -57,10 +57,12 @@ __global__ void __launch_bounds__(kCThreads) k_compact(Flag flag, uint64_t n_sta
     }
     uint32_t total;
     uint32_t pos = block_excl_sum<kCThreads>(__popc(bits), s_warp, &total);
-    if (tid == 0) {
-      uint64_t excl = lb_exclusive(tstatus, tile, total, epoch, status);
-      s_base = excl;
-      if (tile == n_tiles - 1) *out_count = excl + total;
+    if (tid < 32) {
+      const uint64_t excl = lb_exclusive_warp(tstatus, tile, total, epoch, status);
+      if (tid == 0) {
+        s_base = excl;
+        if (tile == n_tiles - 1) *out_count = excl + total;
+      }
     }
     __syncthreads();
     const uint64_t base = s_base;

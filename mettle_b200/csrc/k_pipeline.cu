@@ -665,10 +665,12 @@ __global__ void __launch_bounds__(kThreads) k_pipeline(const __grid_constant__ P
 #pragma unroll
       for (int i = 0; i < PER; ++i)
         if (s_keep[tid * PER + i]) s_list[pos++] = (uint16_t)(tid * PER + i);
-      if (tid == 0) {
-        uint64_t excl = lb_exclusive(d.tile_status, tile, total, d.epoch, d.status);
-        s_base = excl;
-        if (tile == n_tiles - 1) *d.out_count = excl + total;
+      if (tid < 32) {
+        const uint64_t excl = lb_exclusive_warp(d.tile_status, tile, total, d.epoch, d.status);
+        if (tid == 0) {
+          s_base = excl;
+          if (tile == n_tiles - 1) *d.out_count = excl + total;
+        }
       }
       __syncthreads();
       const uint64_t base = s_base;
@@ -687,6 +689,20 @@ __global__ void __launch_bounds__(kThreads) k_pipeline(const __grid_constant__ P
             v.lo = tc_get(tc, col, s_list[p]);
             v.hi = v.lo >> 63;
             store_val(out, ot, o, v);
+          }
+        } else if (pg.n == 3 && pg.ins[0].op == VM_COL && pg.ins[1].op == VM_CONST && pg.ins[2].op >= VM_ADD &&
+                   pg.ins[2].op <= VM_MUL && pg.ins[2].type != P_I128) {
+          // column op constant, evaluated inline
+          const int col = pg.ins[0].arg;
+          const Val kc{pg.ins[1].k, pg.ins[1].k2};
+          const int16_t aop = pg.ins[2].op, aty = pg.ins[2].type;
+          for (uint32_t p = tid; p < total; p += THREADS) {
+            const uint64_t o = base + p;
+            if (o >= d.out_capacity) { st |= ST_CAPACITY; continue; }
+            Val v;
+            v.lo = tc_get(tc, col, s_list[p]);
+            v.hi = v.lo >> 63;
+            store_val(out, ot, o, vm_arith(aop, aty, v, kc, st));
           }
         } else {
           for (uint32_t p = tid; p < total; p += THREADS) {
@@ -928,7 +944,9 @@ static cudaError_t launch_sink(const PipeDesc& d, uint64_t n_hint, cudaStream_t 
   int blocks_per_sm = 0;
   {
     std::lock_guard<std::mutex> g(g_occ_mu);
-    if (smem > 48 * 1024 && smem > g_smem_set[SINK]) {
+    // static shared memory counts against the same 48 KB default, so the
+    // opt-in limit is raised for any dynamic size not set before
+    if (smem > g_smem_set[SINK]) {
       cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
       if (e != cudaSuccess) return e;
       g_smem_set[SINK] = smem;

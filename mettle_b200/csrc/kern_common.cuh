@@ -383,6 +383,56 @@ __device__ __forceinline__ uint64_t lb_exclusive(uint64_t* status, uint64_t t, u
   return excl;
 }
 
+// Warp-parallel look-back, called by all 32 lanes of one warp: lane i
+// inspects predecessor t-1-i, so one round trip covers 32 tiles. Sums the
+// aggregates back to the nearest published prefix, publishes this tile's
+// inclusive prefix and returns its exclusive prefix (in every lane).
+__device__ __forceinline__ uint64_t lb_exclusive_warp(uint64_t* status, uint64_t t, uint64_t c, uint32_t epoch,
+                                                      uint32_t* st_flags) {
+  const int lane = threadIdx.x & 31;
+  const uint64_t ep = (uint64_t)(epoch & 0xFFFFu);
+  const uint64_t vmask = (1ULL << 46) - 1;
+  if (t == 0) {
+    if (lane == 0) st_release(status, lb_word(epoch, kLbPre, c));
+    return 0;
+  }
+  if (lane == 0) st_release(status + t, lb_word(epoch, kLbAgg, c));
+  uint64_t excl = 0;
+  int64_t j = (int64_t)t - 1;
+  uint32_t spins = 0;
+  for (;;) {
+    const int64_t idx = j - lane;
+    uint64_t flag, val;
+    if (idx < 0) {
+      flag = kLbPre;  // before the first tile: a prefix of zero
+      val = 0;
+    } else {
+      const uint64_t w = ld_acquire(status + idx);
+      flag = ((w >> 48) == ep) ? ((w >> 46) & 3ULL) : 0ULL;
+      val = w & vmask;
+    }
+    const uint32_t pre = __ballot_sync(0xFFFFFFFFu, flag == kLbPre);
+    const uint32_t none = __ballot_sync(0xFFFFFFFFu, flag == 0);
+    const int limit = pre ? __ffs(pre) - 1 : 31;  // lanes 0..limit are summed
+    const uint32_t upto = limit == 31 ? 0xFFFFFFFFu : ((1u << (limit + 1)) - 1u);
+    if (none & upto) {
+      if (++spins > kSpinLimit) {
+        if (lane == 0) atomicOr(st_flags, ST_SPIN_LIMIT);
+        break;
+      }
+      continue;  // a nearer predecessor has not published yet
+    }
+    uint64_t v = lane <= limit ? val : 0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, o);
+    excl += v;
+    if (pre) break;
+    j -= 32;
+  }
+  if (lane == 0) st_release(status + t, lb_word(epoch, kLbPre, excl + c));
+  return excl;
+}
+
 // ------------------------------------------------------------ block scan
 // Exclusive block-wide sum of one u32 per thread; returns the thread's
 // exclusive prefix, *total gets the block total. Needs THREADS/32 words of
