@@ -89,8 +89,36 @@ class HostTable:
         return len(c.array) if c.array is not None else len(c.values)
 
 
+class _ResultOwner:
+    """Frees the native result once no column view refers to it."""
+
+    def __init__(self, lib, handle):
+        self.lib, self.handle = lib, handle
+
+    def __del__(self):
+        if self.handle:
+            try:
+                self.lib.mtl_result_free(self.handle)
+            except Exception:  # interpreter shutdown
+                pass
+            self.handle = None
+
+
+def _view(owner, ptr, nbytes, dtype):
+    """Zero-copy numpy view of native result bytes, keeping ``owner`` alive."""
+    buf = (C.c_uint8 * nbytes).from_address(ptr)
+    buf._owner = owner
+    arr = np.frombuffer(buf, dtype=dtype)
+    arr.flags.writeable = False  # cached results share these bytes
+    return arr
+
+
 class Result:
-    """A gpu_processing result with numpy columns and DuckDB-typed rows."""
+    """A gpu_processing result with numpy columns and DuckDB-typed rows.
+
+    Columns are read-only views of the native result's page-locked host
+    buffers (no copy); the native result is freed when the last view goes.
+    """
 
     def __init__(self, lib, handle):
         self.names: list[str] = []
@@ -98,41 +126,37 @@ class Result:
         self.columns: list[np.ndarray] = []
         self.valid: list[np.ndarray | None] = []
         self.dicts: list[list[str] | None] = []
-        try:
-            self.rows = int(lib.mtl_result_rows(handle))
-            self.device_ms = float(lib.mtl_result_device_ms(handle))
-            for i in range(lib.mtl_result_columns(handle)):
-                scale = C.c_int32(0)
-                t = lib.mtl_result_column_type(handle, i, C.byref(scale))
-                self.names.append(lib.mtl_result_column_name(handle, i).decode())
-                self.types.append((t, scale.value))
-                width = 16 if t in (L.T_HUGEINT, L.T_DECIMAL128) else (
-                    4 if t in (L.T_INTEGER, L.T_DATE, L.T_FLOAT, L.T_VARCHAR) else 8)
-                ptr = lib.mtl_result_column_data(handle, i)
-                raw = C.string_at(ptr, self.rows * width) if self.rows else b""
-                if width == 16:
-                    arr = np.frombuffer(raw, dtype=np.int64).reshape(-1, 2).copy()
-                else:
-                    dt = {L.T_FLOAT: np.float32, L.T_DOUBLE: np.float64}.get(
-                        t, np.int32 if width == 4 else np.int64)
-                    arr = np.frombuffer(raw, dtype=dt).copy()
-                self.columns.append(arr)
-                vp = lib.mtl_result_column_valid(handle, i)
-                self.valid.append(np.frombuffer(C.string_at(vp, self.rows), dtype=np.uint8).copy()
-                                  if vp and self.rows else None)
-                if t == L.T_VARCHAR:
-                    d, k = [], 0
-                    codes = set(arr.tolist())
-                    mx = max(codes) if codes else -1
-                    while k <= mx:
-                        s = lib.mtl_result_dict(handle, i, k)
-                        d.append(s.decode() if s is not None else None)
-                        k += 1
-                    self.dicts.append(d)
-                else:
-                    self.dicts.append(None)
-        finally:
-            lib.mtl_result_free(handle)
+        owner = _ResultOwner(lib, handle)
+        self.rows = int(lib.mtl_result_rows(handle))
+        self.device_ms = float(lib.mtl_result_device_ms(handle))
+        for i in range(lib.mtl_result_columns(handle)):
+            scale = C.c_int32(0)
+            t = lib.mtl_result_column_type(handle, i, C.byref(scale))
+            self.names.append(lib.mtl_result_column_name(handle, i).decode())
+            self.types.append((t, scale.value))
+            width = 16 if t in (L.T_HUGEINT, L.T_DECIMAL128) else (
+                4 if t in (L.T_INTEGER, L.T_DATE, L.T_FLOAT, L.T_VARCHAR) else 8)
+            ptr = lib.mtl_result_column_data(handle, i)
+            dt = {L.T_FLOAT: np.float32, L.T_DOUBLE: np.float64}.get(
+                t, np.int32 if width == 4 else np.int64)
+            if self.rows and ptr:
+                arr = _view(owner, ptr, self.rows * width, dt)
+            else:
+                arr = np.zeros(0, dtype=dt)
+            if width == 16:
+                arr = arr.reshape(-1, 2)
+            self.columns.append(arr)
+            vp = lib.mtl_result_column_valid(handle, i)
+            self.valid.append(_view(owner, vp, self.rows, np.uint8) if vp and self.rows else None)
+            if t == L.T_VARCHAR:
+                d = []
+                mx = int(arr.max()) if arr.size else -1
+                for k in range(mx + 1):
+                    s = lib.mtl_result_dict(handle, i, k)
+                    d.append(s.decode() if s is not None else None)
+                self.dicts.append(d)
+            else:
+                self.dicts.append(None)
 
     def value(self, col: int, row: int):
         t, scale = self.types[col]

@@ -187,6 +187,14 @@ int mtl_ctx_create(const mtl_budgets* budgets, int device, mtl_ctx** out) {
     if (budgets->processing_region_bytes > fr)
       fail(MTL_BUDGET_EXCEEDED, "processing region larger than free device memory");
     c.arena.init(budgets->processing_region_bytes);
+    // Keep freed column buffers reserved in the device's default pool (a
+    // process-local allocator attribute) so table re-registration reuses them.
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+      uint64_t keep = budgets->cache_region_bytes;
+      cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+    cudaGetLastError();
   });
   if (rc != MTL_OK) {
     delete h;
@@ -388,7 +396,7 @@ int mtl_column_evict(mtl_ctx* ctx, const char* table, const char* column) {
     if (!col) fail(MTL_INVALID, "column not found");
     if (col->pins) fail(MTL_INVALID, "column is in use by a prepared statement");
     if (col->dev) {
-      cudaFree(col->dev);
+      cudaFreeAsync(col->dev, 0);
       c.dev_cache_bytes -= col->dev_bytes;
       col->dev = nullptr;
       col->dev_bytes = 0;
@@ -621,7 +629,7 @@ int mtl_cache_reset(mtl_ctx* ctx) {
     for (auto& t : c.tables)
       for (auto& col : t.second->cols)
         if (col->dev && col->pins == 0) {
-          cudaFree(col->dev);
+          cudaFreeAsync(col->dev, 0);
           c.dev_cache_bytes -= col->dev_bytes;
           col->dev = nullptr;
           col->dev_bytes = 0;

@@ -254,11 +254,42 @@ struct Program {
 };
 
 // ------------------------------------------------------------ results
+// Host bytes of a result column. Large buffers are page-locked and come from
+// a process-wide pool, so device->host copies run at full PCIe rate and
+// repeated queries do not pay cudaHostAlloc.
+class HostBuf {
+ public:
+  HostBuf() = default;
+  HostBuf(const HostBuf&) = delete;
+  HostBuf& operator=(const HostBuf&) = delete;
+  HostBuf(HostBuf&& o) noexcept { swap(o); }
+  HostBuf& operator=(HostBuf&& o) noexcept {
+    swap(o);
+    return *this;
+  }
+  ~HostBuf();
+  void resize(size_t bytes);  // contents are not preserved
+  uint8_t* data() { return p_; }
+  const uint8_t* data() const { return p_; }
+  size_t size() const { return n_; }
+
+ private:
+  void swap(HostBuf& o) {
+    std::swap(p_, o.p_);
+    std::swap(n_, o.n_);
+    std::swap(cap_, o.cap_);
+    std::swap(pinned_, o.pinned_);
+  }
+  uint8_t* p_ = nullptr;
+  size_t n_ = 0, cap_ = 0;
+  bool pinned_ = false;
+};
+
 struct ResultCol {
   std::string name;
   LType type;
   int width = 0;
-  std::vector<uint8_t> data;
+  HostBuf data;
   std::vector<uint8_t> valid;  // empty = all valid
   std::vector<std::string> dict;
 };

@@ -77,6 +77,69 @@ Column* Table::find(const std::string& n) const {
   return nullptr;
 }
 
+// ------------------------------------------------------------ host buffers
+namespace {
+std::mutex g_pin_mu;
+std::map<size_t, std::vector<void*>> g_pin_free;  // capacity -> free blocks
+size_t g_pin_pooled = 0;
+constexpr size_t kPinnedFrom = 64 * 1024;        // smaller results stay pageable
+constexpr size_t kPinnedPoolMax = 8ull << 30;    // bytes kept for reuse
+}  // namespace
+
+void HostBuf::resize(size_t bytes) {
+  if (bytes <= cap_) {
+    n_ = bytes;
+    return;
+  }
+  this->~HostBuf();
+  p_ = nullptr;
+  n_ = cap_ = 0;
+  pinned_ = false;
+  if (bytes >= kPinnedFrom) {
+    size_t cap = kPinnedFrom;
+    while (cap < bytes) cap <<= 1;
+    {
+      std::lock_guard<std::mutex> g(g_pin_mu);
+      auto it = g_pin_free.find(cap);
+      if (it != g_pin_free.end() && !it->second.empty()) {
+        p_ = (uint8_t*)it->second.back();
+        it->second.pop_back();
+        g_pin_pooled -= cap;
+      }
+    }
+    if (!p_ && cudaHostAlloc((void**)&p_, cap, cudaHostAllocDefault) != cudaSuccess) {
+      cudaGetLastError();
+      p_ = nullptr;
+    }
+    if (p_) {
+      pinned_ = true;
+      cap_ = cap;
+      n_ = bytes;
+      return;
+    }
+  }
+  p_ = (uint8_t*)malloc(bytes ? bytes : 1);
+  if (!p_) throw std::bad_alloc();
+  cap_ = bytes;
+  n_ = bytes;
+}
+
+HostBuf::~HostBuf() {
+  if (!p_) return;
+  if (pinned_) {
+    std::lock_guard<std::mutex> g(g_pin_mu);
+    if (g_pin_pooled + cap_ <= kPinnedPoolMax) {
+      g_pin_free[cap_].push_back(p_);
+      g_pin_pooled += cap_;
+    } else {
+      cudaFreeHost(p_);
+    }
+  } else {
+    free(p_);
+  }
+  p_ = nullptr;
+}
+
 uint64_t Result::approx_bytes() const {
   uint64_t b = 0;
   for (auto& c : cols) b += c.data.size() + c.valid.size();
@@ -157,7 +220,8 @@ uint64_t Arena::largest_free() const {
 }
 
 Column::~Column() {
-  if (dev) cudaFree(dev);
+  // stream-ordered pool: no device-wide synchronization on free
+  if (dev) cudaFreeAsync(dev, 0);
   if (host_owned) {
     if (host_owned_pinned) cudaFreeHost(host_owned);
     else ::free(host_owned);
@@ -195,14 +259,17 @@ void* column_device(Ctx& ctx, Column& c) {
       for (auto& cc : t.second->cols)
         if (cc->dev && cc->pins == 0 && (!victim || cc->last_use < victim->last_use)) victim = cc.get();
     if (!victim) fail(MTL_BUDGET_EXCEEDED, "cache region exhausted by columns in use");
-    cudaFree(victim->dev);
+    cudaFreeAsync(victim->dev, ctx.copy_stream);
     victim->dev = nullptr;
     ctx.dev_cache_bytes -= victim->dev_bytes;
     victim->dev_bytes = 0;
     ctx.cc.evictions++;
   }
+  // Column buffers come from the device's stream-ordered pool (kept reserved
+  // by a release threshold set at context creation), so re-registering a
+  // table does not pay cudaMalloc/cudaFree each time.
   void* d = nullptr;
-  CK(cudaMalloc(&d, bytes ? bytes : 16));
+  CK(cudaMallocAsync(&d, bytes ? bytes : 16, ctx.copy_stream));
   if (bytes) {
     CK(cudaMemcpyAsync(d, c.host, bytes, cudaMemcpyHostToDevice, ctx.copy_stream));
     CK(cudaStreamSynchronize(ctx.copy_stream));
@@ -222,14 +289,14 @@ void column_minmax(Ctx& ctx, Column& c) {
   if (rows == 0) return;
   void* d = column_device(ctx, c);
   int64_t* buf = nullptr;
-  CK(cudaMalloc(&buf, 16));
+  CK(cudaMallocAsync((void**)&buf, 16, ctx.copy_stream));
   int64_t init[2] = {INT64_MAX, INT64_MIN};
   CK(cudaMemcpyAsync(buf, init, 16, cudaMemcpyHostToDevice, ctx.copy_stream));
   CK(launch_minmax_i(d, pt, rows, buf, ctx.copy_stream));
   int64_t out[2];
   CK(cudaMemcpyAsync(out, buf, 16, cudaMemcpyDeviceToHost, ctx.copy_stream));
+  CK(cudaFreeAsync(buf, ctx.copy_stream));
   CK(cudaStreamSynchronize(ctx.copy_stream));
-  cudaFree(buf);
   c.vmin = out[0];
   c.vmax = out[1];
   c.has_minmax = true;
@@ -250,25 +317,37 @@ void column_distinct(Ctx& ctx, Table& t, Column& c) {
     return;
   }
   void* d = column_device(ctx, c);
-  const uint64_t cap = std::max<uint64_t>(64, 2 * t.rows);
-  int64_t* table = nullptr;
-  uint32_t* special = nullptr;
+  cudaStream_t s = ctx.copy_stream;
   unsigned long long* out = nullptr;
-  CK(cudaMalloc(&table, cap * 8));
-  CK(cudaMalloc(&special, 16));
-  CK(cudaMalloc(&out, 16));
-  CK(cudaMemsetAsync(table, 0xFF, cap * 8, ctx.copy_stream));
-  CK(cudaMemsetAsync(special, 0, 16, ctx.copy_stream));
-  CK(cudaMemsetAsync(out, 0, 16, ctx.copy_stream));
-  // F32/F64 columns hash their bit patterns (distinct estimate only).
-  CK(launch_count_dups(d, pt == P_F32 ? P_I32 : (pt == P_F64 ? P_I64 : pt), t.rows, table, cap, special, out,
-                       ctx.copy_stream));
+  CK(cudaMallocAsync((void**)&out, 16, s));
+  CK(cudaMemsetAsync(out, 0, 16, s));
+  if (pt == P_I32 || pt == P_I64) column_minmax(ctx, c);
+  const __int128 span = c.has_minmax ? (__int128)c.vmax - (__int128)c.vmin + 1 : 0;
+  if (span > 0 && span <= (__int128)(8 * t.rows + (1u << 24))) {
+    // small value range: a presence bitmap (span / 8 bytes)
+    const uint64_t words = ((uint64_t)span + 31) / 32;
+    uint32_t* bits = nullptr;
+    CK(cudaMallocAsync((void**)&bits, words * 4, s));
+    CK(cudaMemsetAsync(bits, 0, words * 4, s));
+    CK(launch_count_dups_dense(d, pt, t.rows, c.vmin, (uint64_t)span, bits, out, s));
+    CK(cudaFreeAsync(bits, s));
+  } else {
+    const uint64_t cap = std::max<uint64_t>(64, 2 * t.rows);
+    int64_t* table = nullptr;
+    uint32_t* special = nullptr;
+    CK(cudaMallocAsync((void**)&table, cap * 8, s));
+    CK(cudaMallocAsync((void**)&special, 16, s));
+    CK(cudaMemsetAsync(table, 0xFF, cap * 8, s));
+    CK(cudaMemsetAsync(special, 0, 16, s));
+    // F32/F64 columns hash their bit patterns (distinct estimate only).
+    CK(launch_count_dups(d, pt == P_F32 ? P_I32 : (pt == P_F64 ? P_I64 : pt), t.rows, table, cap, special, out, s));
+    CK(cudaFreeAsync(table, s));
+    CK(cudaFreeAsync(special, s));
+  }
   unsigned long long dups = 0;
-  CK(cudaMemcpyAsync(&dups, out, 8, cudaMemcpyDeviceToHost, ctx.copy_stream));
-  CK(cudaStreamSynchronize(ctx.copy_stream));
-  cudaFree(table);
-  cudaFree(special);
-  cudaFree(out);
+  CK(cudaMemcpyAsync(&dups, out, 8, cudaMemcpyDeviceToHost, s));
+  CK(cudaFreeAsync(out, s));
+  CK(cudaStreamSynchronize(s));
   c.distinct = t.rows - dups;
   c.has_distinct = true;
   c.has_unique = true;

@@ -374,6 +374,27 @@ cudaError_t launch_count_dups(const void* col, int ptype, uint64_t n, int64_t* t
   return cudaGetLastError();
 }
 
+// Duplicate count for an integer column whose value range is small: one
+// presence bit per value in [vmin, vmin + span).
+__global__ void k_count_dups_dense(const void* __restrict__ col, int ptype, uint64_t n, int64_t vmin, uint64_t span,
+                                   uint32_t* bits, unsigned long long* out) {
+  unsigned long long dups = 0;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t k = (uint64_t)(load_bits(col, ptype, i) - vmin);
+    if (k >= span) continue;  // cannot happen for a true min/max
+    const uint32_t bit = 1u << (k & 31);
+    if (atomicOr(bits + (k >> 5), bit) & bit) ++dups;
+  }
+  for (int o = 16; o > 0; o >>= 1) dups += __shfl_down_sync(0xFFFFFFFFu, dups, o);
+  if ((threadIdx.x & 31) == 0 && dups) atomicAdd(out, dups);
+}
+
+cudaError_t launch_count_dups_dense(const void* col, int ptype, uint64_t n, int64_t vmin, uint64_t span,
+                                    uint32_t* bits, unsigned long long* out, cudaStream_t s) {
+  k_count_dups_dense<<<grid_for(n, 256), 256, 0, s>>>(col, ptype, n, vmin, span, bits, out);
+  return cudaGetLastError();
+}
+
 __global__ void k_fill_u64(uint64_t* p, uint64_t n, uint64_t v) {
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
     p[i] = v;

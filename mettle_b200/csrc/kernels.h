@@ -101,6 +101,9 @@ cudaError_t launch_minmax_i(const void* col, int ptype, uint64_t n, int64_t* out
 // table of `cap` i64 slots (all bits set = empty); out[0] = duplicates.
 cudaError_t launch_count_dups(const void* col, int ptype, uint64_t n, int64_t* table, uint64_t cap,
                               uint32_t* special, unsigned long long* out, cudaStream_t s);
+// Same count with a presence bitmap over [vmin, vmin + span) (span / 8 bytes).
+cudaError_t launch_count_dups_dense(const void* col, int ptype, uint64_t n, int64_t vmin, uint64_t span,
+                                    uint32_t* bits, unsigned long long* out, cudaStream_t s);
 
 // ---- utility
 cudaError_t launch_fill_u64(uint64_t* p, uint64_t n, uint64_t v, cudaStream_t s);
