@@ -296,6 +296,27 @@ def run_reference(args):
     if rank != 0:
         return
     import oracle as orc
+    if args.config == "c5":
+        tables = W.served_tables()
+        stream = W.served_stream(args.c5_queries)
+        budget = 60.0  # bounded sample of the stream
+        t0, k = time.perf_counter(), 0
+        while time.perf_counter() - t0 < budget and k < len(stream):
+            _oracle_query(stream[k], tables)
+            k += 1
+        el = time.perf_counter() - t0
+        value = k / el
+        line = {"impl": "reference", "metric": "served queries/s", "value": value, "unit": "queries/s",
+                "n_gpus": args.gpus, "steps": k, "warmup": 0, "ms_per_step": el * 1e3 / max(k, 1),
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64",
+                "data": "synthetic", "config": {"workload": f"c5 served mixed stream, first {k} of {len(stream)} queries"},
+                "cpu_baseline": {"value": value, "unit": "queries/s", "cores": orc.threads(), "kind": "port",
+                                 "sample": f"first {k} queries of the stream back to back on the host cores "
+                                           f"({el:.1f} s); the reference itself (Rust + Apple Metal) cannot run "
+                                           "on this box"},
+                "e2e": {"value": value, "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return
     wl = Workload(args.config)
     for _ in range(min(args.warmup, 1)):
         wl.cpu_run()
@@ -432,17 +453,212 @@ def run_mettle(args):
         dist.destroy_process_group()
 
 
+# ------------------------------------------------------------------ served stream
+def _checksum(res) -> tuple:
+    """Size-independent digest of a result: row count, exact integer sums
+    per column (wrapping), float sums, and the first rows' bytes."""
+    import hashlib
+    ints, floats = [], []
+    head = hashlib.blake2b(digest_size=16)
+    for c in res.columns:
+        if c.dtype.kind == "f":
+            floats.append(float(c.astype(np.float64).sum()))
+        else:
+            v = c.reshape(-1)
+            ints.append(int(v.sum(dtype=np.int64)) if v.itemsize == 4 else int(v.view(np.int64).sum()))
+            head.update(np.ascontiguousarray(v[:512]).tobytes())
+    return res.rows, tuple(ints), tuple(floats), head.hexdigest()
+
+
+def _same(a: tuple, b: tuple, rel: float = 1e-6) -> bool:
+    if a[0] != b[0] or a[1] != b[1] or a[3] != b[3]:
+        return False
+    return all(abs(x - y) <= rel * max(abs(x), abs(y), 1e-300) for x, y in zip(a[2], b[2]))
+
+
+def _oracle_query(q: dict, tables: dict):
+    import oracle as orc
+    tpl, d = tables[q["table"]]
+    if q["tpl"] == "c1":
+        rows = orc.sort_rows(d["value"], orc.filter_rows([(d["value"], ">", q["k"])]))
+        return orc.gather(d["value"], rows)
+    if q["tpl"] == "c2":
+        rows = orc.filter_rows([(d[q["col"]], q["op"], q["v"])])
+        return orc.gather(d["a"], rows)
+    return orc.groupby_c3(d["k"], d["v"], d["f"], limit=q["limit"])
+
+
+def _run_stream(conn, stream, arrivals, served: bool):
+    """Runs the stream with the given arrival offsets (s). Returns per-query
+    latency (arrival -> result on the host, ms), makespan (s) and digests."""
+    import queue
+    n = len(stream)
+    lat = [0.0] * n
+    digests = [None] * n
+    done_at = [0.0] * n
+    t0 = time.perf_counter()
+    if served:
+        q: "queue.Queue" = queue.Queue()
+
+        def waiter():
+            while True:
+                item = q.get()
+                if item is None:
+                    return
+                i, req, t_sub = item
+                res = req.wait(timeout_s=600)
+                t_done = time.perf_counter()
+                done_at[i] = t_done
+                lat[i] = (t_done - (t0 + arrivals[i])) * 1e3
+                digests[i] = _checksum(res)
+                req.close()
+
+        th = threading.Thread(target=waiter)
+        th.start()
+        for i, qq in enumerate(stream):
+            wait = t0 + arrivals[i] - time.perf_counter()
+            if wait > 0:
+                time.sleep(wait)
+            q.put((i, conn.submit(qq["sql"]), time.perf_counter()))
+        q.put(None)
+        th.join()
+    else:
+        for i, qq in enumerate(stream):
+            wait = t0 + arrivals[i] - time.perf_counter()
+            if wait > 0:
+                time.sleep(wait)
+            res = conn.gpu_processing(qq["sql"])
+            t_done = time.perf_counter()
+            done_at[i] = t_done
+            lat[i] = (t_done - (t0 + arrivals[i])) * 1e3
+            digests[i] = _checksum(res)
+    makespan = max(done_at) - t0
+    return lat, makespan, digests
+
+
+def run_served(args):
+    """Served mixed stream (2,000 queries, Poisson arrivals at swept rates)
+    against the same stream as plain one-query-at-a-time launches."""
+    ws, rank, local = dist_env()
+    import torch
+    torch.cuda.set_device(local)
+    dist = dist_init(ws)
+    from mettle_b200 import Connection
+    from mettle_b200 import _lib as L
+    os.environ["METTLE_DISABLE_QUERY_CACHE"] = "1"  # every query runs on the device
+    tables = W.served_tables()
+    stream = W.served_stream(args.c5_queries)
+    conn = Connection(device=local)
+    conn.execute("CALL gpu_buffer_init('40 GB', '20 GB')")
+    for name, (tpl, d) in tables.items():
+        if tpl == "c1":
+            conn.create_table(name, {"value": (L.T_INTEGER, d["value"])})
+        elif tpl == "c2":
+            conn.create_table(name, {"a": (L.T_INTEGER, d["a"]), "b": (L.T_BIGINT, d["b"]),
+                                     "c": (L.T_FLOAT, d["c"]), "d": (L.T_DATE, d["d"]),
+                                     "e": (L.T_TIMESTAMP, d["e"])})
+        else:
+            conn.create_table(name, {"k": (L.T_BIGINT, d["k"]), "v": (L.T_BIGINT, d["v"]),
+                                     "f": (L.T_FLOAT, d["f"])})
+        conn.gpu_register_table(name, upload=True)
+    # warm: plans, statistics and column uploads for every template/table
+    seen = set()
+    for qq in stream:
+        key = (qq["tpl"], qq["table"], qq.get("col"))
+        if key not in seen:
+            seen.add(key)
+            conn.gpu_processing(qq["sql"])
+    # oracle spot checks of the first queries of each template
+    parity_oracle = True
+    if rank == 0:
+        checked = set()
+        for qq in stream:
+            if qq["tpl"] in checked or (qq["tpl"] != "c3" and tables[qq["table"]][1].get("a", np.empty(0)).size > 20_000_000):
+                continue
+            checked.add(qq["tpl"])
+            res = conn.gpu_processing(qq["sql"])
+            want = _oracle_query(qq, tables)
+            if qq["tpl"] == "c3":
+                parity_oracle &= bool(np.array_equal(res.columns[0], want["k"]) and
+                                      np.array_equal(res.columns[2], want["cnt"]))
+            else:
+                parity_oracle &= bool(np.array_equal(res.columns[0], want))
+    # closed-loop plain capacity on a prefix of the stream sets the swept rates
+    pre = stream[: min(len(stream), 200)]
+    _, mk, _ = _run_stream(conn, pre, [0.0] * len(pre), served=False)
+    plain_cap = len(pre) / mk
+    rng = np.random.default_rng(11)
+    sweep = []
+    for factor in args.c5_rates:
+        rate = plain_cap * factor
+        gaps = rng.exponential(1.0 / rate, len(stream))
+        arrivals = np.cumsum(gaps) - gaps[0]
+        barrier(dist, local)
+        pl, pmk, pdig = _run_stream(conn, stream, arrivals, served=False)
+        barrier(dist, local)
+        sl, smk, sdig = _run_stream(conn, stream, arrivals, served=True)
+        same = all(_same(a, b) for a, b in zip(pdig, sdig))
+        n = len(stream)
+        sweep.append({
+            "offered_qps": rate, "rate_factor": factor,
+            "served": {"qps": n / smk, "p50_ms": float(np.percentile(sl, 50)), "p99_ms": float(np.percentile(sl, 99))},
+            "plain": {"qps": n / pmk, "p50_ms": float(np.percentile(pl, 50)), "p99_ms": float(np.percentile(pl, 99))},
+            "identical": same})
+    top = sweep[-1]
+    served_qps = reduce_sum(dist, top["served"]["qps"], f"cuda:{local}")
+    st = conn.serve_stats()
+    cpu = None
+    if rank == 0 and ws == 1 and args.cpu_seconds > 0:
+        import oracle as orc
+        t0, k = time.perf_counter(), 0
+        while time.perf_counter() - t0 < args.cpu_seconds and k < len(stream):
+            _oracle_query(stream[k], tables)
+            k += 1
+        el = time.perf_counter() - t0
+        cpu = {"value": k / el, "unit": "queries/s", "cores": orc.threads(), "kind": "port",
+               "sample": f"first {k} queries of the stream run back to back through the OpenMP oracle "
+                         f"({el:.1f} s; scan queries gather one column)"}
+    if rank == 0:
+        line = {
+            "metric": "served queries/s", "value": served_qps, "unit": "queries/s", "n_gpus": ws,
+            "steps": len(stream), "warmup": len(seen), "ms_per_step": 1e3 / top["served"]["qps"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64",
+            "data": "synthetic",
+            "config": {"workload": f"c5 served mixed stream: {len(stream)} queries (templates c1/c2/c3, tables 1M-60M "
+                                   "rows), Poisson arrivals swept as multiples of the plain closed-loop rate; "
+                                   "gpu_buffer_init('40 GB','20 GB')",
+                       "l2": "tables larger than L2 (126 MB) except the 1M-row ones; no flush",
+                       "parallelism": f"replicas x{ws}" if ws > 1 else "1 GPU"},
+            "p50_ms": top["served"]["p50_ms"], "p99_ms": top["served"]["p99_ms"],
+            "plain": top["plain"], "sweep": sweep, "identical": all(s["identical"] for s in sweep),
+            "parity_oracle": parity_oracle, "plain_closed_loop_qps": plain_cap,
+            "roofline": None, "cpu_baseline": cpu,
+            "e2e": {"value": served_qps, "unit": "queries/s", "h2d_bytes_per_step": len(stream[0]["sql"]),
+                    "d2h_bytes_per_step": None,
+                    "note": "columns resident in the HBM column cache (the served form); results downloaded"},
+            "gpu_launches": None, "serve_stats": st,
+        }
+        print(json.dumps(line), flush=True)
+    conn.close()
+    if dist is not None:
+        dist.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="mettle", choices=["mettle", "reference"])
-    ap.add_argument("--config", default="c4", choices=["c1", "c2", "c3", "c4"])
+    ap.add_argument("--config", default="c4", choices=["c1", "c2", "c3", "c4", "c5"])
+    ap.add_argument("--c5-queries", type=int, default=2000)
+    ap.add_argument("--c5-rates", type=float, nargs="+", default=[0.5, 1.0, 2.0])
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
+    elif args.config == "c5":
+        run_served(args)
     else:
         run_mettle(args)
 

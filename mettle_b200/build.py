@@ -70,7 +70,8 @@ def build(verbose: bool = False, jobs: int | None = None) -> Path:
         objs = list(ex.map(lambda s: _compile(s, verbose), srcs))
     newest = max(o.stat().st_mtime for o in objs)
     if not LIB.exists() or LIB.stat().st_mtime < newest:
-        cmd = [nvcc(), *host_compiler(), *ARCH, "-shared", "-o", str(LIB), *map(str, objs), "-lpthread"]
+        cmd = [nvcc(), *host_compiler(), *ARCH, "-shared", "-o", str(LIB), *map(str, objs), "-lpthread",
+               "-Xlinker", "--no-undefined"]
         if verbose:
             print(" ".join(cmd), flush=True)
         res = subprocess.run(cmd, capture_output=True, text=True)

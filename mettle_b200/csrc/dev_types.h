@@ -83,6 +83,8 @@ struct VmIns {
 struct VmProg {
   int32_t n;
   int32_t out_type;
+  int32_t depth;  // deepest stack the program reaches
+  int32_t pad;
   VmIns ins[kMaxIns];
 };
 
@@ -106,6 +108,8 @@ struct DBuild {
   uint32_t* hash_special;   // hash: slot + 1 of the key equal to kEmptyKey
   uint32_t* payload[kMaxSrc];  // payload[s][slot] = row id of source s
   uint32_t* n_slots;        // number of slots assigned (device counter)
+  int32_t unique_keys;      // the key column holds no duplicates (no check needed)
+  int32_t pad;
 };
 
 struct DProbe {

@@ -592,6 +592,12 @@ struct Compiler {
     memset(&p, 0, sizeof(p));
     emit(pb, p, e);
     p.out_type = e.ptype;
+    int sp = 0;
+    for (int k = 0; k < p.n; ++k) {
+      const int16_t op = p.ins[k].op;
+      if (op == VM_COL || op == VM_CONST || op == VM_SLOT) p.depth = std::max(p.depth, ++sp);
+      else if (op != VM_CAST && op != VM_NEG) --sp;
+    }
     return i;
   }
 
@@ -612,6 +618,7 @@ struct Compiler {
     column_minmax(ctx, k);
     const uint64_t rows = t.rows;
     b.key_ptype = storage_ptype(k.type);
+    b.unique_keys = (k.has_unique && k.unique) ? 1 : 0;
     b.n_slots = (uint32_t*)scratch(8);
     memset_step(b.n_slots, 0, 8);
     bool dense = false;
@@ -1215,17 +1222,14 @@ struct Compiler {
       fill_aggs(pb, true);
       push_pipeline(pb, root_rows);
       const uint64_t cap = std::max<uint64_t>(1, plan.sources[rep_src].table->rows);
-      uint32_t* gidx = (uint32_t*)scratch(cap * 4);
-      uint64_t* gcnt = (uint64_t*)scratch(8);
-      compact_step(slot_hit, cap, (const uint64_t*)builds[rep_src].n_slots, gidx, gcnt, false);
+      const uint64_t* n_dev = (const uint64_t*)builds[rep_src].n_slots;
       std::vector<FinalOut> fo;
       for (size_t i = 0; i < plan.outputs.size(); ++i) {
         const BOut& o = plan.outputs[i];
         dense[i].ptype = storage_ptype(o.type);
         dense[i].width = ptype_width(dense[i].ptype);
-        dense[i].dev = scratch(cap * dense[i].width);
         if (o.agg_idx >= 0) {
-          fo.push_back(agg_final((int)i, dense[i].dev));
+          fo.push_back(agg_final((int)i, nullptr));
         } else {
           FinalOut f;
           memset(&f, 0, sizeof(f));
@@ -1235,10 +1239,14 @@ struct Compiler {
           f.col = column_device(ctx, *c);
           pinned_cols.insert(c);
           f.rid = builds[rep_src].payload[rep_src];
-          f.out = dense[i].dev;
           fo.push_back(f);
         }
       }
+      if (agg_topk_fused(fo, slot_hit, nullptr, n_dev, cap, tie)) return;
+      uint32_t* gidx = (uint32_t*)scratch(cap * 4);
+      uint64_t* gcnt = (uint64_t*)scratch(8);
+      compact_step(slot_hit, cap, n_dev, gidx, gcnt, false);
+      for (size_t i = 0; i < fo.size(); ++i) fo[i].out = dense[i].dev = scratch(cap * dense[i].width);
       finalize_step(upload_finals(fo), (int)fo.size(), gidx, gcnt, cap);
       order_and_limit(gcnt, cap, tie);
       return;
@@ -1266,29 +1274,96 @@ struct Compiler {
       }
     }
     push_pipeline(pb, root_rows);
-    uint32_t* gidx = (uint32_t*)scratch(cap * 4);
-    uint64_t* gcnt = (uint64_t*)scratch(8);
-    compact_step(pb.d.table.state, cap, nullptr, gidx, gcnt, true);
     std::vector<FinalOut> fo;
     for (size_t i = 0; i < plan.outputs.size(); ++i) {
       const BOut& o = plan.outputs[i];
       dense[i].ptype = storage_ptype(o.type);
       dense[i].width = ptype_width(dense[i].ptype);
-      dense[i].dev = scratch(cap * dense[i].width);
       if (o.agg_idx >= 0) {
-        fo.push_back(agg_final((int)i, dense[i].dev));
+        fo.push_back(agg_final((int)i, nullptr));
       } else {
         FinalOut f;
         memset(&f, 0, sizeof(f));
         const int32_t pt = dense[i].ptype;
         f.kind = pt == P_I32 ? F_COPY_I32 : pt == P_F32 ? F_COPY_F32 : F_COPY_I64;
         f.a = pb.d.table.keys[o.group_idx];
-        f.out = dense[i].dev;
         fo.push_back(f);
       }
     }
+    if (agg_topk_fused(fo, nullptr, pb.d.table.state, nullptr, cap, tie)) return;
+    uint32_t* gidx = (uint32_t*)scratch(cap * 4);
+    uint64_t* gcnt = (uint64_t*)scratch(8);
+    compact_step(pb.d.table.state, cap, nullptr, gidx, gcnt, true);
+    for (size_t i = 0; i < fo.size(); ++i) fo[i].out = dense[i].dev = scratch(cap * dense[i].width);
     finalize_step(upload_finals(fo), (int)fo.size(), gidx, gcnt, cap);
     order_and_limit(gcnt, cap, tie);
+  }
+
+  // Aggregate ORDER BY ... LIMIT K with K <= 32: one fused top-K over the
+  // live groups' states (no compaction, per-group outputs or key array),
+  // then the visible outputs of the K winners only. Returns false when the
+  // query needs the general path.
+  bool agg_topk_fused(const std::vector<FinalOut>& fo, const uint8_t* flag, const uint32_t* state,
+                      const uint64_t* n_dev, uint64_t cap, const std::vector<int>& tie_outs) {
+    if (plan.order.empty() || plan.limit < 1 || plan.limit > 32 || cap == 0 || cap >= 0xFFFFFFFFull) return false;
+    TopkFinalSpec ts;
+    memset(&ts, 0, sizeof(ts));
+    int bits = 0;
+    auto part_bits = [](int32_t pt) { return pt == P_I128 ? 128 : (pt == P_I32 || pt == P_F32) ? 32 : 64; };
+    auto add_part = [&](int out_i, bool desc) {
+      const int32_t pt = dense[out_i].ptype;
+      if (bits + part_bits(pt) > 256 || ts.n_parts >= kMaxOrder) return false;
+      ts.ptype[ts.n_parts] = pt;
+      ts.desc[ts.n_parts] = desc ? 1 : 0;
+      ts.part[ts.n_parts] = fo[out_i];
+      ts.n_parts++;
+      bits += part_bits(pt);
+      return true;
+    };
+    for (const BOrder& o : plan.order)
+      if (!add_part(o.out, o.desc)) return false;
+    for (int t : tie_outs) {
+      bool in_order = false;
+      for (const BOrder& o : plan.order) in_order |= o.out == t;
+      if (!in_order) add_part(t, false);
+    }
+    ts.total_bits = bits;
+    ts.bits0 = part_bits(ts.ptype[0]);
+    ts.flag = flag;
+    ts.state = state;
+    ts.n_dev = n_dev;
+    ts.n_max = cap;
+    const int K = (int)plan.limit;
+    uint32_t* og = (uint32_t*)scratch((uint64_t)K * 4);
+    uint64_t* oc = (uint64_t*)scratch(8);
+    Step t;
+    t.k = Step::TOPK_FINAL;
+    t.tfs = ts;
+    t.topk = K;
+    t.out_idx = og;
+    t.out_count = oc;
+    t.temp = scratch(topk_final_temp_bytes(cap, K));
+    P.steps.push_back(t);
+    P.kernels += 2;
+    std::vector<FinalOut> vis;
+    for (size_t i = 0; i < plan.outputs.size(); ++i) {
+      if (plan.outputs[i].hidden) continue;
+      FinalOut f = fo[i];
+      f.out = scratch((uint64_t)K * dense[i].width);
+      vis.push_back(f);
+      OutBuf ob;
+      ob.name = plan.outputs[i].name;
+      ob.type = plan.outputs[i].type;
+      ob.dev = f.out;
+      ob.width = dense[i].width;
+      ob.dict = plan.outputs[i].dict;
+      P.outs.push_back(ob);
+    }
+    if (!vis.empty()) finalize_step(upload_finals(vis), (int)vis.size(), og, oc, (uint64_t)K);
+    P.limit = plan.limit;
+    P.out_count = oc;
+    P.n_max = (uint64_t)K;
+    return true;
   }
 
   void compact_step(const void* flag, uint64_t n, const uint64_t* n_dev, uint32_t* out_idx, uint64_t* out_count,
@@ -1456,6 +1531,7 @@ static const char* step_kind_name(Step::Kind k) {
     case Step::ENCODE: return "encode_keys";
     case Step::RADIX: return "radix_sort";
     case Step::TOPK: return "topk";
+    case Step::TOPK_FINAL: return "topk_states";
     case Step::GATHER: return "gather";
   }
   return "step";
@@ -1496,6 +1572,7 @@ void run_program(Ctx& ctx, Program& p, cudaStream_t s) {
         CK(launch_topk(st.keys, st.kidx, st.count, st.n_max, st.topk, st.out_idx, st.out_count, st.temp, p.status,
                        s));
         break;
+      case Step::TOPK_FINAL: CK(launch_topk_final(st.tfs, st.topk, st.out_idx, st.out_count, st.temp, s)); break;
       case Step::GATHER: CK(launch_gather_width(st.gin, st.width, st.idx, st.count, st.n_max, st.gout, s)); break;
     }
     if (p.profile) CK(cudaEventRecord(p.prof_ev[2 * i + 1], s));

@@ -1,5 +1,6 @@
 // k_misc.cu — compaction of aggregate tables, final aggregate outputs,
 // gathers, the scalar SQL hooks and column statistics (sm_100a).
+#include "final_common.cuh"
 #include "kern_common.cuh"
 #include "kernels.h"
 
@@ -142,68 +143,6 @@ cudaError_t launch_gather_width(const void* in, int width, const uint32_t* idx, 
 }
 
 // ------------------------------------------------------------ finalize
-// AVG of a 128-bit integer sum as DuckDB computes it on x86-64
-// (IntegerAverageOperationHugeint): the quotient is formed in x87 extended
-// precision (64-bit significand, round to nearest even) and then stored as
-// a double (a second rounding to 53 bits). Emulated exactly with integer
-// arithmetic; the sum is assumed below 2^64 in magnitude (the long double
-// image of larger sums is rounded, and this emulation rounds it the same
-// way only when the discarded bits are not a tie).
-__device__ double avg_extended(__int128 sum, unsigned long long count) {
-  if (sum == 0 || count == 0) return 0.0;
-  const bool neg = sum < 0;
-  unsigned __int128 S = neg ? (unsigned __int128)(-sum) : (unsigned __int128)sum;
-  const unsigned __int128 C = count;
-  int lenS = 0;
-  {
-    uint64_t hi = (uint64_t)(S >> 64), lo = (uint64_t)S;
-    lenS = hi ? 128 - __clzll((long long)hi) : 64 - __clzll((long long)lo);
-  }
-  // Round S itself to a 64-bit significand if it is wider.
-  int sexp = 0;
-  if (lenS > 64) {
-    int drop = lenS - 64;
-    unsigned __int128 q = S >> drop, rem = S & ((((unsigned __int128)1) << drop) - 1);
-    unsigned __int128 half = ((unsigned __int128)1) << (drop - 1);
-    if (rem > half || (rem == half && (q & 1))) q += 1;
-    if (q >> 64) { q >>= 1; drop += 1; }
-    S = q;
-    sexp = drop;
-    lenS = 64;
-  }
-  const int lenC = 64 - __clzll((long long)count);
-  // Quotient with a 64-bit significand: Q = floor(S * 2^k / C).
-  int k = 64 - (lenS - lenC);
-  unsigned __int128 Q, R, D;
-  for (int attempt = 0; attempt < 3; ++attempt) {
-    if (k >= 0) {
-      unsigned __int128 N = S << k;
-      D = C;
-      Q = N / D;
-      R = N % D;
-    } else {
-      D = C << (-k);
-      Q = S / D;
-      R = S % D;
-    }
-    if (Q >> 64) { --k; continue; }
-    if (!(Q >> 63)) { ++k; continue; }
-    break;
-  }
-  // Round to 64 bits (nearest even) on the exact remainder.
-  unsigned __int128 twoR = R << 1;
-  if (twoR > D || (twoR == D && (Q & 1))) Q += 1;
-  if (Q >> 64) { Q >>= 1; --k; }
-  // Second rounding, 64 -> 53 bits, on the 11 dropped bits alone.
-  uint64_t q64 = (uint64_t)Q;
-  uint64_t low = q64 & 0x7FFULL, m = q64 >> 11;
-  if (low > 0x400ULL || (low == 0x400ULL && (m & 1))) m += 1;
-  int e = 11 - k + sexp;
-  if (m >> 53) { m >>= 1; e += 1; }
-  double r = ldexp((double)m, e);
-  return neg ? -r : r;
-}
-
 __global__ void k_finalize(const FinalOut* __restrict__ outs, int n_outs, const uint32_t* __restrict__ idx,
                            const uint64_t* count, uint64_t n_max) {
   const uint64_t n = count ? *count : n_max;
@@ -211,44 +150,19 @@ __global__ void k_finalize(const FinalOut* __restrict__ outs, int n_outs, const 
     const uint64_t g = idx ? idx[i] : i;
     for (int o = 0; o < n_outs; ++o) {
       const FinalOut f = outs[o];
+      uint64_t lo, hi;
+      final_value(f, g, lo, hi);
       switch (f.kind) {
+        case F_SUM_I128:
+        case F_SUM_I64_AS_I128: ((longlong2*)f.out)[i] = make_longlong2((long long)lo, (long long)hi); break;
         case F_COPY_I32:
-        case F_COPY_F32: ((uint32_t*)f.out)[i] = (uint32_t)f.a[g]; break;
-        case F_COPY_I64:
-        case F_COPY_F64: ((uint64_t*)f.out)[i] = f.a[g]; break;
-        case F_SUM_I128: ((longlong2*)f.out)[i] = make_longlong2((long long)f.a[g], (long long)f.a_hi[g]); break;
-        case F_SUM_I64_AS_I128: {
-          long long v = (long long)f.a[g];
-          ((longlong2*)f.out)[i] = make_longlong2(v, v < 0 ? -1LL : 0LL);
+        case F_COPY_F32:
+        case F_MINMAX_F32: ((uint32_t*)f.out)[i] = (uint32_t)lo; break;
+        case F_GATHER_COL:
+          if (f.width == 4) ((uint32_t*)f.out)[i] = (uint32_t)lo;
+          else ((uint64_t*)f.out)[i] = lo;
           break;
-        }
-        case F_MINMAX_F32: ((float*)f.out)[i] = (float)unord_f64(f.a[g]); break;
-        case F_MINMAX_F64: ((double*)f.out)[i] = unord_f64(f.a[g]); break;
-        case F_AVG_I128_LD: {
-          __int128 s = f.a_hi ? (__int128)(((unsigned __int128)(uint64_t)f.a_hi[g] << 64) | f.a[g])
-                              : (__int128)(long long)f.a[g];
-          ((double*)f.out)[i] = avg_extended(s, f.cnt[g]);
-          break;
-        }
-        case F_AVG_I64_D:
-          ((double*)f.out)[i] = __ddiv_rn(__ll2double_rn((long long)f.a[g]), __ull2double_rn(f.cnt[g]));
-          break;
-        case F_AVG_F64:
-          ((double*)f.out)[i] = __ddiv_rn(__longlong_as_double((long long)f.a[g]), __ull2double_rn(f.cnt[g]));
-          break;
-        case F_AVG_DEC: {
-          __int128 s = f.a_hi ? (__int128)(((unsigned __int128)(uint64_t)f.a_hi[g] << 64) | f.a[g])
-                              : (__int128)(long long)f.a[g];
-          ((double*)f.out)[i] = avg_extended(s, f.cnt[g] * (unsigned long long)f.scale);
-          break;
-        }
-        case F_GATHER_COL: {
-          const uint32_t r = f.rid[g];
-          if (f.width == 4) ((uint32_t*)f.out)[i] = ((const uint32_t*)f.col)[r];
-          else ((uint64_t*)f.out)[i] = ((const uint64_t*)f.col)[r];
-          break;
-        }
-        default: break;
+        default: ((uint64_t*)f.out)[i] = lo; break;
       }
     }
   }

@@ -68,7 +68,8 @@ __device__ __forceinline__ void build_insert(const DBuild& b, int64_t key, uint3
     // launch, so the plain store is visible to them.
     b.dense_map[k] = slot + 1;
     const uint32_t bit = 1u << (k & 31);
-    if (atomicOr(b.dense_bits + (k >> 5), bit) & bit) st |= ST_DUP_BUILD_KEY;
+    if (b.unique_keys) atomicOr(b.dense_bits + (k >> 5), bit);  // no reply needed
+    else if (atomicOr(b.dense_bits + (k >> 5), bit) & bit) st |= ST_DUP_BUILD_KEY;
     return;
   }
   if (key == kEmptyKey) {
@@ -327,18 +328,57 @@ __device__ __forceinline__ int64_t stream_value(const StreamLayout& S, const uin
   return ((const int64_t*)(buf + S.off[k]))[r];
 }
 
-__device__ __forceinline__ int64_t tc_get(const TileCtx& t, int col, uint32_t r) {
+// Where one column's values come from in this tile, resolved once per op:
+// the streamed tile buffer, or the column in HBM through the row id of its
+// source.
+struct ColAcc {
+  const uint8_t* sm;  // streamed tile buffer of the column, or null
+  const void* g;
+  int32_t ptype;
+  int32_t src;
+  int32_t width;
+};
+
+__device__ __forceinline__ ColAcc col_acc(const TileCtx& t, int col) {
   const DCol& c = t.d->cols[col];
+  ColAcc a{nullptr, c.ptr, c.ptype, c.src, ptype_width(c.ptype)};
   if (c.src == t.d->drive_src) {
     const int k = stream_index(*t.S, col);
-    if (k >= 0) return stream_value(*t.S, t.buf, k, c.ptype, r);
+    if (k >= 0) a.sm = t.buf + t.S->off[k];
   }
-  return load_bits(c.ptr, c.ptype, tc_rid(t, c.src, r));
+  return a;
 }
 
-// Expression VM over one tile row.
-__device__ Val vm_eval_t(const VmProg& p, const TileCtx& t, uint32_t r, uint32_t& st) {
-  Val stack[6];
+__device__ __forceinline__ int64_t acc_get(const ColAcc& a, const TileCtx& t, uint32_t r) {
+  if (a.sm) {
+    if (a.width == 4)
+      return a.ptype == P_I32 ? (int64_t)((const int32_t*)a.sm)[r] : (int64_t)((const uint32_t*)a.sm)[r];
+    return ((const int64_t*)a.sm)[r];
+  }
+  return load_bits(a.g, a.ptype, tc_rid(t, a.src, r));
+}
+
+__device__ __forceinline__ int64_t tc_get(const TileCtx& t, int col, uint32_t r) {
+  return acc_get(col_acc(t, col), t, r);
+}
+
+// Stack slots of the expression VM held in registers. Every instruction's
+// stack position depends on the program only, so it is the same in all
+// lanes and the slot selects below are uniform branches.
+struct RegStack {
+  Val s0, s1, s2, s3;
+  __device__ __forceinline__ Val get(int i) const { return i == 0 ? s0 : i == 1 ? s1 : i == 2 ? s2 : s3; }
+  __device__ __forceinline__ void put(int i, const Val& v) {
+    if (i == 0) s0 = v;
+    else if (i == 1) s1 = v;
+    else if (i == 2) s2 = v;
+    else s3 = v;
+  }
+};
+
+// Programs deeper than the register stack.
+__device__ __noinline__ Val vm_eval_deep(const VmProg& p, const TileCtx& t, uint32_t r, uint32_t& st) {
+  Val stack[kMaxIns];
   int sp = 0;
   for (int i = 0; i < p.n; ++i) {
     const VmIns& in = p.ins[i];
@@ -383,6 +423,53 @@ __device__ Val vm_eval_t(const VmProg& p, const TileCtx& t, uint32_t r, uint32_t
   return stack[0];
 }
 
+// Expression VM over one tile row.
+__device__ __forceinline__ Val vm_eval_t(const VmProg& p, const TileCtx& t, uint32_t r, uint32_t& st) {
+  if (p.depth > 4) return vm_eval_deep(p, t, r, st);
+  RegStack S;
+  S.s0 = S.s1 = S.s2 = S.s3 = Val{0, 0};
+  int sp = 0;
+  for (int i = 0; i < p.n; ++i) {
+    const VmIns& in = p.ins[i];
+    switch (in.op) {
+      case VM_COL: {
+        const int32_t pt = t.d->cols[in.arg].ptype;
+        Val v;
+        v.lo = tc_get(t, in.arg, r);
+        v.hi = (pt == P_I32 || pt == P_I64) ? (v.lo >> 63) : 0;
+        S.put(sp++, v);
+        break;
+      }
+      case VM_CONST:
+        S.put(sp++, Val{in.k, in.k2});
+        break;
+      case VM_CAST:
+        S.put(sp - 1, vm_cast(S.get(sp - 1), in.arg, in.type, in.k, in.k2, st));
+        break;
+      case VM_NEG: {
+        Val v = S.get(sp - 1);
+        if (in.type == P_F32 || in.type == P_F64)
+          v.lo ^= (in.type == P_F32) ? (int64_t)0x80000000LL : (int64_t)0x8000000000000000ULL;
+        else
+          v = vm_arith(VM_SUB, in.type, Val{0, 0}, v, st);
+        S.put(sp - 1, v);
+        break;
+      }
+      case VM_SLOT:
+        S.put(sp++, Val{0, 0});
+        break;
+      default: {
+        const Val b = S.get(sp - 1);
+        const Val a = S.get(sp - 2);
+        --sp;
+        S.put(sp - 1, vm_arith(in.op, in.type, a, b, st));
+        break;
+      }
+    }
+  }
+  return S.s0;
+}
+
 // Warp-aggregated append of tile row r to a shared selection list. Every
 // lane of the warp must call it (keep may be false).
 __device__ __forceinline__ void sel_push(bool keep, uint32_t r, uint16_t* out, uint32_t* cnt) {
@@ -416,18 +503,42 @@ __device__ __forceinline__ IntRange to_range(const DPred& p) {
 }
 
 // Filter op over the current selection: one loop per (column type, source),
-// chosen once per tile.
+// chosen once per tile. A thread evaluates all of its (at most kTile /
+// kThreads) rows before the first ballot, so their loads are in flight
+// together, and each warp reserves its output range with one atomic.
 template <typename GET>
 __device__ __forceinline__ void filter_loop(uint32_t n_sel, bool ident, const uint16_t* in, uint16_t* out,
                                             uint32_t* cnt, GET get_keep) {
-  for (uint32_t i0 = 0; i0 < n_sel; i0 += kThreads) {
-    const uint32_t i = i0 + threadIdx.x;
-    const bool act = i < n_sel;
-    const uint32_t r = act ? (ident ? i : (uint32_t)in[i]) : 0u;
-    const bool keep = act && get_keep(r);
-    sel_push(keep, r, out, cnt);
+  constexpr int U = kTile / kThreads;
+  const int lane = threadIdx.x & 31;
+  uint32_t km = 0;  // bit j: row j of this thread is kept
+#pragma unroll
+  for (int j = 0; j < U; ++j) {
+    const uint32_t i = (uint32_t)j * kThreads + threadIdx.x;
+    if (i < n_sel && get_keep(ident ? i : (uint32_t)in[i])) km |= 1u << j;
+  }
+  uint32_t tot = 0;
+#pragma unroll
+  for (int j = 0; j < U; ++j) tot += __popc(__ballot_sync(0xFFFFFFFFu, (km >> j) & 1u));
+  uint32_t base = 0;
+  if (lane == 0 && tot) base = atomicAdd(cnt, tot);
+  base = __shfl_sync(0xFFFFFFFFu, base, 0);
+  const uint32_t lt = (1u << lane) - 1u;
+#pragma unroll
+  for (int j = 0; j < U; ++j) {
+    const uint32_t m = __ballot_sync(0xFFFFFFFFu, (km >> j) & 1u);
+    if ((km >> j) & 1u) {
+      const uint32_t i = (uint32_t)j * kThreads + threadIdx.x;
+      out[base + __popc(m & lt)] = (uint16_t)(ident ? i : (uint32_t)in[i]);
+    }
+    base += __popc(m);
   }
 }
+
+// Join probe over the current selection, kProbeBatch rows per thread at a
+// time: keys, then the presence words and map entries (dense) or first
+// probed slots (hash) of the whole batch are loaded before any is used.
+constexpr int kProbeBatch = 4;
 
 template <int SINK>
 __global__ void __launch_bounds__(kThreads) k_pipeline(const __grid_constant__ PipeDesc d) {
@@ -612,32 +723,80 @@ __global__ void __launch_bounds__(kThreads) k_pipeline(const __grid_constant__ P
         const DBuild& bd = d.builds[pr.build];
         const bool want_slot = op.idx == d.slot_probe;
         const uint32_t fill = pr.fill_mask & ~(1u << d.drive_src);
-        for (uint32_t i0 = 0; i0 < n_sel; i0 += THREADS) {
-          const uint32_t i = i0 + tid;
-          const bool act = i < n_sel;
-          const uint32_t r = act ? (ident ? i : (uint32_t)sel_in[i]) : 0u;
-          bool keep = false;
-          uint32_t slot = 0;
-          if (act) {
-            const int64_t key = tc_get(tc, pr.key_col, r);
-            if (bd.kind == B_DENSE) {
-              const uint64_t kk = (uint64_t)(key - bd.key_min);
-              if (kk < bd.capacity && ((bd.dense_bits[kk >> 5] >> (kk & 31)) & 1u)) {
-                keep = true;
-                slot = bd.dense_map[kk] - 1u;
-              }
-            } else {
-              keep = build_lookup(bd, key, slot, st);
+        const int lane = tid & 31;
+        const uint32_t lt = (1u << lane) - 1u;
+        const ColAcc ka = col_acc(tc, pr.key_col);
+        (void)c;
+        for (uint32_t i0 = 0; i0 < n_sel; i0 += THREADS * kProbeBatch) {
+          uint32_t r[kProbeBatch], slot[kProbeBatch];
+          bool act[kProbeBatch], keep[kProbeBatch];
+          int64_t key[kProbeBatch];
+#pragma unroll
+          for (int j = 0; j < kProbeBatch; ++j) {
+            const uint32_t i = i0 + (uint32_t)j * THREADS + tid;
+            act[j] = i < n_sel;
+            r[j] = act[j] ? (ident ? i : (uint32_t)sel_in[i]) : 0u;
+            key[j] = act[j] ? acc_get(ka, tc, r[j]) : 0;
+          }
+          if (bd.kind == B_DENSE) {
+            uint32_t w[kProbeBatch], mv[kProbeBatch];
+            uint64_t kk[kProbeBatch];
+#pragma unroll
+            for (int j = 0; j < kProbeBatch; ++j) {
+              kk[j] = (uint64_t)(key[j] - bd.key_min);
+              const bool inb = act[j] && kk[j] < bd.capacity;
+              // The map entry is read beside its presence word; it is only
+              // used when the presence bit is set.
+              w[j] = inb ? bd.dense_bits[kk[j] >> 5] : 0u;
+              mv[j] = inb ? bd.dense_map[kk[j]] : 0u;
             }
-            if (keep) {
-              if (want_slot) s_slot[r] = slot;
-              for (int s = 0; s < kMaxSrc; ++s)
-                if ((fill >> s) & 1u)
-                  s_srid[(size_t)((slot_of_src >> (4 * s)) & 0xFu) * TILE + r] = bd.payload[s][slot];
+#pragma unroll
+            for (int j = 0; j < kProbeBatch; ++j) {
+              keep[j] = ((w[j] >> (kk[j] & 31)) & 1u) != 0;
+              slot[j] = mv[j] - 1u;
+            }
+          } else {
+            uint64_t h[kProbeBatch];
+            int64_t k0[kProbeBatch];
+#pragma unroll
+            for (int j = 0; j < kProbeBatch; ++j) {
+              h[j] = hash_slot(hash64((uint64_t)key[j]), bd.capacity);
+              k0[j] = (act[j] && key[j] != kEmptyKey) ? bd.hash_keys[h[j]] : kEmptyKey;
+            }
+#pragma unroll
+            for (int j = 0; j < kProbeBatch; ++j) {
+              keep[j] = false;
+              slot[j] = 0;
+              if (!act[j]) continue;
+              if (k0[j] == key[j] && key[j] != kEmptyKey) {
+                keep[j] = true;
+                slot[j] = bd.hash_slot[h[j]] - 1u;
+              } else if (k0[j] != kEmptyKey || key[j] == kEmptyKey) {
+                keep[j] = build_lookup(bd, key[j], slot[j], st);
+              }
             }
           }
-          (void)c;
-          sel_push(keep, r, sel_out, cnt);
+          uint32_t m[kProbeBatch];
+          uint32_t tot = 0;
+#pragma unroll
+          for (int j = 0; j < kProbeBatch; ++j) {
+            if (keep[j]) {
+              if (want_slot) s_slot[r[j]] = slot[j];
+              for (int s = 0; s < kMaxSrc; ++s)
+                if ((fill >> s) & 1u)
+                  s_srid[(size_t)((slot_of_src >> (4 * s)) & 0xFu) * TILE + r[j]] = bd.payload[s][slot[j]];
+            }
+            m[j] = __ballot_sync(0xFFFFFFFFu, keep[j]);
+            tot += __popc(m[j]);
+          }
+          uint32_t obase = 0;
+          if (lane == 0 && tot) obase = atomicAdd(cnt, tot);
+          obase = __shfl_sync(0xFFFFFFFFu, obase, 0);
+#pragma unroll
+          for (int j = 0; j < kProbeBatch; ++j) {
+            if (keep[j]) sel_out[obase + __popc(m[j] & lt)] = (uint16_t)r[j];
+            obase += __popc(m[j]);
+          }
         }
       }
       __syncthreads();
@@ -718,27 +877,23 @@ __global__ void __launch_bounds__(kThreads) k_pipeline(const __grid_constant__ P
             if (base + p < d.out_capacity) d.out_rids[s][base + p] = tc_rid(tc, s, s_list[p]);
     } else if (SINK == SK_BUILD) {
       const DBuild& bd = d.builds[d.sink_build];
-      for (uint32_t i0 = 0; i0 < n_sel; i0 += THREADS) {
-        const uint32_t i = i0 + tid;
-        const bool act = i < n_sel;
-        const uint32_t r = act ? (ident ? i : (uint32_t)sel_in[i]) : 0u;
-        const uint32_t m = __ballot_sync(0xFFFFFFFFu, act);
-        const int lane = tid & 31;
-        uint32_t sbase = 0;
-        if (lane == 0 && m) sbase = atomicAdd(bd.n_slots, (uint32_t)__popc(m));
-        sbase = __shfl_sync(0xFFFFFFFFu, sbase, 0);
-        if (act) {
-          const uint32_t slot = sbase + __popc(m & ((1u << lane) - 1u));
-          const int64_t key = tc_get(tc, d.build_key_col, r);
-          for (int s = 0; s < kMaxSrc; ++s)
-            if ((d.build_payload_mask >> s) & 1u) bd.payload[s][slot] = tc_rid(tc, s, r);
-          // A representative-row aggregate downstream keeps its states by
-          // this slot: initialize them here, so the (build-table sized)
-          // state arrays need no clearing per query.
-          for (int a = 0; a < d.n_aggs; ++a) agg_init_global(d.aggs[a], slot);
-          if (d.slot_hit) d.slot_hit[slot] = 0;
-          build_insert(bd, key, slot, st);
-        }
+      // One slot reservation per tile: the tile's surviving rows take
+      // consecutive slots.
+      if (tid == 0) s_base = n_sel ? (uint64_t)atomicAdd(bd.n_slots, n_sel) : 0;
+      __syncthreads();
+      const uint32_t sbase = (uint32_t)s_base;
+      for (uint32_t i = tid; i < n_sel; i += THREADS) {
+        const uint32_t r = ident ? i : (uint32_t)sel_in[i];
+        const uint32_t slot = sbase + i;
+        const int64_t key = tc_get(tc, d.build_key_col, r);
+        for (int s = 0; s < kMaxSrc; ++s)
+          if ((d.build_payload_mask >> s) & 1u) bd.payload[s][slot] = tc_rid(tc, s, r);
+        // A representative-row aggregate downstream keeps its states by
+        // this slot: initialize them here, so the (build-table sized)
+        // state arrays need no clearing per query.
+        for (int a = 0; a < d.n_aggs; ++a) agg_init_global(d.aggs[a], slot);
+        if (d.slot_hit) d.slot_hit[slot] = 0;
+        build_insert(bd, key, slot, st);
       }
     } else {
       for (uint32_t i = tid; i < n_sel; i += THREADS) {

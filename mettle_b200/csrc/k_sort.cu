@@ -7,6 +7,7 @@
 // 128-thread group with a serial merge (kernels.metal:1249); its tie order
 // (sum DESC, secondary ASC, row id ASC, kernels.metal:1102-1118) is kept by
 // encoding every ORDER BY part, then the tie-break parts, into one key.
+#include "final_common.cuh"
 #include "kern_common.cuh"
 #include "kernels.h"
 
@@ -26,27 +27,6 @@ int sms() {
 }  // namespace
 
 // ------------------------------------------------------------ key encoding
-struct U256 {
-  uint64_t w[4];  // w[0] most significant
-};
-
-__device__ __forceinline__ void shl_or(U256& k, int bits, uint64_t lo, uint64_t hi) {
-  // k = (k << bits) | value, value given as (hi, lo) with `bits` significant bits.
-  while (bits > 0) {
-    int b = bits > 64 ? 64 : bits;
-    uint64_t part = bits > 64 ? hi : lo;
-    if (bits > 64) bits -= 64; else bits = 0;
-    if (b == 64) {
-      k.w[0] = k.w[1]; k.w[1] = k.w[2]; k.w[2] = k.w[3]; k.w[3] = part;
-    } else {
-      k.w[0] = (k.w[0] << b) | (k.w[1] >> (64 - b));
-      k.w[1] = (k.w[1] << b) | (k.w[2] >> (64 - b));
-      k.w[2] = (k.w[2] << b) | (k.w[3] >> (64 - b));
-      k.w[3] = (k.w[3] << b) | (part & ((1ULL << b) - 1));
-    }
-  }
-}
-
 __global__ void k_encode(const __grid_constant__ SortKeySpec spec, const uint64_t* count, uint64_t n_max,
                          SortItem* __restrict__ keys, uint32_t* __restrict__ idx) {
   const uint64_t n = count ? *count : n_max;
@@ -55,37 +35,20 @@ __global__ void k_encode(const __grid_constant__ SortKeySpec spec, const uint64_
     for (int p = 0; p < spec.n_parts; ++p) {
       const int pt = spec.ptype[p];
       uint64_t lo = 0, hi = 0;
-      int bits = 64;
       switch (pt) {
         case P_I32:
-          lo = (uint64_t)(uint32_t)(((const int32_t*)spec.col[p])[i] ^ (int32_t)0x80000000);
-          bits = 32;
-          break;
-        case P_F32: {
-          uint32_t b = ((const uint32_t*)spec.col[p])[i];
-          lo = (b & 0x80000000u) ? (uint64_t)(~b) : (uint64_t)(b | 0x80000000u);
-          lo &= 0xFFFFFFFFULL;
-          bits = 32;
-          break;
-        }
-        case P_I64: lo = ord_i64(((const int64_t*)spec.col[p])[i]); break;
-        case P_F64: lo = ord_f64_bits(((const uint64_t*)spec.col[p])[i]); break;
+        case P_F32: lo = ((const uint32_t*)spec.col[p])[i]; break;
+        case P_I64:
+        case P_F64: lo = ((const uint64_t*)spec.col[p])[i]; break;
         case P_I128: {
-          // longlong2 {lo, hi}: flip the sign bit of hi for an unsigned image.
-          longlong2 v = ((const longlong2*)spec.col[p])[i];
+          const longlong2 v = ((const longlong2*)spec.col[p])[i];
           lo = (uint64_t)v.x;
-          hi = (uint64_t)v.y ^ 0x8000000000000000ULL;
-          bits = 128;
+          hi = (uint64_t)v.y;
           break;
         }
         default: break;
       }
-      if (spec.desc[p]) {
-        lo = ~lo;
-        hi = ~hi;
-        if (bits == 32) lo &= 0xFFFFFFFFULL;
-      }
-      shl_or(k, bits, lo, hi);
+      key_part(k, pt, spec.desc[p] != 0, lo, hi);
     }
     SortItem it;
     it.w[0] = k.w[0]; it.w[1] = k.w[1]; it.w[2] = k.w[2]; it.w[3] = k.w[3];
@@ -470,6 +433,125 @@ __global__ void __launch_bounds__(THREADS) k_topk_warp(const SortItem* __restric
       out_idx[(uint64_t)blockIdx.x * K + lane] = L.ix;
     }
   }
+}
+
+// Fused aggregate top-K (K <= 32): the ORDER BY image of each live group is
+// computed from its aggregate states and offered straight to the warp lists,
+// so no per-group output columns, key array or compacted group list is
+// written. Ties are broken by the group index, which orders groups the same
+// way as the order-preserving compaction the unfused path uses. A group
+// whose first ORDER BY part alone already places it after the warp's current
+// K-th key is dropped before its other parts (often gathers through a
+// representative row) are read.
+__device__ __forceinline__ bool u256_gt(const U256& a, const Cand& b) {
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+    if (a.w[i] != b.w[i]) return a.w[i] > b.w[i];
+  return false;
+}
+
+template <int THREADS, int U>
+__global__ void __launch_bounds__(THREADS) k_topk_final(const __grid_constant__ TopkFinalSpec spec, int K,
+                                                        SortItem* __restrict__ out_keys,
+                                                        uint32_t* __restrict__ out_idx) {
+  constexpr int WARPS = THREADS / 32;
+  __shared__ Cand s_l[WARPS][32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint64_t n = spec.n_dev ? (*spec.n_dev < spec.n_max ? *spec.n_dev : spec.n_max) : spec.n_max;
+  const uint64_t per = (n + gridDim.x - 1) / gridDim.x;
+  const uint64_t lo = (uint64_t)blockIdx.x * per;
+  const uint64_t hi = lo + per < n ? lo + per : n;
+  Cand L = cand_inf();
+  for (uint64_t base = lo + (uint64_t)warp * 32 * U; base < hi; base += (uint64_t)THREADS * U) {
+    bool v[U];
+    uint64_t g[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      g[u] = base + (uint64_t)u * 32 + lane;
+      v[u] = g[u] < hi;
+    }
+    if (spec.flag) {
+#pragma unroll
+      for (int u = 0; u < U; ++u) v[u] = v[u] && spec.flag[g[u]] != 0;
+    }
+    if (spec.state) {
+#pragma unroll
+      for (int u = 0; u < U; ++u) v[u] = v[u] && spec.state[g[u]] == 2u;
+    }
+    const Cand thr = cand_shfl(L, K - 1);
+    U256 k[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      k[u] = U256{{0, 0, 0, 0}};
+      if (v[u]) {
+        uint64_t vlo, vhi;
+        final_value(spec.part[0], g[u], vlo, vhi);
+        key_part(k[u], spec.ptype[0], spec.desc[0] != 0, vlo, vhi);
+        U256 probe = k[u];
+        shl_or(probe, spec.total_bits - spec.bits0, 0, 0);
+        if (u256_gt(probe, thr)) v[u] = false;
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      Cand c = cand_inf();
+      if (v[u]) {
+        for (int p = 1; p < spec.n_parts; ++p) {
+          uint64_t vlo, vhi;
+          final_value(spec.part[p], g[u], vlo, vhi);
+          key_part(k[u], spec.ptype[p], spec.desc[p] != 0, vlo, vhi);
+        }
+        c.w[0] = k[u].w[0]; c.w[1] = k[u].w[1]; c.w[2] = k[u].w[2]; c.w[3] = k[u].w[3];
+        c.ix = (uint32_t)g[u];
+      }
+      warp_offer(L, c, v[u], K, lane);
+    }
+  }
+  s_l[warp][lane] = L;
+  __syncthreads();
+  if (warp == 0) {
+    for (int w = 1; w < WARPS; ++w) {
+      const Cand c = s_l[w][lane];
+      warp_offer(L, c, lane < K && c.ix != 0xFFFFFFFFu, K, lane);
+    }
+    if (lane < K) {
+      SortItem it;
+      it.w[0] = L.w[0]; it.w[1] = L.w[1]; it.w[2] = L.w[2]; it.w[3] = L.w[3];
+      out_keys[(uint64_t)blockIdx.x * K + lane] = it;
+      out_idx[(uint64_t)blockIdx.x * K + lane] = L.ix;
+    }
+  }
+}
+
+constexpr int kTfThreads = 512;  // first pass
+constexpr int kTfItems = 2;      // groups per lane per step
+static unsigned topk_final_ctas(uint64_t n_max) {
+  static int per_sm = 0;
+  if (!per_sm) {
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_topk_final<kTfThreads, kTfItems>, kTfThreads, 0);
+    if (per_sm <= 0) per_sm = 1;
+  }
+  uint64_t ctas = (uint64_t)sms() * (uint64_t)per_sm;
+  const uint64_t want = (n_max + kTfThreads * kTfItems * 4 - 1) / (kTfThreads * kTfItems * 4);
+  if (want < ctas) ctas = want ? want : 1;
+  return (unsigned)ctas;
+}
+
+size_t topk_final_temp_bytes(uint64_t n_max, int k) {
+  return (size_t)topk_final_ctas(n_max) * (size_t)k * (sizeof(SortItem) + sizeof(uint32_t)) + 256;
+}
+
+cudaError_t launch_topk_final(const TopkFinalSpec& spec, int k, uint32_t* out_g, uint64_t* out_count, void* temp,
+                              cudaStream_t s) {
+  if (k <= 0 || k > 32 || spec.n_parts <= 0 || spec.n_parts > kMaxOrder || spec.total_bits > 256 ||
+      spec.bits0 <= 0 || spec.bits0 > spec.total_bits)
+    return cudaErrorInvalidValue;
+  const unsigned ctas = topk_final_ctas(spec.n_max);
+  SortItem* pk = (SortItem*)temp;
+  uint32_t* pi = (uint32_t*)(pk + (uint64_t)ctas * k);
+  k_topk_final<kTfThreads, kTfItems><<<ctas, kTfThreads, 0, s>>>(spec, k, pk, pi);
+  k_topk_warp<1024><<<1, 1024, 0, s>>>(pk, pi, nullptr, (uint64_t)ctas * k, k, nullptr, out_g, out_count, 1);
+  return cudaGetLastError();
 }
 
 size_t topk_temp_bytes(uint64_t n_max, int k) {

@@ -83,6 +83,29 @@ size_t topk_temp_bytes(uint64_t n_max, int k);
 cudaError_t launch_topk(const SortItem* keys, const uint32_t* idx, const uint64_t* count, uint64_t n_max, int k,
                         uint32_t* out_idx, uint64_t* out_count, void* temp, uint32_t* status, cudaStream_t s);
 
+// Fused aggregate top-K (K <= 32) straight from the aggregate states: the
+// candidates are the groups g < n (n = min(*n_dev, n_max) when n_dev is
+// given) whose flag byte is nonzero or whose table state is READY (2), or
+// every g < n when both are null. A candidate's key is the order-preserving
+// image of the ORDER BY parts (each a FinalOut evaluated at g, of physical
+// type ptype), ties broken by g. Writes the K best g, best first, and their
+// number.
+struct TopkFinalSpec {
+  int32_t n_parts;
+  int32_t total_bits;  // bits of all parts
+  int32_t bits0;       // bits of the first part
+  int32_t ptype[kMaxOrder];
+  int32_t desc[kMaxOrder];
+  FinalOut part[kMaxOrder];
+  const uint8_t* flag;
+  const uint32_t* state;
+  const uint64_t* n_dev;
+  uint64_t n_max;
+};
+size_t topk_final_temp_bytes(uint64_t n_max, int k);
+cudaError_t launch_topk_final(const TopkFinalSpec& spec, int k, uint32_t* out_g, uint64_t* out_count, void* temp,
+                              cudaStream_t s);
+
 // ---- gathers for final materialization (k_misc.cu)
 // out[i] = in[idx[i]] for fixed width elements (4, 8 or 16 bytes).
 cudaError_t launch_gather_width(const void* in, int width, const uint32_t* idx, const uint64_t* count,

@@ -183,3 +183,81 @@ def register_q3(conn, t: Q3Tables, upload: bool = True, borrow: bool = False):
                                    "l_shipdate": (L.T_DATE, t.lineitem["l_shipdate"])})
     for name in ("customer", "orders", "lineitem"):
         conn.gpu_register_table(name, upload=upload, borrow=borrow)
+
+
+# ------------------------------------------------------------------ config 5
+# Tables of the served mixed stream: (name, template, rows, generator kwargs).
+SERVED_TABLES = [
+    ("numbers", "c1", 1_000_000, {}),
+    ("s1m", "c2", 1_000_000, {}),
+    ("s10m", "c2", 10_000_000, {}),
+    ("s60m", "c2", 60_000_000, {}),
+    ("g1m", "c3", 1_000_000, {"groups": 1000, "dist": "uniform"}),
+    ("g10m", "c3", 10_000_000, {"groups": 1_000_000, "dist": "zipf"}),
+    ("g60m", "c3", 60_000_000, {"groups": 1000, "dist": "zipf"}),
+]
+
+
+def served_tables(salt: int = 5) -> dict[str, tuple[str, dict[str, np.ndarray]]]:
+    out = {}
+    for i, (name, tpl, n, kw) in enumerate(SERVED_TABLES):
+        if tpl == "c1":
+            out[name] = (tpl, numbers(n, seed_salt=salt + i))
+        elif tpl == "c2":
+            out[name] = (tpl, scan(n, seed_salt=salt + i))
+        else:
+            out[name] = (tpl, groupby(n, seed_salt=salt + i, **kw))
+    return out
+
+
+def _scan_value(col: str, q: float):
+    """Numeric literal at quantile q of a scan column and its SQL spelling."""
+    if col == "a":
+        v = int(q * 2**31)
+        return v, str(v)
+    if col == "b":
+        v = int(-(2**62) + q * 2**63)
+        return v, str(v)
+    if col == "c":
+        # two-digit DECIMAL literal; compared as FLOAT(digits) / FLOAT(100)
+        digits = int(round(q * 100))
+        v = float(np.float32(digits) / np.float32(100))
+        return v, f"{digits // 100}.{digits % 100:02d}"
+    if col == "d":
+        v = DAY0 + int(q * SPAN_DAYS)
+        return v, f"DATE '{day_to_iso(v)}'"
+    us_day = 86_400_000_000
+    v = DAY0 * us_day + int(q * SPAN_DAYS * us_day) // 1_000_000 * 1_000_000
+    t = _dt.datetime(1970, 1, 1) + _dt.timedelta(microseconds=v)
+    return v, f"TIMESTAMP '{t.strftime('%Y-%m-%d %H:%M:%S')}'"
+
+
+def served_stream(n: int = 2000, seed: int = 7) -> list[dict]:
+    """The mixed query stream: templates of the plain small query, the scan
+    and the grouped aggregate, with seeded constants and tables of 10^6 to
+    6*10^7 rows. Each entry holds the SQL and the numeric form of its
+    constants (for the CPU oracle)."""
+    r = np.random.default_rng(seed)
+    scans = [t for t, tpl, _, _ in SERVED_TABLES if tpl == "c2"]
+    groups = [t for t, tpl, _, _ in SERVED_TABLES if tpl == "c3"]
+    out = []
+    for i in range(n):
+        kind = int(r.integers(0, 3))
+        if kind == 0:
+            k = int(r.integers(0, 1_000_000))
+            out.append({"tpl": "c1", "table": "numbers", "k": k,
+                        "sql": f"SELECT value, value * 10 AS scaled FROM numbers WHERE value > {k} ORDER BY value"})
+        elif kind == 1:
+            table = scans[int(r.integers(0, len(scans)))]
+            col = "abcde"[int(r.integers(0, 5))]
+            op = ["<", "<=", ">", ">="][int(r.integers(0, 4))]
+            sel = float(r.choice([0.01, 0.1, 0.5]))
+            v, lit = _scan_value(col, sel if op in ("<", "<=") else 1.0 - sel)
+            out.append({"tpl": "c2", "table": table, "col": col, "op": op, "v": v,
+                        "sql": f"SELECT a, b + 5 AS b5, c * 10 AS c10, d, e FROM {table} WHERE {col} {op} {lit}"})
+        else:
+            table = groups[int(r.integers(0, len(groups)))]
+            lim = int(r.integers(10, 101))
+            out.append({"tpl": "c3", "table": table, "limit": lim,
+                        "sql": C3_SQL.replace("FROM t", f"FROM {table}").replace("LIMIT 100", f"LIMIT {lim}")})
+    return out
