@@ -834,47 +834,43 @@ __global__ void __launch_bounds__(kThreads) k_pipeline(const __grid_constant__ P
       __syncthreads();
       const uint64_t base = s_base;
       // write phase: one output column at a time over the compacted rows
+      const uint32_t lim = base >= d.out_capacity ? 0u
+                           : (uint32_t)(d.out_capacity - base < (uint64_t)total ? d.out_capacity - base : total);
+      if (lim < total) st |= ST_CAPACITY;
       for (int q = 0; q < d.n_out; ++q) {
         const VmProg& pg = d.progs[d.out_prog[q]];
         void* out = d.out_ptr[q];
         const int32_t ot = pg.out_type;
         if (pg.n == 1 && pg.ins[0].op == VM_COL) {
           // plain column: typed copy
-          const int col = pg.ins[0].arg;
-          for (uint32_t p = tid; p < total; p += THREADS) {
-            const uint64_t o = base + p;
-            if (o >= d.out_capacity) { st |= ST_CAPACITY; continue; }
+          const ColAcc ca = col_acc(tc, pg.ins[0].arg);
+#pragma unroll 4
+          for (uint32_t p = tid; p < lim; p += THREADS) {
             Val v;
-            v.lo = tc_get(tc, col, s_list[p]);
+            v.lo = acc_get(ca, tc, s_list[p]);
             v.hi = v.lo >> 63;
-            store_val(out, ot, o, v);
+            store_val(out, ot, base + p, v);
           }
         } else if (pg.n == 3 && pg.ins[0].op == VM_COL && pg.ins[1].op == VM_CONST && pg.ins[2].op >= VM_ADD &&
                    pg.ins[2].op <= VM_MUL && pg.ins[2].type != P_I128) {
           // column op constant, evaluated inline
-          const int col = pg.ins[0].arg;
+          const ColAcc ca = col_acc(tc, pg.ins[0].arg);
           const Val kc{pg.ins[1].k, pg.ins[1].k2};
           const int16_t aop = pg.ins[2].op, aty = pg.ins[2].type;
-          for (uint32_t p = tid; p < total; p += THREADS) {
-            const uint64_t o = base + p;
-            if (o >= d.out_capacity) { st |= ST_CAPACITY; continue; }
+#pragma unroll 4
+          for (uint32_t p = tid; p < lim; p += THREADS) {
             Val v;
-            v.lo = tc_get(tc, col, s_list[p]);
+            v.lo = acc_get(ca, tc, s_list[p]);
             v.hi = v.lo >> 63;
-            store_val(out, ot, o, vm_arith(aop, aty, v, kc, st));
+            store_val(out, ot, base + p, vm_arith(aop, aty, v, kc, st));
           }
         } else {
-          for (uint32_t p = tid; p < total; p += THREADS) {
-            const uint64_t o = base + p;
-            if (o >= d.out_capacity) { st |= ST_CAPACITY; continue; }
-            store_val(out, ot, o, vm_eval_t(pg, tc, s_list[p], st));
-          }
+          for (uint32_t p = tid; p < lim; p += THREADS) store_val(out, ot, base + p, vm_eval_t(pg, tc, s_list[p], st));
         }
       }
       for (int s = 0; s < kMaxSrc; ++s)
         if ((d.out_rid_mask >> s) & 1u)
-          for (uint32_t p = tid; p < total; p += THREADS)
-            if (base + p < d.out_capacity) d.out_rids[s][base + p] = tc_rid(tc, s, s_list[p]);
+          for (uint32_t p = tid; p < lim; p += THREADS) d.out_rids[s][base + p] = tc_rid(tc, s, s_list[p]);
     } else if (SINK == SK_BUILD) {
       const DBuild& bd = d.builds[d.sink_build];
       // One slot reservation per tile: the tile's surviving rows take
