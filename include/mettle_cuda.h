@@ -218,6 +218,26 @@ int mtl_scalar_arith(mtl_ctx *ctx, int32_t op, int32_t type, const void *in, uin
 int mtl_scalar_compare(mtl_ctx *ctx, int32_t op, int32_t type, const void *in, uint64_t n, int64_t ilit,
                        double flit, uint8_t *out);
 
+/* ------------------------------------------------- allocation-free top-K */
+/* No counterpart in the reference. Top-K rows of one BIGINT or TIMESTAMP
+ * column already in device memory, for callers that cannot allocate device
+ * memory when they need the result (their device memory is all handed to
+ * their own pool, or they must not let cudaMalloc/cudaFree synchronize the
+ * device). Nothing is allocated: the kernels' scratch is a fixed 1 MiB array
+ * in device memory that the library holds on every GPU that loads it.
+ * values: n int64 values on the current device. out_rows: k uint32 row
+ * numbers, best first (DESC when descending != 0, else ASC; ties go to the
+ * lower row number); out_count: the number written (min(n, k)). Both are
+ * device pointers. stream: a cudaStream_t (NULL = the legacy default
+ * stream); the call only enqueues work. Limits: 1 <= k <= 32,
+ * n <= 2^32 - 2; a call that would need more scratch than the array holds is
+ * rejected with MTL_INVALID and a message. The first call on a device looks
+ * up the array's address with that device current; make it before any
+ * stream capture. All calls share the array: calls whose kernels overlap on
+ * the GPU race and can return wrong rows. */
+int mtl_topk_noalloc(int32_t type, const void *values, uint64_t n, int32_t k, int32_t descending,
+                     uint32_t *out_rows, uint64_t *out_count, void *stream);
+
 /* -------------------------------------------------------------- serving */
 typedef struct mtl_serve_stats {
   int64_t submitted, completed, rejected, in_flight, queued;
