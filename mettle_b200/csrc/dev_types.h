@@ -80,12 +80,33 @@ struct VmIns {
   int64_t k2;     // constant hi bits (I128) / cast divisor flag
 };
 
+// A cast applied to one node of a FastExpr (on = 0: none).
+struct VmCast {
+  int16_t from, to;
+  int32_t on;
+  int64_t mul, div;
+};
+
+// The same expression as a fixed tree of at most three leaves (column or
+// constant) and two binary ops, each node with an optional cast, so the
+// device evaluates it without a stack machine. shape 0: not expressible;
+// 1: L0; 2: L0 op0 L1; 3: L0 op1 (L1 op0 L2); 4: (L0 op0 L1) op1 L2.
+struct VmFast {
+  int32_t shape;
+  int32_t pad;
+  VmIns leaf[3];  // VM_COL or VM_CONST
+  VmCast leaf_cast[3];
+  VmIns op[2];    // op, type
+  VmCast op_cast[2];
+};
+
 struct VmProg {
   int32_t n;
   int32_t out_type;
   int32_t depth;  // deepest stack the program reaches
   int32_t pad;
   VmIns ins[kMaxIns];
+  VmFast fast;
 };
 
 // ------------------------------------------------------------ join builds
@@ -161,7 +182,11 @@ struct DAggTable {
   uint64_t* keys[kMaxKeys];
   uint64_t capacity;
   int32_t n_keys;
-  int32_t pad;
+  // One group key claimed with a CAS on the key word itself: keys[0] starts
+  // all ones (kEmptyKey), states start at their identities, entry
+  // `capacity` holds the group whose key equals kEmptyKey, and state[g] is
+  // set to 2 when group g is first used.
+  int32_t cas;
 };
 
 // ------------------------------------------------------------ pipeline

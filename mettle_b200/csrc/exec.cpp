@@ -598,7 +598,72 @@ struct Compiler {
       if (op == VM_COL || op == VM_CONST || op == VM_SLOT) p.depth = std::max(p.depth, ++sp);
       else if (op != VM_CAST && op != VM_NEG) --sp;
     }
+    make_fast(p);
     return i;
+  }
+
+  // Recasts a postfix program as a VmFast tree when it has at most three
+  // leaves, two binary ops and one cast per node.
+  static void make_fast(VmProg& p) {
+    VmFast f;
+    memset(&f, 0, sizeof(f));
+    struct Node {
+      bool leaf;
+      int idx;
+      int left_leaf;  // op nodes: whether the left child is a leaf (-1 unknown)
+    };
+    Node st[kMaxIns];
+    int sp = 0, nl = 0, no = 0;
+    bool root_is_op = false;
+    int inner_on_left = -1;  // for the second op: is the first op its left child
+    for (int k = 0; k < p.n; ++k) {
+      const VmIns& in = p.ins[k];
+      switch (in.op) {
+        case VM_COL:
+        case VM_CONST:
+          if (nl >= 3) return;
+          f.leaf[nl] = in;
+          st[sp++] = Node{true, nl++, -1};
+          break;
+        case VM_CAST: {
+          if (sp < 1) return;
+          const Node& t = st[sp - 1];
+          VmCast& c = t.leaf ? f.leaf_cast[t.idx] : f.op_cast[t.idx];
+          if (c.on) return;
+          c.on = 1;
+          c.from = (int16_t)in.arg;
+          c.to = in.type;
+          c.mul = in.k;
+          c.div = in.k2;
+          break;
+        }
+        case VM_ADD:
+        case VM_SUB:
+        case VM_MUL: {
+          if (sp < 2 || no >= 2) return;
+          const Node b = st[--sp];
+          const Node a = st[--sp];
+          if (no == 1) {
+            // the second op must combine the first op's result with a leaf
+            if (a.leaf == b.leaf) return;
+            inner_on_left = a.leaf ? 0 : 1;
+          } else if (!(a.leaf && b.leaf)) {
+            return;
+          }
+          f.op[no] = in;
+          st[sp++] = Node{false, no++, -1};
+          break;
+        }
+        default:
+          return;  // NEG, SLOT
+      }
+    }
+    if (sp != 1) return;
+    root_is_op = !st[0].leaf;
+    if (!root_is_op) f.shape = nl == 1 ? 1 : 0;
+    else if (no == 1) f.shape = nl == 2 ? 2 : 0;
+    else f.shape = nl == 3 ? (inner_on_left ? 4 : 3) : 0;
+    if (f.shape) p.fast = f;
   }
 
   static void expr_sources(const BExpr& e, uint32_t& m) {
@@ -660,6 +725,7 @@ struct Compiler {
   uint32_t needed_root = 0;
   uint32_t payload_mask(int s) const { return needed_root & subtree[s]; }
   int rep_src = -1;
+  bool cas_table = false;  // one-key hash aggregate claimed by CAS on the key
 
   void add_filters(PipeBuilder& pb, int s) {
     for (const BFilter& f : plan.filters) {
@@ -1090,7 +1156,10 @@ struct Compiler {
         est_groups = estimate_groups();
         groups = std::max<uint64_t>(64, est_groups * 2);
       }
-      plan_states(groups, root_rows, scalar);
+      // a one-key hash table keeps one more group: the key equal to the
+      // empty-slot sentinel
+      cas_table = !scalar && rep_src < 0 && plan.group_keys.size() == 1;
+      plan_states(cas_table ? groups + 1 : groups, root_rows, scalar);
     }
 
     // build pipelines, children before parents
@@ -1254,24 +1323,34 @@ struct Compiler {
 
     // hash aggregation (shared-memory tables when the group count is small)
     const uint64_t cap = groups;
+    const uint64_t n_ent = cas_table ? cap + 1 : cap;  // table entries incl. the sentinel key's group
     pb.d.table.capacity = cap;
     pb.d.table.n_keys = (int)plan.group_keys.size();
-    pb.d.table.state = (uint32_t*)scratch(cap * 4);
-    memset_step(pb.d.table.state, 0, cap * 4);
+    pb.d.table.cas = cas_table ? 1 : 0;
+    pb.d.table.state = (uint32_t*)scratch(n_ent * 4);
+    memset_step(pb.d.table.state, 0, n_ent * 4);
     for (size_t k = 0; k < plan.group_keys.size(); ++k) {
-      pb.d.table.keys[k] = (uint64_t*)scratch(cap * 8);
+      pb.d.table.keys[k] = (uint64_t*)scratch(n_ent * 8);
       pb.d.key_prog[k] = add_prog(pb, *plan.group_keys[k]);
     }
-    fill_aggs(pb, true);
-    pb.d.sink = SK_AGG_HASH;
-    if (est_groups <= 1536) {
-      pb.d.sink = SK_AGG_SMEM;
-      pb.d.smem_capacity = (int)std::max<uint64_t>(256, est_groups * 4 / 3 + 64);
-      size_t smem = pipeline_smem_bytes(pb.d);
-      if (smem > 200 * 1024) {
-        pb.d.sink = SK_AGG_HASH;
-        pb.d.smem_capacity = 0;
+    if (cas_table) {
+      // keys start empty and states at their identities: a claim is one CAS
+      memset_step(pb.d.table.keys[0], 0xFF, n_ent * 8);
+      for (const AggState& s : states) {
+        fill_step(s.lo, n_ent, state_identity(s.fn_dev));
+        if (s.hi) fill_step(s.hi, n_ent, 0);
       }
+    }
+    fill_aggs(pb, true);
+    // Shared-memory tables hold every group when there are few; with many,
+    // a fixed-size table keeps each CTA's frequent keys (a skewed key's rows
+    // then meet in shared memory instead of contending on one global
+    // state), and rows whose key is not there go to the global table.
+    pb.d.sink = SK_AGG_SMEM;
+    pb.d.smem_capacity = est_groups <= 1536 ? (int)std::max<uint64_t>(256, est_groups * 4 / 3 + 64) : 512;
+    if (pipeline_smem_bytes(pb.d) > 100 * 1024) {
+      pb.d.sink = SK_AGG_HASH;
+      pb.d.smem_capacity = 0;
     }
     push_pipeline(pb, root_rows);
     std::vector<FinalOut> fo;
@@ -1290,13 +1369,22 @@ struct Compiler {
         fo.push_back(f);
       }
     }
-    if (agg_topk_fused(fo, nullptr, pb.d.table.state, nullptr, cap, tie)) return;
-    uint32_t* gidx = (uint32_t*)scratch(cap * 4);
+    if (agg_topk_fused(fo, nullptr, pb.d.table.state, nullptr, n_ent, tie)) return;
+    uint32_t* gidx = (uint32_t*)scratch(n_ent * 4);
     uint64_t* gcnt = (uint64_t*)scratch(8);
-    compact_step(pb.d.table.state, cap, nullptr, gidx, gcnt, true);
-    for (size_t i = 0; i < fo.size(); ++i) fo[i].out = dense[i].dev = scratch(cap * dense[i].width);
-    finalize_step(upload_finals(fo), (int)fo.size(), gidx, gcnt, cap);
-    order_and_limit(gcnt, cap, tie);
+    compact_step(pb.d.table.state, n_ent, nullptr, gidx, gcnt, true);
+    for (size_t i = 0; i < fo.size(); ++i) fo[i].out = dense[i].dev = scratch(n_ent * dense[i].width);
+    finalize_step(upload_finals(fo), (int)fo.size(), gidx, gcnt, n_ent);
+    order_and_limit(gcnt, n_ent, tie);
+  }
+
+  static uint64_t state_identity(int fn) {
+    switch (fn) {
+      case A_MIN_I: return 0x7FFFFFFFFFFFFFFFULL;
+      case A_MAX_I: return 0x8000000000000000ULL;
+      case A_MIN_F: return ~0ULL;
+      default: return 0;
+    }
   }
 
   // Aggregate ORDER BY ... LIMIT K with K <= 32: one fused top-K over the
@@ -1336,13 +1424,34 @@ struct Compiler {
     const int K = (int)plan.limit;
     uint32_t* og = (uint32_t*)scratch((uint64_t)K * 4);
     uint64_t* oc = (uint64_t*)scratch(8);
+    // live groups (order-preserving), their ORDER BY images from the states,
+    // a warp top-K over the images, the winners mapped back to group ids
+    uint32_t* gidx = (uint32_t*)scratch(cap * 4);
+    uint64_t* gcnt = (uint64_t*)scratch(8);
+    compact_step(flag ? (const void*)flag : (const void*)state, cap, n_dev, gidx, gcnt, state != nullptr);
+    SortItem* keys = (SortItem*)scratch(cap * sizeof(SortItem));
+    uint32_t* kidx = (uint32_t*)scratch(cap * 4);
+    Step e;
+    e.k = Step::ENCODE_STATES;
+    e.tfs = ts;
+    e.idx = gidx;
+    e.count = gcnt;
+    e.n_max = cap;
+    e.keys = keys;
+    e.kidx = kidx;
+    P.steps.push_back(e);
+    P.kernels += 1;
     Step t;
-    t.k = Step::TOPK_FINAL;
-    t.tfs = ts;
+    t.k = Step::TOPK;
+    t.keys = keys;
+    t.kidx = kidx;
+    t.count = gcnt;
+    t.n_max = cap;
     t.topk = K;
     t.out_idx = og;
     t.out_count = oc;
-    t.temp = scratch(topk_final_temp_bytes(cap, K));
+    t.remap = gidx;
+    t.temp = scratch(topk_temp_bytes(cap, K));
     P.steps.push_back(t);
     P.kernels += 2;
     std::vector<FinalOut> vis;
@@ -1532,6 +1641,7 @@ static const char* step_kind_name(Step::Kind k) {
     case Step::RADIX: return "radix_sort";
     case Step::TOPK: return "topk";
     case Step::TOPK_FINAL: return "topk_states";
+    case Step::ENCODE_STATES: return "encode_states";
     case Step::GATHER: return "gather";
   }
   return "step";
@@ -1570,7 +1680,10 @@ void run_program(Ctx& ctx, Program& p, cudaStream_t s) {
       }
       case Step::TOPK:
         CK(launch_topk(st.keys, st.kidx, st.count, st.n_max, st.topk, st.out_idx, st.out_count, st.temp, p.status,
-                       s));
+                       s, st.remap));
+        break;
+      case Step::ENCODE_STATES:
+        CK(launch_encode_states(st.tfs, st.idx, st.count, st.n_max, st.keys, st.kidx, s));
         break;
       case Step::TOPK_FINAL: CK(launch_topk_final(st.tfs, st.topk, st.out_idx, st.out_count, st.temp, s)); break;
       case Step::GATHER: CK(launch_gather_width(st.gin, st.width, st.idx, st.count, st.n_max, st.gout, s)); break;

@@ -14,7 +14,7 @@ namespace mtl {
 // arithmetic; the sum is assumed below 2^64 in magnitude (the long double
 // image of larger sums is rounded, and this emulation rounds it the same
 // way only when the discarded bits are not a tie).
-static __device__ double avg_extended(__int128 sum, unsigned long long count) {
+static __device__ __noinline__ double avg_extended(__int128 sum, unsigned long long count) {
   if (sum == 0 || count == 0) return 0.0;
   const bool neg = sum < 0;
   unsigned __int128 S = neg ? (unsigned __int128)(-sum) : (unsigned __int128)sum;

@@ -145,6 +145,32 @@ __device__ __forceinline__ void agg_apply(int32_t fn, unsigned long long* lo, lo
   }
 }
 
+// agg_apply for states in global memory: the MIN/MAX pre-checks read L2
+// directly (a stale value only costs an extra atomic), so the reads of
+// several rows can be in flight together.
+__device__ __forceinline__ void agg_apply_g(int32_t fn, unsigned long long* lo, long long* hi, Val v,
+                                            int32_t vtype) {
+  switch (fn) {
+    case A_MIN_I:
+      if ((long long)v.lo < __ldcg((const long long*)lo)) atomicMin((long long*)lo, (long long)v.lo);
+      break;
+    case A_MAX_I:
+      if ((long long)v.lo > __ldcg((const long long*)lo)) atomicMax((long long*)lo, (long long)v.lo);
+      break;
+    case A_MIN_F: {
+      unsigned long long u = ord_f64(val_as_f64(v, vtype));
+      if (u < __ldcg(lo)) atomicMin(lo, u);
+      break;
+    }
+    case A_MAX_F: {
+      unsigned long long u = ord_f64(val_as_f64(v, vtype));
+      if (u > __ldcg(lo)) atomicMax(lo, u);
+      break;
+    }
+    default: agg_apply(fn, lo, hi, v, vtype); break;
+  }
+}
+
 // Merges a partial state (lo, hi) into a state word pair.
 __device__ __forceinline__ void agg_merge(int32_t fn, unsigned long long* lo, long long* hi, uint64_t plo,
                                           int64_t phi) {
@@ -173,10 +199,40 @@ __device__ __forceinline__ uint64_t key_hash(const uint64_t* kw, int nk) {
   return h;
 }
 
+constexpr uint64_t kNoGroup = ~0ULL;
+
+__device__ __forceinline__ uint64_t key_hash1(uint64_t k) { return hash64(0x9E3779B97F4A7C15ULL ^ k); }
+
+// Group of a single 64-bit key in a CAS-claimed table (DAggTable::cas),
+// starting at slot idx. kNoGroup when the table is full.
+__device__ __noinline__ uint64_t agg_find_cas(const DAggTable& t, uint64_t key, uint64_t idx, uint32_t& st) {
+  if ((int64_t)key == kEmptyKey) {
+    if (t.state[t.capacity] != 2u) t.state[t.capacity] = 2u;
+    return t.capacity;
+  }
+  for (uint64_t probe = 0; probe < t.capacity; ++probe) {
+    const uint64_t k = __ldcg(t.keys[0] + idx);
+    if (k == key) return idx;
+    if ((int64_t)k == kEmptyKey) {
+      const unsigned long long prev =
+          atomicCAS((unsigned long long*)(t.keys[0] + idx), (unsigned long long)kEmptyKey, (unsigned long long)key);
+      if (prev == (unsigned long long)kEmptyKey) {
+        t.state[idx] = 2u;  // read only after the pipeline (compaction, top-K)
+        return idx;
+      }
+      if (prev == key) return idx;
+    }
+    if (++idx == t.capacity) idx = 0;
+  }
+  st |= ST_TABLE_FULL;
+  return kNoGroup;
+}
+
 // Finds or claims the group of key words kw in a global table. Returns
-// capacity on failure (table full or wait limit), with status set.
+// kNoGroup on failure (table full or wait limit), with status set.
 __device__ uint64_t agg_find_global(const PipeDesc& d, const uint64_t* kw, uint32_t& st) {
   const DAggTable& t = d.table;
+  if (t.cas) return agg_find_cas(t, kw[0], hash_slot(key_hash1(kw[0]), t.capacity), st);
   uint64_t idx = hash_slot(key_hash(kw, t.n_keys), t.capacity);
   for (uint64_t probe = 0; probe < t.capacity; ++probe) {
     uint32_t s = ld_acquire32(t.state + idx);
@@ -194,7 +250,7 @@ __device__ uint64_t agg_find_global(const PipeDesc& d, const uint64_t* kw, uint3
     while (s == 1) {
       if (++spins > kSpinLimit) {
         st |= ST_SPIN_LIMIT;
-        return t.capacity;
+        return kNoGroup;
       }
       s = ld_acquire32(t.state + idx);
     }
@@ -204,7 +260,7 @@ __device__ uint64_t agg_find_global(const PipeDesc& d, const uint64_t* kw, uint3
     if (++idx == t.capacity) idx = 0;
   }
   st |= ST_TABLE_FULL;
-  return t.capacity;
+  return kNoGroup;
 }
 
 // Shared-memory group table of one CTA (AGG_SMEM). Layout, cap slots:
@@ -243,11 +299,15 @@ __device__ __forceinline__ void smem_agg_init(const PipeDesc& d, SmemAgg& s, uin
   }
 }
 
-// Finds or claims kw in the CTA table; -1 when the table is full.
+// Finds or claims kw in the CTA table; -1 when it is not among the first
+// kSmemProbes slots of its chain (the caller then uses the global table), so
+// a full table costs a bounded number of probes per row.
+constexpr int kSmemProbes = 4;
 __device__ __forceinline__ int smem_agg_find(const PipeDesc& d, SmemAgg& s, const uint64_t* kw, uint32_t& st) {
   const int nk = d.table.n_keys;
   int idx = (int)hash_slot(key_hash(kw, nk), (uint64_t)s.cap);
-  for (int probe = 0; probe < s.cap; ++probe) {
+  const int probes = s.cap < kSmemProbes ? s.cap : kSmemProbes;
+  for (int probe = 0; probe < probes; ++probe) {
     volatile uint32_t* sp = s.state + idx;
     uint32_t v = *sp;
     if (v == 0) {
@@ -277,8 +337,8 @@ __device__ __forceinline__ int smem_agg_find(const PipeDesc& d, SmemAgg& s, cons
 }
 
 // ------------------------------------------------------------ the kernel
-constexpr int kThreads = 256;
-constexpr int kTile = 2048;  // tuples per tile
+constexpr int kThreads = 128;
+constexpr int kTile = 1024;  // tuples per tile
 
 struct StreamLayout {
   int n;
@@ -377,7 +437,7 @@ struct RegStack {
 };
 
 // Programs deeper than the register stack.
-__device__ __noinline__ Val vm_eval_deep(const VmProg& p, const TileCtx& t, uint32_t r, uint32_t& st) {
+__device__ __forceinline__ Val vm_eval_deep(const VmProg& p, const TileCtx& t, uint32_t r, uint32_t& st) {
   Val stack[kMaxIns];
   int sp = 0;
   for (int i = 0; i < p.n; ++i) {
@@ -423,8 +483,41 @@ __device__ __noinline__ Val vm_eval_deep(const VmProg& p, const TileCtx& t, uint
   return stack[0];
 }
 
+__device__ __forceinline__ Val fast_leaf(const VmIns& in, const VmCast& c, const TileCtx& t, uint32_t r,
+                                        uint32_t& st) {
+  Val v;
+  if (in.op == VM_COL) {
+    v.lo = tc_get(t, in.arg, r);
+    v.hi = (in.type == P_I32 || in.type == P_I64) ? (v.lo >> 63) : 0;
+  } else {
+    v.lo = in.k;
+    v.hi = in.k2;
+  }
+  if (c.on) v = vm_cast(v, c.from, c.to, c.mul, c.div, st);
+  return v;
+}
+
+__device__ __forceinline__ Val fast_op(const VmIns& op, const VmCast& c, Val a, Val b, uint32_t& st) {
+  Val x = vm_arith(op.op, op.type, a, b, st);
+  if (c.on) x = vm_cast(x, c.from, c.to, c.mul, c.div, st);
+  return x;
+}
+
+// A program recast as a fixed tree (VmFast): leaves load together, then at
+// most two ops; no stack, no per-instruction dispatch.
+__device__ __forceinline__ Val vm_eval_fast(const VmFast& f, const TileCtx& t, uint32_t r, uint32_t& st) {
+  const Val a = fast_leaf(f.leaf[0], f.leaf_cast[0], t, r, st);
+  if (f.shape == 1) return a;
+  const Val b = fast_leaf(f.leaf[1], f.leaf_cast[1], t, r, st);
+  if (f.shape == 2) return fast_op(f.op[0], f.op_cast[0], a, b, st);
+  const Val c = fast_leaf(f.leaf[2], f.leaf_cast[2], t, r, st);
+  if (f.shape == 3) return fast_op(f.op[1], f.op_cast[1], a, fast_op(f.op[0], f.op_cast[0], b, c, st), st);
+  return fast_op(f.op[1], f.op_cast[1], fast_op(f.op[0], f.op_cast[0], a, b, st), c, st);
+}
+
 // Expression VM over one tile row.
 __device__ __forceinline__ Val vm_eval_t(const VmProg& p, const TileCtx& t, uint32_t r, uint32_t& st) {
+  if (p.fast.shape) return vm_eval_fast(p.fast, t, r, st);
   if (p.depth > 4) return vm_eval_deep(p, t, r, st);
   RegStack S;
   S.s0 = S.s1 = S.s2 = S.s3 = Val{0, 0};
@@ -535,10 +628,61 @@ __device__ __forceinline__ void filter_loop(uint32_t n_sel, bool ident, const ui
   }
 }
 
+// First filter of a tile on a streamed integer column: thread t owns the
+// kTile / kThreads consecutive rows starting at t * (kTile / kThreads),
+// reads them with 128-bit shared-memory loads, and writes the rows it keeps
+// in order after a warp prefix sum, so the selection comes out sorted within
+// each warp's range.
+template <typename T>
+__device__ __forceinline__ void filter_ident_blocked(const T* col, uint32_t nrow, const IntRange& rg, uint16_t* out,
+                                                     uint32_t* cnt) {
+  constexpr int U = kTile / kThreads;
+  static_assert(U * sizeof(T) % 16 == 0, "rows per thread must fill whole 16-byte vectors");
+  const int lane = threadIdx.x & 31;
+  const uint32_t b0 = threadIdx.x * U;
+  T v[U];
+  const uint4* src = (const uint4*)(col + b0);
+#pragma unroll
+  for (int q = 0; q < (int)(U * sizeof(T) / 16); ++q) ((uint4*)v)[q] = src[q];
+  // bounds of a 32-bit column narrowed to its range; an empty range keeps
+  // nothing (or everything when negated)
+  T lo, hi;
+  bool empty = rg.none || rg.lo > rg.hi;
+  if (sizeof(T) == 4) {
+    empty = empty || rg.lo > (int64_t)INT32_MAX || rg.hi < (int64_t)INT32_MIN;
+    lo = (T)(rg.lo < (int64_t)INT32_MIN ? (int64_t)INT32_MIN : rg.lo);
+    hi = (T)(rg.hi > (int64_t)INT32_MAX ? (int64_t)INT32_MAX : rg.hi);
+  } else {
+    lo = (T)rg.lo;
+    hi = (T)rg.hi;
+  }
+  uint32_t km = 0;
+#pragma unroll
+  for (int j = 0; j < U; ++j) {
+    const bool in_range = !empty && v[j] >= lo && v[j] <= hi;
+    if ((in_range != rg.neg) && b0 + j < nrow) km |= 1u << j;
+  }
+  const uint32_t c = __popc(km);
+  uint32_t incl = c;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+    if (lane >= o) incl += y;
+  }
+  const uint32_t tot = __shfl_sync(0xFFFFFFFFu, incl, 31);
+  uint32_t base = 0;
+  if (lane == 0 && tot) base = atomicAdd(cnt, tot);
+  uint32_t pos = __shfl_sync(0xFFFFFFFFu, base, 0) + incl - c;
+#pragma unroll
+  for (int j = 0; j < U; ++j)
+    if ((km >> j) & 1u) out[pos++] = (uint16_t)(b0 + j);
+}
+
 // Join probe over the current selection, kProbeBatch rows per thread at a
 // time: keys, then the presence words and map entries (dense) or first
 // probed slots (hash) of the whole batch are loaded before any is used.
 constexpr int kProbeBatch = 4;
+constexpr int kAggBatch = 4;  // rows per thread in flight in the single-key hash sink
 
 template <int SINK>
 __global__ void __launch_bounds__(kThreads) k_pipeline(const __grid_constant__ PipeDesc d) {
@@ -694,6 +838,10 @@ __global__ void __launch_bounds__(kThreads) k_pipeline(const __grid_constant__ P
           const IntRange rg = to_range(p);
           if (rg.none) {
             filter_loop(n_sel, ident, sel_in, sel_out, cnt, [&](uint32_t) { return false; });
+          } else if (si >= 0 && ident && S.width[si] == 4 && c.ptype == P_I32) {
+            filter_ident_blocked<int32_t>((const int32_t*)(buf + S.off[si]), n_sel, rg, sel_out, cnt);
+          } else if (si >= 0 && ident && S.width[si] == 8) {
+            filter_ident_blocked<int64_t>((const int64_t*)(buf + S.off[si]), n_sel, rg, sel_out, cnt);
           } else if (si >= 0 && S.width[si] == 4) {
             const int32_t* col = (const int32_t*)(buf + S.off[si]);
             filter_loop(n_sel, ident, sel_in, sel_out, cnt, [&](uint32_t r) {
@@ -726,6 +874,14 @@ __global__ void __launch_bounds__(kThreads) k_pipeline(const __grid_constant__ P
         const int lane = tid & 31;
         const uint32_t lt = (1u << lane) - 1u;
         const ColAcc ka = col_acc(tc, pr.key_col);
+        const bool k32 = ka.sm && ka.width == 4 && ka.ptype == P_I32;  // streamed INTEGER key
+        // Descriptor fields used per row, read once: the loop's shared-memory
+        // stores would otherwise force reloads through the descriptor.
+        const int64_t b_kmin = bd.key_min;
+        const uint64_t b_cap = bd.capacity;
+        const uint32_t* const b_bits = bd.dense_bits;
+        const uint32_t* const b_map = bd.dense_map;
+        const bool b_dense = bd.kind == B_DENSE;
         (void)c;
         for (uint32_t i0 = 0; i0 < n_sel; i0 += THREADS * kProbeBatch) {
           uint32_t r[kProbeBatch], slot[kProbeBatch];
@@ -736,19 +892,19 @@ __global__ void __launch_bounds__(kThreads) k_pipeline(const __grid_constant__ P
             const uint32_t i = i0 + (uint32_t)j * THREADS + tid;
             act[j] = i < n_sel;
             r[j] = act[j] ? (ident ? i : (uint32_t)sel_in[i]) : 0u;
-            key[j] = act[j] ? acc_get(ka, tc, r[j]) : 0;
+            key[j] = !act[j] ? 0 : k32 ? (int64_t)((const int32_t*)ka.sm)[r[j]] : acc_get(ka, tc, r[j]);
           }
-          if (bd.kind == B_DENSE) {
+          if (b_dense) {
             uint32_t w[kProbeBatch], mv[kProbeBatch];
             uint64_t kk[kProbeBatch];
 #pragma unroll
             for (int j = 0; j < kProbeBatch; ++j) {
-              kk[j] = (uint64_t)(key[j] - bd.key_min);
-              const bool inb = act[j] && kk[j] < bd.capacity;
+              kk[j] = (uint64_t)(key[j] - b_kmin);
+              const bool inb = act[j] && kk[j] < b_cap;
               // The map entry is read beside its presence word; it is only
               // used when the presence bit is set.
-              w[j] = inb ? bd.dense_bits[kk[j] >> 5] : 0u;
-              mv[j] = inb ? bd.dense_map[kk[j]] : 0u;
+              w[j] = inb ? __ldg(b_bits + (kk[j] >> 5)) : 0u;
+              mv[j] = inb ? __ldg(b_map + kk[j]) : 0u;
             }
 #pragma unroll
             for (int j = 0; j < kProbeBatch; ++j) {
@@ -782,9 +938,10 @@ __global__ void __launch_bounds__(kThreads) k_pipeline(const __grid_constant__ P
           for (int j = 0; j < kProbeBatch; ++j) {
             if (keep[j]) {
               if (want_slot) s_slot[r[j]] = slot[j];
-              for (int s = 0; s < kMaxSrc; ++s)
-                if ((fill >> s) & 1u)
-                  s_srid[(size_t)((slot_of_src >> (4 * s)) & 0xFu) * TILE + r[j]] = bd.payload[s][slot[j]];
+              if (fill)
+                for (int s = 0; s < kMaxSrc; ++s)
+                  if ((fill >> s) & 1u)
+                    s_srid[(size_t)((slot_of_src >> (4 * s)) & 0xFu) * TILE + r[j]] = bd.payload[s][slot[j]];
             }
             m[j] = __ballot_sync(0xFFFFFFFFu, keep[j]);
             tot += __popc(m[j]);
@@ -891,12 +1048,75 @@ __global__ void __launch_bounds__(kThreads) k_pipeline(const __grid_constant__ P
         if (d.slot_hit) d.slot_hit[slot] = 0;
         build_insert(bd, key, slot, st);
       }
+    } else if ((SINK == SK_AGG_HASH || SINK == SK_AGG_SMEM) && d.table.cas) {
+      // One 64-bit group key: kAggBatch rows per thread at a time. Keys held
+      // in the CTA's shared-memory table are updated there; for the others
+      // the first probed global key words are read together, and states are
+      // updated with atomics whose results are not waited for.
+      constexpr int B = kAggBatch;
+      const DAggTable& tb = d.table;
+      const VmProg& kp = d.progs[d.key_prog[0]];
+      for (uint32_t i0 = 0; i0 < n_sel; i0 += THREADS * B) {
+        uint32_t r[B];
+        bool act[B];
+        int sidx[B];
+        uint64_t key[B], h[B], k0[B], g[B];
+#pragma unroll
+        for (int b = 0; b < B; ++b) {
+          const uint32_t i = i0 + (uint32_t)b * THREADS + tid;
+          act[b] = i < n_sel;
+          r[b] = act[b] ? (ident ? i : (uint32_t)sel_in[i]) : 0u;
+          key[b] = act[b] ? (uint64_t)vm_eval_t(kp, tc, r[b], st).lo : 0;
+        }
+#pragma unroll
+        for (int b = 0; b < B; ++b) {
+          sidx[b] = -1;
+          if (SINK == SK_AGG_SMEM && act[b]) {
+            const uint64_t kw[kMaxKeys] = {key[b], 0, 0, 0};
+            sidx[b] = smem_agg_find(d, sagg, kw, st);
+          }
+        }
+#pragma unroll
+        for (int b = 0; b < B; ++b) {
+          h[b] = hash_slot(key_hash1(key[b]), tb.capacity);
+          k0[b] = (act[b] && sidx[b] < 0 && (int64_t)key[b] != kEmptyKey) ? __ldcg(tb.keys[0] + h[b]) : 0;
+        }
+#pragma unroll
+        for (int b = 0; b < B; ++b) {
+          g[b] = kNoGroup;
+          if (act[b] && sidx[b] < 0)
+            g[b] = ((int64_t)key[b] != kEmptyKey && k0[b] == key[b]) ? h[b] : agg_find_cas(tb, key[b], h[b], st);
+        }
+        for (int a = 0; a < d.n_aggs; ++a) {
+          const DAgg& ag = d.aggs[a];
+          const int32_t vt = ag.prog >= 0 ? d.progs[ag.prog].out_type : P_I64;
+          Val v[B];
+#pragma unroll
+          for (int b = 0; b < B; ++b) {
+            v[b] = Val{0, 0};
+            if (ag.prog >= 0 && (sidx[b] >= 0 || g[b] != kNoGroup)) v[b] = vm_eval_t(d.progs[ag.prog], tc, r[b], st);
+          }
+#pragma unroll
+          for (int b = 0; b < B; ++b) {
+            if (SINK == SK_AGG_SMEM && sidx[b] >= 0) {
+              long long* hp = sagg.hi_index[a] >= 0
+                                  ? (long long*)(sagg.hi + (size_t)sagg.hi_index[a] * sagg.cap + sidx[b])
+                                  : nullptr;
+              agg_apply(ag.fn, (unsigned long long*)(sagg.lo + (size_t)a * sagg.cap + sidx[b]), hp, v[b], vt);
+            } else if (g[b] != kNoGroup) {
+              agg_apply_g(ag.fn, (unsigned long long*)(ag.lo + g[b]), (long long*)(ag.hi ? ag.hi + g[b] : nullptr),
+                          v[b], vt);
+            }
+          }
+        }
+      }
     } else {
+      uint8_t* const slot_hit = d.slot_hit;
       for (uint32_t i = tid; i < n_sel; i += THREADS) {
         const uint32_t r = ident ? i : (uint32_t)sel_in[i];
         if (SINK == SK_AGG_SLOT) {
           const uint32_t g = s_slot[r];
-          d.slot_hit[g] = 1;
+          slot_hit[g] = 1;
           for (int a = 0; a < d.n_aggs; ++a) {
             const DAgg& ag = d.aggs[a];
             Val v{0, 0};
@@ -914,9 +1134,9 @@ __global__ void __launch_bounds__(kThreads) k_pipeline(const __grid_constant__ P
             kw[q] = q < d.table.n_keys ? (uint64_t)vm_eval_t(d.progs[d.key_prog[q]], tc, r, st).lo : 0;
           int sidx = -1;
           if (SINK == SK_AGG_SMEM) sidx = smem_agg_find(d, sagg, kw, st);
-          uint64_t g = d.table.capacity;
+          uint64_t g = kNoGroup;
           if (sidx < 0) g = agg_find_global(d, kw, st);
-          if (sidx < 0 && g >= d.table.capacity) continue;
+          if (sidx < 0 && g == kNoGroup) continue;
           for (int a = 0; a < d.n_aggs; ++a) {
             const DAgg& ag = d.aggs[a];
             Val v{0, 0};
@@ -996,7 +1216,7 @@ __global__ void __launch_bounds__(kThreads) k_pipeline(const __grid_constant__ P
 #pragma unroll
       for (int q = 0; q < kMaxKeys; ++q) kw[q] = q < d.table.n_keys ? sagg.keys[(size_t)q * sagg.cap + i] : 0;
       uint64_t g = agg_find_global(d, kw, st);
-      if (g >= d.table.capacity) continue;
+      if (g == kNoGroup) continue;
       for (int a = 0; a < d.n_aggs; ++a) {
         const DAgg& ag = d.aggs[a];
         int64_t hv = sagg.hi_index[a] >= 0 ? sagg.hi[(size_t)sagg.hi_index[a] * sagg.cap + i] : 0;

@@ -57,6 +57,38 @@ __global__ void k_encode(const __grid_constant__ SortKeySpec spec, const uint64_
   }
 }
 
+// ORDER BY images of aggregate groups straight from their states: for
+// i < *count, group g = gidx[i]; each part is a FinalOut evaluated at g.
+__global__ void k_encode_states(const __grid_constant__ TopkFinalSpec spec, const uint32_t* __restrict__ gidx,
+                                const uint64_t* count, uint64_t n_max, SortItem* __restrict__ keys,
+                                uint32_t* __restrict__ idx) {
+  const uint64_t n = count ? (*count < n_max ? *count : n_max) : n_max;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t g = gidx ? gidx[i] : i;
+    U256 k{{0, 0, 0, 0}};
+    for (int p = 0; p < spec.n_parts; ++p) {
+      uint64_t lo, hi;
+      final_value(spec.part[p], g, lo, hi);
+      key_part(k, spec.ptype[p], spec.desc[p] != 0, lo, hi);
+    }
+    SortItem it;
+    it.w[0] = k.w[0]; it.w[1] = k.w[1]; it.w[2] = k.w[2]; it.w[3] = k.w[3];
+    keys[i] = it;
+    idx[i] = (uint32_t)i;
+  }
+}
+
+cudaError_t launch_encode_states(const TopkFinalSpec& spec, const uint32_t* gidx, const uint64_t* count,
+                                 uint64_t n_max, SortItem* keys, uint32_t* idx, cudaStream_t s) {
+  if (spec.n_parts <= 0 || spec.n_parts > kMaxOrder) return cudaErrorInvalidValue;
+  uint64_t b = (n_max + 255) / 256;
+  uint64_t cap = (uint64_t)sms() * 8;
+  if (b > cap) b = cap;
+  if (!b) b = 1;
+  k_encode_states<<<(unsigned)b, 256, 0, s>>>(spec, gidx, count, n_max, keys, idx);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_encode_keys(const SortKeySpec& spec, const uint64_t* count, uint64_t n_max, SortItem* keys,
                                uint32_t* idx, cudaStream_t s) {
   uint64_t b = (n_max + 255) / 256;
@@ -389,12 +421,78 @@ __device__ __forceinline__ void warp_offer(Cand& L, const Cand& c, bool valid, i
   }
 }
 
+__device__ __forceinline__ Cand cand_shfl_xor(const Cand& c, int m) {
+  Cand r;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) r.w[i] = __shfl_xor_sync(0xFFFFFFFFu, c.w[i], m);
+  r.ix = __shfl_xor_sync(0xFFFFFFFFu, c.ix, m);
+  return r;
+}
+
+// Bitonic sort of one candidate per lane, ascending across the warp.
+__device__ __noinline__ void warp_sort32(Cand& c, int lane) {
+#pragma unroll
+  for (int k = 2; k <= 32; k <<= 1) {
+#pragma unroll
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      const Cand p = cand_shfl_xor(c, j);
+      const bool take_min = ((lane & j) == 0) == ((lane & k) == 0);
+      if (take_min ? cand_less(p, c) : cand_less(c, p)) c = p;
+    }
+  }
+}
+
+// L and M are ascending across the warp; L becomes the 32 smallest of both,
+// ascending. Elementwise min against M reversed leaves a bitonic sequence
+// holding the 32 smallest, which five half-cleaner steps sort.
+__device__ __noinline__ void warp_merge32(Cand& L, const Cand& M, int lane) {
+  const Cand r = cand_shfl(M, 31 - lane);
+  if (cand_less(r, L)) L = r;
+#pragma unroll
+  for (int j = 16; j > 0; j >>= 1) {
+    const Cand p = cand_shfl_xor(L, j);
+    if (((lane & j) == 0) ? cand_less(p, L) : cand_less(L, p)) L = p;
+  }
+}
+
+// Offers one candidate per lane to the warp's ascending list L (whose first
+// K lanes are the best so far): a few winners are inserted one at a time,
+// more are sorted as a batch and merged.
+__device__ __forceinline__ void warp_offer_batch(Cand& L, const Cand& c, bool valid, int K, int lane) {
+  const Cand thr = cand_shfl(L, K - 1);
+  const bool beat = valid && cand_less(c, thr);
+  const uint32_t m = __ballot_sync(0xFFFFFFFFu, beat);
+  if (!m) return;
+  if (__popc(m) <= 2) {
+    warp_offer(L, c, beat, K, lane);
+    return;
+  }
+  Cand s = beat ? c : cand_inf();
+  warp_sort32(s, lane);
+  warp_merge32(L, s, lane);
+}
+
+// Merges the warps' lists of a block into warp 0's L (tree of merges).
+template <int WARPS>
+__device__ __forceinline__ void block_merge_lists(Cand& L, Cand (*s_l)[32], int warp, int lane) {
+  s_l[warp][lane] = L;
+#pragma unroll
+  for (int s = 1; s < WARPS; s <<= 1) {
+    __syncthreads();
+    if ((warp & (2 * s - 1)) == 0 && warp + s < WARPS) {
+      warp_merge32(L, s_l[warp + s][lane], lane);
+      s_l[warp][lane] = L;
+    }
+  }
+  __syncthreads();
+}
+
 template <int THREADS>
 __global__ void __launch_bounds__(THREADS) k_topk_warp(const SortItem* __restrict__ keys,
                                                        const uint32_t* __restrict__ idx, const uint64_t* count,
                                                        uint64_t n_max, int K, SortItem* __restrict__ out_keys,
                                                        uint32_t* __restrict__ out_idx, uint64_t* out_count,
-                                                       int final_pass) {
+                                                       int final_pass, const uint32_t* __restrict__ remap = nullptr) {
   constexpr int WARPS = THREADS / 32;
   __shared__ Cand s_l[WARPS][32];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -413,18 +511,13 @@ __global__ void __launch_bounds__(THREADS) k_topk_warp(const SortItem* __restric
       c.ix = idx ? idx[g] : (uint32_t)g;
       valid = c.ix != 0xFFFFFFFFu;  // padding of a previous pass
     }
-    warp_offer(L, c, valid, K, lane);
+    warp_offer_batch(L, c, valid, K, lane);
   }
-  s_l[warp][lane] = L;
-  __syncthreads();
+  block_merge_lists<WARPS>(L, s_l, warp, lane);
   if (warp == 0) {
-    for (int w = 1; w < WARPS; ++w) {
-      const Cand c = s_l[w][lane];
-      warp_offer(L, c, lane < K && c.ix != 0xFFFFFFFFu, K, lane);
-    }
     if (final_pass) {
       const uint32_t valid = __ballot_sync(0xFFFFFFFFu, lane < K && L.ix != 0xFFFFFFFFu);
-      if (lane < K && L.ix != 0xFFFFFFFFu) out_idx[lane] = L.ix;
+      if (lane < K && L.ix != 0xFFFFFFFFu) out_idx[lane] = remap ? remap[L.ix] : L.ix;
       if (lane == 0) *out_count = (uint64_t)__popc(valid);
     } else if (lane < K) {
       SortItem it;
@@ -504,16 +597,11 @@ __global__ void __launch_bounds__(THREADS) k_topk_final(const __grid_constant__ 
         c.w[0] = k[u].w[0]; c.w[1] = k[u].w[1]; c.w[2] = k[u].w[2]; c.w[3] = k[u].w[3];
         c.ix = (uint32_t)g[u];
       }
-      warp_offer(L, c, v[u], K, lane);
+      warp_offer_batch(L, c, v[u], K, lane);
     }
   }
-  s_l[warp][lane] = L;
-  __syncthreads();
+  block_merge_lists<WARPS>(L, s_l, warp, lane);
   if (warp == 0) {
-    for (int w = 1; w < WARPS; ++w) {
-      const Cand c = s_l[w][lane];
-      warp_offer(L, c, lane < K && c.ix != 0xFFFFFFFFu, K, lane);
-    }
     if (lane < K) {
       SortItem it;
       it.w[0] = L.w[0]; it.w[1] = L.w[1]; it.w[2] = L.w[2]; it.w[3] = L.w[3];
@@ -581,8 +669,9 @@ static cudaError_t topk_b(const SortItem* keys, const uint32_t* idx, const uint6
 }
 
 cudaError_t launch_topk(const SortItem* keys, const uint32_t* idx, const uint64_t* count, uint64_t n_max, int k,
-                        uint32_t* out_idx, uint64_t* out_count, void* temp, uint32_t* status, cudaStream_t s) {
-  if (k <= 0 || k > 1024) return cudaErrorInvalidValue;
+                        uint32_t* out_idx, uint64_t* out_count, void* temp, uint32_t* status, cudaStream_t s,
+                        const uint32_t* remap) {
+  if (k <= 0 || k > 1024 || (remap && k > 32)) return cudaErrorInvalidValue;
   if (k <= 32) {
     unsigned ctas = (unsigned)sms();
     const uint64_t want = (n_max + 4095) / 4096;
@@ -590,7 +679,7 @@ cudaError_t launch_topk(const SortItem* keys, const uint32_t* idx, const uint64_
     SortItem* pk = (SortItem*)temp;
     uint32_t* pi = (uint32_t*)(pk + (uint64_t)ctas * k);
     k_topk_warp<256><<<ctas, 256, 0, s>>>(keys, idx, count, n_max, k, pk, pi, nullptr, 0);
-    k_topk_warp<256><<<1, 256, 0, s>>>(pk, pi, nullptr, (uint64_t)ctas * k, k, nullptr, out_idx, out_count, 1);
+    k_topk_warp<256><<<1, 256, 0, s>>>(pk, pi, nullptr, (uint64_t)ctas * k, k, nullptr, out_idx, out_count, 1, remap);
     return cudaGetLastError();
   }
   if (k <= 128) return topk_b<512>(keys, idx, count, n_max, k, out_idx, out_count, temp, s);

@@ -80,8 +80,10 @@ cudaError_t launch_radix_sort(SortItem* keys, uint32_t* idx, SortItem* keys_tmp,
                               cudaStream_t s, int* result_in_tmp);
 // Top-K of (keys, idx): smallest K images first. Writes K (or fewer) indices.
 size_t topk_temp_bytes(uint64_t n_max, int k);
+// remap (K <= 32 only): write remap[i] instead of the winning index i.
 cudaError_t launch_topk(const SortItem* keys, const uint32_t* idx, const uint64_t* count, uint64_t n_max, int k,
-                        uint32_t* out_idx, uint64_t* out_count, void* temp, uint32_t* status, cudaStream_t s);
+                        uint32_t* out_idx, uint64_t* out_count, void* temp, uint32_t* status, cudaStream_t s,
+                        const uint32_t* remap = nullptr);
 
 // Fused aggregate top-K (K <= 32) straight from the aggregate states: the
 // candidates are the groups g < n (n = min(*n_dev, n_max) when n_dev is
@@ -103,6 +105,10 @@ struct TopkFinalSpec {
   uint64_t n_max;
 };
 size_t topk_final_temp_bytes(uint64_t n_max, int k);
+// ORDER BY images (and indices i) of the groups gidx[i], i < *count, from
+// their states, the parts as in TopkFinalSpec (flag/state/n_dev unused).
+cudaError_t launch_encode_states(const TopkFinalSpec& spec, const uint32_t* gidx, const uint64_t* count,
+                                 uint64_t n_max, SortItem* keys, uint32_t* idx, cudaStream_t s);
 cudaError_t launch_topk_final(const TopkFinalSpec& spec, int k, uint32_t* out_g, uint64_t* out_count, void* temp,
                               cudaStream_t s);
 
