@@ -187,6 +187,10 @@ struct DAggTable {
   // `capacity` holds the group whose key equals kEmptyKey, and state[g] is
   // set to 2 when group g is first used.
   int32_t cas;
+  // Words between consecutive groups in keys[0] and the states (0 or 1:
+  // one array per state; larger: all of a group's words in one entry).
+  int32_t stride;
+  int32_t pad;
 };
 
 // ------------------------------------------------------------ pipeline

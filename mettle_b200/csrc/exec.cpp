@@ -393,6 +393,7 @@ struct Compiler {
     f.ptr = p;
     f.bytes = (bytes + 15) & ~15ULL;
     f.pattern = 0x0101010101010101ULL * (uint64_t)(byte & 0xFF);
+    f.stride = 0;
     fills.push_back(f);
   }
   void fill_step(void* p, uint64_t words, uint64_t v) {
@@ -400,6 +401,16 @@ struct Compiler {
     f.ptr = p;
     f.bytes = (words * 8 + 15) & ~15ULL;
     f.pattern = v;
+    f.stride = 0;
+    fills.push_back(f);
+  }
+  // one 8-byte word every stride_words words, n times
+  void fill_strided(void* p, uint64_t n, uint64_t stride_words, uint64_t v) {
+    FillSeg f;
+    f.ptr = p;
+    f.bytes = n * stride_words * 8;
+    f.pattern = v;
+    f.stride = stride_words * 8;
     fills.push_back(f);
   }
   void emit_fills() {
@@ -726,6 +737,7 @@ struct Compiler {
   uint32_t payload_mask(int s) const { return needed_root & subtree[s]; }
   int rep_src = -1;
   bool cas_table = false;  // one-key hash aggregate claimed by CAS on the key
+  int state_stride = 1;    // words between groups in the aggregate states
 
   void add_filters(PipeBuilder& pb, int s) {
     for (const BFilter& f : plan.filters) {
@@ -874,7 +886,7 @@ struct Compiler {
     return bound < ((__int128)1 << 63) - 1;
   }
 
-  void plan_states(uint64_t groups, uint64_t rows, bool need_count) {
+  void plan_states(uint64_t groups, uint64_t rows, bool need_count, bool alloc = true) {
     agg_sum_state.assign(plan.aggs.size(), -1);
     agg_cnt_state.assign(plan.aggs.size(), -1);
     agg_state.assign(plan.aggs.size(), -1);
@@ -882,8 +894,10 @@ struct Compiler {
       AggState s;
       s.fn_dev = fn;
       s.prog_agg = agg;
-      s.lo = (uint64_t*)scratch(groups * 8);
-      if (fn == A_SUM_I128) s.hi = (int64_t*)scratch(groups * 8);
+      if (alloc) {
+        s.lo = (uint64_t*)scratch(groups * 8);
+        if (fn == A_SUM_I128) s.hi = (int64_t*)scratch(groups * 8);
+      }
       states.push_back(s);
       return (int)states.size() - 1;
     };
@@ -958,6 +972,7 @@ struct Compiler {
     const AggState& st = states[si];
     f.a = st.lo;
     f.a_hi = st.hi;
+    f.stride = state_stride;
     switch (g.fn) {
       case AG_COUNT: f.kind = F_COPY_I64; break;
       case AG_SUM:
@@ -1159,7 +1174,7 @@ struct Compiler {
       // a one-key hash table keeps one more group: the key equal to the
       // empty-slot sentinel
       cas_table = !scalar && rep_src < 0 && plan.group_keys.size() == 1;
-      plan_states(cas_table ? groups + 1 : groups, root_rows, scalar);
+      plan_states(cas_table ? groups + 1 : groups, root_rows, scalar, !cas_table);
     }
 
     // build pipelines, children before parents
@@ -1330,27 +1345,45 @@ struct Compiler {
     pb.d.table.state = (uint32_t*)scratch(n_ent * 4);
     memset_step(pb.d.table.state, 0, n_ent * 4);
     for (size_t k = 0; k < plan.group_keys.size(); ++k) {
-      pb.d.table.keys[k] = (uint64_t*)scratch(n_ent * 8);
+      if (!cas_table) pb.d.table.keys[k] = (uint64_t*)scratch(n_ent * 8);
       pb.d.key_prog[k] = add_prog(pb, *plan.group_keys[k]);
     }
     if (cas_table) {
-      // keys start empty and states at their identities: a claim is one CAS
-      memset_step(pb.d.table.keys[0], 0xFF, n_ent * 8);
-      for (const AggState& s : states) {
-        fill_step(s.lo, n_ent, state_identity(s.fn_dev));
-        if (s.hi) fill_step(s.hi, n_ent, 0);
+      // One entry per group holds its key and all of its states, so a row
+      // touches one 32-byte-aligned entry. Keys start empty and states at
+      // their identities: a claim is one CAS.
+      int n_hi = 0;
+      for (const AggState& s : states) n_hi += s.fn_dev == A_SUM_I128;
+      const uint64_t words = 1 + states.size() + (uint64_t)n_hi;
+      const uint64_t stride = (words + 3) & ~3ULL;
+      uint64_t* aos = (uint64_t*)scratch(n_ent * stride * 8);
+      state_stride = (int)stride;
+      pb.d.table.keys[0] = aos;
+      pb.d.table.stride = (int32_t)stride;
+      fill_strided(aos, n_ent, stride, ~0ULL);
+      uint64_t hw = 1 + states.size();
+      for (size_t s = 0; s < states.size(); ++s) {
+        states[s].lo = aos + 1 + s;
+        fill_strided(states[s].lo, n_ent, stride, state_identity(states[s].fn_dev));
+        if (states[s].fn_dev == A_SUM_I128) {
+          states[s].hi = (int64_t*)(aos + hw++);
+          fill_strided(states[s].hi, n_ent, stride, 0);
+        }
       }
+    } else {
+      pb.d.table.stride = 1;
     }
     fill_aggs(pb, true);
-    // Shared-memory tables hold every group when there are few; with many,
-    // a fixed-size table keeps each CTA's frequent keys (a skewed key's rows
-    // then meet in shared memory instead of contending on one global
-    // state), and rows whose key is not there go to the global table.
-    pb.d.sink = SK_AGG_SMEM;
-    pb.d.smem_capacity = est_groups <= 1536 ? (int)std::max<uint64_t>(256, est_groups * 4 / 3 + 64) : 512;
-    if (pipeline_smem_bytes(pb.d) > 100 * 1024) {
-      pb.d.sink = SK_AGG_HASH;
-      pb.d.smem_capacity = 0;
+    // Few groups: each CTA aggregates in shared memory and merges into the
+    // global table at the end. Many: rows update the global table directly.
+    pb.d.sink = SK_AGG_HASH;
+    if (est_groups <= 1536) {
+      pb.d.sink = SK_AGG_SMEM;
+      pb.d.smem_capacity = (int)std::max<uint64_t>(256, est_groups * 4 / 3 + 64);
+      if (pipeline_smem_bytes(pb.d) > 150 * 1024) {
+        pb.d.sink = SK_AGG_HASH;
+        pb.d.smem_capacity = 0;
+      }
     }
     push_pipeline(pb, root_rows);
     std::vector<FinalOut> fo;
@@ -1366,6 +1399,7 @@ struct Compiler {
         const int32_t pt = dense[i].ptype;
         f.kind = pt == P_I32 ? F_COPY_I32 : pt == P_F32 ? F_COPY_F32 : F_COPY_I64;
         f.a = pb.d.table.keys[o.group_idx];
+        f.stride = pb.d.table.stride;
         fo.push_back(f);
       }
     }

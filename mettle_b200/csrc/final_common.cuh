@@ -73,6 +73,7 @@ static __device__ __noinline__ double avg_extended(__int128 sum, unsigned long l
 // types in the low 32 bits of lo).
 __device__ __forceinline__ void final_value(const FinalOut& f, uint64_t g, uint64_t& lo, uint64_t& hi) {
   hi = 0;
+  if (f.kind != F_GATHER_COL && f.stride > 1) g *= (uint64_t)f.stride;
   switch (f.kind) {
     case F_COPY_I32:
     case F_COPY_F32: lo = (uint32_t)f.a[g]; break;

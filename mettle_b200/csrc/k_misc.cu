@@ -320,6 +320,12 @@ cudaError_t launch_fill_u64(uint64_t* p, uint64_t n, uint64_t v, cudaStream_t s)
 
 __global__ void k_fill_segments(const FillSeg* __restrict__ segs) {
   const FillSeg sg = segs[blockIdx.y];
+  if (sg.stride) {
+    const uint64_t n = sg.bytes / sg.stride;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+      *(uint64_t*)((char*)sg.ptr + i * sg.stride) = sg.pattern;
+    return;
+  }
   const uint64_t n16 = sg.bytes / 16;
   const ulonglong2 v = make_ulonglong2(sg.pattern, sg.pattern);
   ulonglong2* p = (ulonglong2*)sg.ptr;

@@ -210,12 +210,14 @@ __device__ __noinline__ uint64_t agg_find_cas(const DAggTable& t, uint64_t key, 
     if (t.state[t.capacity] != 2u) t.state[t.capacity] = 2u;
     return t.capacity;
   }
+  const uint64_t stride = t.stride > 1 ? (uint64_t)t.stride : 1;
   for (uint64_t probe = 0; probe < t.capacity; ++probe) {
-    const uint64_t k = __ldcg(t.keys[0] + idx);
+    uint64_t* const kp = t.keys[0] + idx * stride;
+    const uint64_t k = __ldcg(kp);
     if (k == key) return idx;
     if ((int64_t)k == kEmptyKey) {
       const unsigned long long prev =
-          atomicCAS((unsigned long long*)(t.keys[0] + idx), (unsigned long long)kEmptyKey, (unsigned long long)key);
+          atomicCAS((unsigned long long*)kp, (unsigned long long)kEmptyKey, (unsigned long long)key);
       if (prev == (unsigned long long)kEmptyKey) {
         t.state[idx] = 2u;  // read only after the pipeline (compaction, top-K)
         return idx;
@@ -1056,6 +1058,9 @@ __global__ void __launch_bounds__(kThreads) k_pipeline(const __grid_constant__ P
       constexpr int B = kAggBatch;
       const DAggTable& tb = d.table;
       const VmProg& kp = d.progs[d.key_prog[0]];
+      const uint64_t gstride = tb.stride > 1 ? (uint64_t)tb.stride : 1;
+      const uint64_t* const gkeys = tb.keys[0];
+      const uint64_t gcap = tb.capacity;
       for (uint32_t i0 = 0; i0 < n_sel; i0 += THREADS * B) {
         uint32_t r[B];
         bool act[B];
@@ -1078,8 +1083,8 @@ __global__ void __launch_bounds__(kThreads) k_pipeline(const __grid_constant__ P
         }
 #pragma unroll
         for (int b = 0; b < B; ++b) {
-          h[b] = hash_slot(key_hash1(key[b]), tb.capacity);
-          k0[b] = (act[b] && sidx[b] < 0 && (int64_t)key[b] != kEmptyKey) ? __ldcg(tb.keys[0] + h[b]) : 0;
+          h[b] = hash_slot(key_hash1(key[b]), gcap);
+          k0[b] = (act[b] && sidx[b] < 0 && (int64_t)key[b] != kEmptyKey) ? __ldcg(gkeys + h[b] * gstride) : 0;
         }
 #pragma unroll
         for (int b = 0; b < B; ++b) {
@@ -1104,8 +1109,9 @@ __global__ void __launch_bounds__(kThreads) k_pipeline(const __grid_constant__ P
                                   : nullptr;
               agg_apply(ag.fn, (unsigned long long*)(sagg.lo + (size_t)a * sagg.cap + sidx[b]), hp, v[b], vt);
             } else if (g[b] != kNoGroup) {
-              agg_apply_g(ag.fn, (unsigned long long*)(ag.lo + g[b]), (long long*)(ag.hi ? ag.hi + g[b] : nullptr),
-                          v[b], vt);
+              const uint64_t o = g[b] * gstride;
+              agg_apply_g(ag.fn, (unsigned long long*)(ag.lo + o), (long long*)(ag.hi ? ag.hi + o : nullptr), v[b],
+                          vt);
             }
           }
         }
@@ -1217,10 +1223,11 @@ __global__ void __launch_bounds__(kThreads) k_pipeline(const __grid_constant__ P
       for (int q = 0; q < kMaxKeys; ++q) kw[q] = q < d.table.n_keys ? sagg.keys[(size_t)q * sagg.cap + i] : 0;
       uint64_t g = agg_find_global(d, kw, st);
       if (g == kNoGroup) continue;
+      const uint64_t o = g * (d.table.stride > 1 ? (uint64_t)d.table.stride : 1);
       for (int a = 0; a < d.n_aggs; ++a) {
         const DAgg& ag = d.aggs[a];
         int64_t hv = sagg.hi_index[a] >= 0 ? sagg.hi[(size_t)sagg.hi_index[a] * sagg.cap + i] : 0;
-        agg_merge(ag.fn, (unsigned long long*)(ag.lo + g), (long long*)(ag.hi ? ag.hi + g : nullptr),
+        agg_merge(ag.fn, (unsigned long long*)(ag.lo + o), (long long*)(ag.hi ? ag.hi + o : nullptr),
                   sagg.lo[(size_t)a * sagg.cap + i], hv);
       }
     }

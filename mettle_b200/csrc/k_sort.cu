@@ -430,7 +430,7 @@ __device__ __forceinline__ Cand cand_shfl_xor(const Cand& c, int m) {
 }
 
 // Bitonic sort of one candidate per lane, ascending across the warp.
-__device__ __noinline__ void warp_sort32(Cand& c, int lane) {
+__device__ __forceinline__ void warp_sort32(Cand& c, int lane) {
 #pragma unroll
   for (int k = 2; k <= 32; k <<= 1) {
 #pragma unroll
@@ -445,7 +445,7 @@ __device__ __noinline__ void warp_sort32(Cand& c, int lane) {
 // L and M are ascending across the warp; L becomes the 32 smallest of both,
 // ascending. Elementwise min against M reversed leaves a bitonic sequence
 // holding the 32 smallest, which five half-cleaner steps sort.
-__device__ __noinline__ void warp_merge32(Cand& L, const Cand& M, int lane) {
+__device__ __forceinline__ void warp_merge32(Cand& L, const Cand& M, int lane) {
   const Cand r = cand_shfl(M, 31 - lane);
   if (cand_less(r, L)) L = r;
 #pragma unroll
@@ -679,7 +679,7 @@ cudaError_t launch_topk(const SortItem* keys, const uint32_t* idx, const uint64_
     SortItem* pk = (SortItem*)temp;
     uint32_t* pi = (uint32_t*)(pk + (uint64_t)ctas * k);
     k_topk_warp<256><<<ctas, 256, 0, s>>>(keys, idx, count, n_max, k, pk, pi, nullptr, 0);
-    k_topk_warp<256><<<1, 256, 0, s>>>(pk, pi, nullptr, (uint64_t)ctas * k, k, nullptr, out_idx, out_count, 1, remap);
+    k_topk_warp<1024><<<1, 1024, 0, s>>>(pk, pi, nullptr, (uint64_t)ctas * k, k, nullptr, out_idx, out_count, 1, remap);
     return cudaGetLastError();
   }
   if (k <= 128) return topk_b<512>(keys, idx, count, n_max, k, out_idx, out_count, temp, s);

@@ -55,6 +55,8 @@ struct FinalOut {
   const uint64_t* a;     // state or key words, indexed by group g
   const int64_t* a_hi;   // high words
   const uint64_t* cnt;   // counts (AVG)
+  int32_t stride;        // words between consecutive groups' words in a, a_hi, cnt (0 or 1: dense)
+  int32_t pad;
   void* out;
   double scale;          // AVG of DECIMAL: 10^scale
   const void* col;       // F_GATHER_COL column
@@ -143,6 +145,7 @@ struct FillSeg {
   void* ptr;
   uint64_t bytes;
   uint64_t pattern;
+  uint64_t stride;  // 0: fill [ptr, ptr + bytes); else one 8-byte word every `stride` bytes
 };
 cudaError_t launch_fill_segments(const FillSeg* segs_dev, int n_segs, uint64_t max_bytes, cudaStream_t s);
 
