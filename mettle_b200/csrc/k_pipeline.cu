@@ -301,15 +301,12 @@ __device__ __forceinline__ void smem_agg_init(const PipeDesc& d, SmemAgg& s, uin
   }
 }
 
-// Finds or claims kw in the CTA table; -1 when it is not among the first
-// kSmemProbes slots of its chain (the caller then uses the global table), so
-// a full table costs a bounded number of probes per row.
-constexpr int kSmemProbes = 4;
+// Finds or claims kw in the CTA table; -1 when the table is full (the
+// caller then uses the global table).
 __device__ __forceinline__ int smem_agg_find(const PipeDesc& d, SmemAgg& s, const uint64_t* kw, uint32_t& st) {
   const int nk = d.table.n_keys;
   int idx = (int)hash_slot(key_hash(kw, nk), (uint64_t)s.cap);
-  const int probes = s.cap < kSmemProbes ? s.cap : kSmemProbes;
-  for (int probe = 0; probe < probes; ++probe) {
+  for (int probe = 0; probe < s.cap; ++probe) {
     volatile uint32_t* sp = s.state + idx;
     uint32_t v = *sp;
     if (v == 0) {
@@ -339,8 +336,9 @@ __device__ __forceinline__ int smem_agg_find(const PipeDesc& d, SmemAgg& s, cons
 }
 
 // ------------------------------------------------------------ the kernel
-constexpr int kThreads = 128;
-constexpr int kTile = 1024;  // tuples per tile
+constexpr int kWarps = 8;                 // warps per CTA, each an independent tile processor
+constexpr int kThreads = kWarps * 32;
+constexpr int kTile = 256;                // rows per warp-tile
 
 struct StreamLayout {
   int n;
@@ -517,8 +515,8 @@ __device__ __forceinline__ Val vm_eval_fast(const VmFast& f, const TileCtx& t, u
   return fast_op(f.op[1], f.op_cast[1], fast_op(f.op[0], f.op_cast[0], a, b, st), c, st);
 }
 
-// Expression VM over one tile row.
-__device__ __forceinline__ Val vm_eval_t(const VmProg& p, const TileCtx& t, uint32_t r, uint32_t& st) {
+// Expression VM over one tile row, all forms.
+__device__ __forceinline__ Val vm_eval_full(const VmProg& p, const TileCtx& t, uint32_t r, uint32_t& st) {
   if (p.fast.shape) return vm_eval_fast(p.fast, t, r, st);
   if (p.depth > 4) return vm_eval_deep(p, t, r, st);
   RegStack S;
@@ -565,15 +563,9 @@ __device__ __forceinline__ Val vm_eval_t(const VmProg& p, const TileCtx& t, uint
   return S.s0;
 }
 
-// Warp-aggregated append of tile row r to a shared selection list. Every
-// lane of the warp must call it (keep may be false).
-__device__ __forceinline__ void sel_push(bool keep, uint32_t r, uint16_t* out, uint32_t* cnt) {
-  const uint32_t m = __ballot_sync(0xFFFFFFFFu, keep);
-  const int lane = threadIdx.x & 31;
-  uint32_t base = 0;
-  if (lane == 0 && m) base = atomicAdd(cnt, (uint32_t)__popc(m));
-  base = __shfl_sync(0xFFFFFFFFu, base, 0);
-  if (keep) out[base + __popc(m & ((1u << lane) - 1u))] = (uint16_t)r;
+// Expression VM over one tile row.
+__device__ __forceinline__ Val vm_eval_t(const VmProg& p, const TileCtx& t, uint32_t r, uint32_t& st) {
+  return vm_eval_full(p, t, r, st);
 }
 
 // Integer predicates are evaluated as a closed interval [lo, hi] (negated for
@@ -597,51 +589,46 @@ __device__ __forceinline__ IntRange to_range(const DPred& p) {
   return r;
 }
 
-// Filter op over the current selection: one loop per (column type, source),
-// chosen once per tile. A thread evaluates all of its (at most kTile /
-// kThreads) rows before the first ballot, so their loads are in flight
-// together, and each warp reserves its output range with one atomic.
+// Filter op over a warp's selection: one loop per (column type, source),
+// chosen once per op. A lane evaluates all of its (at most kTile / 32)
+// entries before the first ballot, so their loads are in flight together;
+// kept rows are compacted in order with ballots. Returns the new count.
 template <typename GET>
-__device__ __forceinline__ void filter_loop(uint32_t n_sel, bool ident, const uint16_t* in, uint16_t* out,
-                                            uint32_t* cnt, GET get_keep) {
-  constexpr int U = kTile / kThreads;
+__device__ __forceinline__ uint32_t filter_w(uint32_t n_sel, bool ident, const uint16_t* in, uint16_t* out,
+                                             GET get_keep) {
+  constexpr int U = kTile / 32;
   const int lane = threadIdx.x & 31;
-  uint32_t km = 0;  // bit j: row j of this thread is kept
+  const uint32_t lt = (1u << lane) - 1u;
+  uint32_t km = 0;  // bit j: entry j * 32 + lane is kept
 #pragma unroll
   for (int j = 0; j < U; ++j) {
-    const uint32_t i = (uint32_t)j * kThreads + threadIdx.x;
+    const uint32_t i = (uint32_t)j * 32 + lane;
     if (i < n_sel && get_keep(ident ? i : (uint32_t)in[i])) km |= 1u << j;
   }
-  uint32_t tot = 0;
-#pragma unroll
-  for (int j = 0; j < U; ++j) tot += __popc(__ballot_sync(0xFFFFFFFFu, (km >> j) & 1u));
   uint32_t base = 0;
-  if (lane == 0 && tot) base = atomicAdd(cnt, tot);
-  base = __shfl_sync(0xFFFFFFFFu, base, 0);
-  const uint32_t lt = (1u << lane) - 1u;
 #pragma unroll
   for (int j = 0; j < U; ++j) {
     const uint32_t m = __ballot_sync(0xFFFFFFFFu, (km >> j) & 1u);
     if ((km >> j) & 1u) {
-      const uint32_t i = (uint32_t)j * kThreads + threadIdx.x;
+      const uint32_t i = (uint32_t)j * 32 + lane;
       out[base + __popc(m & lt)] = (uint16_t)(ident ? i : (uint32_t)in[i]);
     }
     base += __popc(m);
   }
+  return base;
 }
 
-// First filter of a tile on a streamed integer column: thread t owns the
-// kTile / kThreads consecutive rows starting at t * (kTile / kThreads),
-// reads them with 128-bit shared-memory loads, and writes the rows it keeps
-// in order after a warp prefix sum, so the selection comes out sorted within
-// each warp's range.
+// First filter of a warp-tile on a streamed integer column: lane l owns the
+// kTile / 32 consecutive rows from l * (kTile / 32), reads them with 128-bit
+// shared-memory loads, and writes the rows it keeps after a warp prefix sum,
+// so the selection stays sorted. Returns the new count.
 template <typename T>
-__device__ __forceinline__ void filter_ident_blocked(const T* col, uint32_t nrow, const IntRange& rg, uint16_t* out,
-                                                     uint32_t* cnt) {
-  constexpr int U = kTile / kThreads;
-  static_assert(U * sizeof(T) % 16 == 0, "rows per thread must fill whole 16-byte vectors");
+__device__ __forceinline__ uint32_t filter_ident_blocked(const T* col, uint32_t nrow, const IntRange& rg,
+                                                         uint16_t* out) {
+  constexpr int U = kTile / 32;
+  static_assert(U * sizeof(T) % 16 == 0, "rows per lane must fill whole 16-byte vectors");
   const int lane = threadIdx.x & 31;
-  const uint32_t b0 = threadIdx.x * U;
+  const uint32_t b0 = (uint32_t)lane * U;
   T v[U];
   const uint4* src = (const uint4*)(col + b0);
 #pragma unroll
@@ -671,34 +658,66 @@ __device__ __forceinline__ void filter_ident_blocked(const T* col, uint32_t nrow
     const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
     if (lane >= o) incl += y;
   }
-  const uint32_t tot = __shfl_sync(0xFFFFFFFFu, incl, 31);
-  uint32_t base = 0;
-  if (lane == 0 && tot) base = atomicAdd(cnt, tot);
-  uint32_t pos = __shfl_sync(0xFFFFFFFFu, base, 0) + incl - c;
+  uint32_t pos = incl - c;
 #pragma unroll
   for (int j = 0; j < U; ++j)
     if ((km >> j) & 1u) out[pos++] = (uint16_t)(b0 + j);
+  return __shfl_sync(0xFFFFFFFFu, incl, 31);
 }
 
-// Join probe over the current selection, kProbeBatch rows per thread at a
+// Join probe over the current selection, kProbeBatch rows per lane at a
 // time: keys, then the presence words and map entries (dense) or first
 // probed slots (hash) of the whole batch are loaded before any is used.
 constexpr int kProbeBatch = 4;
-constexpr int kAggBatch = 4;  // rows per thread in flight in the single-key hash sink
+constexpr int kAggBatch = 4;  // rows per lane in flight in the single-key hash sink
+constexpr int kTileFetch = 1;  // warp-tiles taken per fetch of the dynamic tile counter
 
+// Bytes of the CTA-wide shared-memory sink area (the AGG_SMEM table),
+// rounded to 128.
+__host__ __device__ inline uint32_t sink_area_bytes(const PipeDesc& d) {
+  if (d.sink != SK_AGG_SMEM) return 0;
+  uint32_t n128 = 0;
+  for (int a = 0; a < d.n_aggs; ++a) n128 += d.aggs[a].fn == A_SUM_I128;
+  const uint32_t b = (uint32_t)d.smem_capacity * (4 + 8 * (uint32_t)d.table.n_keys + 8 * (uint32_t)d.n_aggs + 8 * n128);
+  return (b + 127) & ~127u;
+}
+
+// Bytes of one warp's shared-memory region, rounded to 128: two stream
+// buffers (row_bytes streamed per row), two selection vectors, probe slots,
+// probed row ids.
+__host__ __device__ inline uint32_t warp_area_bytes(uint32_t row_bytes, int nq) {
+  const uint32_t b = 2 * (uint32_t)kTile * row_bytes + 2 * kTile * 2 + kTile * 4 + (uint32_t)nq * kTile * 4;
+  return (b + 127) & ~127u;
+}
+
+__host__ __device__ inline int probed_source_count(const PipeDesc& d) {
+  int nq = 0;
+  for (int s = 0; s < kMaxSrc; ++s) {
+    if (s == d.drive_src) continue;
+    bool used = false;
+    for (int p = 0; p < d.n_probes; ++p) used |= ((d.probes[p].fill_mask >> s) & 1u) != 0;
+    nq += used;
+  }
+  return nq;
+}
+
+// One CTA of kWarps warps; every warp is an independent tile processor. A
+// warp streams its own kTile-row tiles into its own double buffer (one TMA
+// bulk copy per streamed column, its own mbarriers), runs the ops and the
+// sink over them with warp-level compaction, and never waits for the other
+// warps of the CTA inside the tile loop: a slow tile (a long sink chain, a
+// look-back) stalls only its warp while the others keep the SM busy.
 template <int SINK>
-__global__ void __launch_bounds__(kThreads) k_pipeline(const __grid_constant__ PipeDesc d) {
-  constexpr int THREADS = kThreads, TILE = kTile;
+__global__ void __launch_bounds__(kThreads, (SINK == SK_AGG_SCALAR || SINK == SK_AGG_SMEM) ? 2 : 3)
+    k_pipeline(const __grid_constant__ PipeDesc d) {
+  constexpr int TILE = kTile;
   extern __shared__ __align__(128) uint8_t smem[];
-  __shared__ __align__(8) uint64_t s_mbar[2];
-  __shared__ uint32_t s_warp[THREADS / 32 + 1];
-  __shared__ uint64_t s_base;
-  __shared__ uint64_t s_tile[2];
-  __shared__ uint32_t s_cnt[3];
-  __shared__ uint64_t s_red[SINK == SK_AGG_SCALAR ? kMaxAggs : 1][THREADS / 32];
-  __shared__ int64_t s_redhi[SINK == SK_AGG_SCALAR ? kMaxAggs : 1][THREADS / 32];
+  __shared__ __align__(8) uint64_t s_mbar[kWarps][2];
+  __shared__ uint64_t s_red[SINK == SK_AGG_SCALAR ? kMaxAggs : 1][kWarps];
+  __shared__ int64_t s_redhi[SINK == SK_AGG_SCALAR ? kMaxAggs : 1][kWarps];
 
-  const int tid = threadIdx.x;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const uint32_t lt = (1u << lane) - 1u;
   const uint64_t n = d.in_count ? *d.in_count : d.n;
   const uint64_t n_tiles = (n + TILE - 1) / TILE;
   uint32_t st = 0;
@@ -728,19 +747,18 @@ __global__ void __launch_bounds__(kThreads) k_pipeline(const __grid_constant__ P
       ++nq;
     }
   }
-  // shared layout: stream buffers x2 | sel A | sel B | slot | rid arrays | sink
-  uint8_t* const sbuf0 = smem;
-  uint8_t* const sbuf1 = smem + S.bytes;
-  uint16_t* const selA = (uint16_t*)(smem + 2 * S.bytes);
+  // shared layout: sink area | warp 0 | warp 1 | ...; a warp's region holds
+  // stream buffers x2 | sel A | sel B | slots | probed row ids
+  uint8_t* const wreg = smem + sink_area_bytes(d) + (size_t)warp * warp_area_bytes(S.bytes / TILE, nq);
+  uint8_t* const sbuf0 = wreg;
+  uint8_t* const sbuf1 = wreg + S.bytes;
+  uint16_t* const selA = (uint16_t*)(wreg + 2 * S.bytes);
   uint16_t* const selB = selA + TILE;
   uint32_t* const s_slot = (uint32_t*)(selB + TILE);
   uint32_t* const s_srid = s_slot + TILE;
-  uint8_t* const sink_smem = (uint8_t*)(s_srid + (size_t)nq * TILE);
-  uint8_t* s_keep = sink_smem;                       // MATERIALIZE
-  uint16_t* s_list = (uint16_t*)(sink_smem + TILE);  // MATERIALIZE
 
   SmemAgg sagg;
-  if (SINK == SK_AGG_SMEM) smem_agg_init(d, sagg, sink_smem);
+  if (SINK == SK_AGG_SMEM) smem_agg_init(d, sagg, smem);
   uint64_t plo[SINK == SK_AGG_SCALAR ? kMaxAggs : 1];
   int64_t phi[SINK == SK_AGG_SCALAR ? kMaxAggs : 1];
   if (SINK == SK_AGG_SCALAR) {
@@ -759,42 +777,48 @@ __global__ void __launch_bounds__(kThreads) k_pipeline(const __grid_constant__ P
       phi[a] = 0;
     }
   }
-  if (tid == 0) {
-    if (S.n) {
-      mbar_init(&s_mbar[0], 1);
-      mbar_init(&s_mbar[1], 1);
-      mbar_fence_init();
-    }
-    s_cnt[0] = s_cnt[1] = s_cnt[2] = 0;
+  if (lane == 0 && S.n) {
+    mbar_init(&s_mbar[warp][0], 1);
+    mbar_init(&s_mbar[warp][1], 1);
+    mbar_fence_init();
   }
+  __syncthreads();
 
+  // Tile order: order-preserving compaction takes tiles from a counter in
+  // increasing order (kTileFetch at a time), so every tile's predecessors
+  // are held by running warps; other sinks stride over the tiles.
   const bool dynamic_tiles = SINK == SK_MATERIALIZE;
-  // Thread 0 stages the streamed columns of a full tile into buffer `b`.
+  const uint64_t n_warps = (uint64_t)gridDim.x * kWarps;
+  uint64_t chunk_next = 0, chunk_end = 0;
+  auto fetch = [&](uint64_t prev, bool first) -> uint64_t {
+    if (!dynamic_tiles) return first ? (uint64_t)blockIdx.x * kWarps + warp : prev + n_warps;
+    if (chunk_next < chunk_end) return chunk_next++;
+    uint32_t t = 0;
+    if (lane == 0) t = atomicAdd(d.tile_counter, (uint32_t)kTileFetch);
+    t = __shfl_sync(0xFFFFFFFFu, t, 0);
+    chunk_next = (uint64_t)t + 1;
+    chunk_end = (uint64_t)t + kTileFetch;
+    return (uint64_t)t;
+  };
+  // Lane 0 stages the streamed columns of a full tile into buffer `b`.
   auto issue = [&](uint64_t tile, int b) {
     const uint64_t base = tile * (uint64_t)TILE;
     if (base + TILE > n) return;  // the tail tile is loaded directly
     uint8_t* dst = b ? sbuf1 : sbuf0;
     fence_proxy_async();
-    mbar_arrive_expect_tx(&s_mbar[b], S.bytes);
+    mbar_arrive_expect_tx(&s_mbar[warp][b], S.bytes);
     for (int i = 0; i < S.n; ++i)
       bulk_g2s(dst + S.off[i], (const uint8_t*)d.cols[S.col[i]].ptr + base * (uint64_t)S.width[i],
-               (uint32_t)TILE * (uint32_t)S.width[i], &s_mbar[b]);
+               (uint32_t)TILE * (uint32_t)S.width[i], &s_mbar[warp][b]);
   };
 
-  if (tid == 0) s_tile[0] = dynamic_tiles ? (uint64_t)atomicAdd(d.tile_counter, 1u) : (uint64_t)blockIdx.x;
-  __syncthreads();
-  uint64_t cur = s_tile[0];
-  if (tid == 0 && S.n && cur < n_tiles) issue(cur, 0);
+  uint64_t cur = fetch(0, true);
+  if (lane == 0 && S.n && cur < n_tiles) issue(cur, 0);
   uint32_t parity = 0;
   int b = 0;
-  uint32_t k = 0;
-  uint32_t cq = 0;  // selection-counter rotation
   while (cur < n_tiles) {
-    if (tid == 0) {
-      const uint64_t nx = dynamic_tiles ? (uint64_t)atomicAdd(d.tile_counter, 1u) : cur + gridDim.x;
-      s_tile[(k + 1) & 1] = nx;
-      if (S.n && nx < n_tiles) issue(nx, b ^ 1);
-    }
+    const uint64_t nx = fetch(cur, false);
+    if (lane == 0 && S.n && nx < n_tiles) issue(nx, b ^ 1);
     const uint64_t tile = cur;
     const uint64_t tile_base = tile * (uint64_t)TILE;
     const uint32_t nrow = (uint32_t)(n - tile_base < (uint64_t)TILE ? n - tile_base : (uint64_t)TILE);
@@ -802,36 +826,36 @@ __global__ void __launch_bounds__(kThreads) k_pipeline(const __grid_constant__ P
     if (S.n) {
       bool ok = true;
       if (nrow == TILE) {
-        ok = mbar_wait(&s_mbar[b], (parity >> b) & 1u);
+        ok = mbar_wait(&s_mbar[warp][b], (parity >> b) & 1u);
         parity ^= 1u << b;
       } else {
         for (int i = 0; i < S.n; ++i) {
           const DCol& c = d.cols[S.col[i]];
-          for (int r = tid; r < TILE; r += THREADS) {
+          for (int r = lane; r < TILE; r += 32) {
             int64_t v = (uint32_t)r < nrow ? load_bits(c.ptr, c.ptype, tile_base + r) : 0;
             if (S.width[i] == 4) ((uint32_t*)(buf + S.off[i]))[r] = (uint32_t)v;
             else ((int64_t*)(buf + S.off[i]))[r] = v;
           }
         }
+        __syncwarp();
       }
-      if (__syncthreads_or(!ok)) {
+      if (__any_sync(0xFFFFFFFFu, !ok)) {
         st |= ST_SPIN_LIMIT;
         // give the copy still in flight a bounded chance to land, then stop
-        mbar_wait(&s_mbar[b ^ 1], (parity >> (b ^ 1)) & 1u);
+        if (nx < n_tiles) mbar_wait(&s_mbar[warp][b ^ 1], (parity >> (b ^ 1)) & 1u);
         break;
       }
     }
     TileCtx tc{&d, &S, buf, tile_base, s_srid, slot_of_src};
 
-    // ---- ops over the selection vector
+    // ---- ops over the warp's selection vector
     uint32_t n_sel = nrow;
     bool ident = true;
     uint16_t* sel_in = selA;
     uint16_t* sel_out = selB;
     for (int o = 0; o < d.n_ops && n_sel > 0; ++o) {
-      uint32_t* cnt = &s_cnt[cq];
-      if (tid == 0) s_cnt[(cq + 1) % 3] = 0;  // next op's counter (last read two barriers ago)
       const PipeOp op = d.ops[o];
+      uint32_t kept = 0;
       if (op.kind == OPK_FILTER) {
         const DPred& p = d.preds[op.idx];
         const DCol& c = d.cols[p.col];
@@ -839,42 +863,39 @@ __global__ void __launch_bounds__(kThreads) k_pipeline(const __grid_constant__ P
         if (c.ptype == P_I32 || c.ptype == P_I64) {
           const IntRange rg = to_range(p);
           if (rg.none) {
-            filter_loop(n_sel, ident, sel_in, sel_out, cnt, [&](uint32_t) { return false; });
+            kept = 0;
           } else if (si >= 0 && ident && S.width[si] == 4 && c.ptype == P_I32) {
-            filter_ident_blocked<int32_t>((const int32_t*)(buf + S.off[si]), n_sel, rg, sel_out, cnt);
+            kept = filter_ident_blocked<int32_t>((const int32_t*)(buf + S.off[si]), n_sel, rg, sel_out);
           } else if (si >= 0 && ident && S.width[si] == 8) {
-            filter_ident_blocked<int64_t>((const int64_t*)(buf + S.off[si]), n_sel, rg, sel_out, cnt);
+            kept = filter_ident_blocked<int64_t>((const int64_t*)(buf + S.off[si]), n_sel, rg, sel_out);
           } else if (si >= 0 && S.width[si] == 4) {
             const int32_t* col = (const int32_t*)(buf + S.off[si]);
-            filter_loop(n_sel, ident, sel_in, sel_out, cnt, [&](uint32_t r) {
+            kept = filter_w(n_sel, ident, sel_in, sel_out, [&](uint32_t r) {
               const int64_t x = col[r];
               return (x >= rg.lo && x <= rg.hi) != rg.neg;
             });
           } else if (si >= 0) {
             const int64_t* col = (const int64_t*)(buf + S.off[si]);
-            filter_loop(n_sel, ident, sel_in, sel_out, cnt, [&](uint32_t r) {
+            kept = filter_w(n_sel, ident, sel_in, sel_out, [&](uint32_t r) {
               const int64_t x = col[r];
               return (x >= rg.lo && x <= rg.hi) != rg.neg;
             });
           } else {
-            filter_loop(n_sel, ident, sel_in, sel_out, cnt, [&](uint32_t r) {
+            kept = filter_w(n_sel, ident, sel_in, sel_out, [&](uint32_t r) {
               const int64_t x = load_bits(c.ptr, c.ptype, tc_rid(tc, c.src, r));
               return (x >= rg.lo && x <= rg.hi) != rg.neg;
             });
           }
         } else {
-          filter_loop(n_sel, ident, sel_in, sel_out, cnt, [&](uint32_t r) {
+          kept = filter_w(n_sel, ident, sel_in, sel_out, [&](uint32_t r) {
             return eval_pred_bits(tc_get(tc, p.col, r), c.ptype, p);
           });
         }
       } else {
         const DProbe& pr = d.probes[op.idx];
-        const DCol& c = d.cols[pr.key_col];
         const DBuild& bd = d.builds[pr.build];
         const bool want_slot = op.idx == d.slot_probe;
         const uint32_t fill = pr.fill_mask & ~(1u << d.drive_src);
-        const int lane = tid & 31;
-        const uint32_t lt = (1u << lane) - 1u;
         const ColAcc ka = col_acc(tc, pr.key_col);
         const bool k32 = ka.sm && ka.width == 4 && ka.ptype == P_I32;  // streamed INTEGER key
         // Descriptor fields used per row, read once: the loop's shared-memory
@@ -884,14 +905,13 @@ __global__ void __launch_bounds__(kThreads) k_pipeline(const __grid_constant__ P
         const uint32_t* const b_bits = bd.dense_bits;
         const uint32_t* const b_map = bd.dense_map;
         const bool b_dense = bd.kind == B_DENSE;
-        (void)c;
-        for (uint32_t i0 = 0; i0 < n_sel; i0 += THREADS * kProbeBatch) {
+        for (uint32_t i0 = 0; i0 < n_sel; i0 += 32 * kProbeBatch) {
           uint32_t r[kProbeBatch], slot[kProbeBatch];
           bool act[kProbeBatch], keep[kProbeBatch];
           int64_t key[kProbeBatch];
 #pragma unroll
           for (int j = 0; j < kProbeBatch; ++j) {
-            const uint32_t i = i0 + (uint32_t)j * THREADS + tid;
+            const uint32_t i = i0 + (uint32_t)j * 32 + lane;
             act[j] = i < n_sel;
             r[j] = act[j] ? (ident ? i : (uint32_t)sel_in[i]) : 0u;
             key[j] = !act[j] ? 0 : k32 ? (int64_t)((const int32_t*)ka.sm)[r[j]] : acc_get(ka, tc, r[j]);
@@ -934,8 +954,6 @@ __global__ void __launch_bounds__(kThreads) k_pipeline(const __grid_constant__ P
               }
             }
           }
-          uint32_t m[kProbeBatch];
-          uint32_t tot = 0;
 #pragma unroll
           for (int j = 0; j < kProbeBatch; ++j) {
             if (keep[j]) {
@@ -945,53 +963,25 @@ __global__ void __launch_bounds__(kThreads) k_pipeline(const __grid_constant__ P
                   if ((fill >> s) & 1u)
                     s_srid[(size_t)((slot_of_src >> (4 * s)) & 0xFu) * TILE + r[j]] = bd.payload[s][slot[j]];
             }
-            m[j] = __ballot_sync(0xFFFFFFFFu, keep[j]);
-            tot += __popc(m[j]);
-          }
-          uint32_t obase = 0;
-          if (lane == 0 && tot) obase = atomicAdd(cnt, tot);
-          obase = __shfl_sync(0xFFFFFFFFu, obase, 0);
-#pragma unroll
-          for (int j = 0; j < kProbeBatch; ++j) {
-            if (keep[j]) sel_out[obase + __popc(m[j] & lt)] = (uint16_t)r[j];
-            obase += __popc(m[j]);
+            const uint32_t m = __ballot_sync(0xFFFFFFFFu, keep[j]);
+            if (keep[j]) sel_out[kept + __popc(m & lt)] = (uint16_t)r[j];
+            kept += __popc(m);
           }
         }
       }
-      __syncthreads();
-      n_sel = *cnt;
+      __syncwarp();
+      n_sel = kept;
       ident = false;
       uint16_t* t_ = sel_in;
       sel_in = sel_out;
       sel_out = t_;
-      cq = (cq + 1) % 3;
     }
 
-    // ---- sink over the surviving tile rows
+    // ---- sink over the surviving rows (sorted: ballots keep row order)
     if (SINK == SK_MATERIALIZE) {
-      for (int r = tid; r < TILE; r += THREADS) s_keep[r] = 0;
-      __syncthreads();
-      for (uint32_t i = tid; i < n_sel; i += THREADS) s_keep[ident ? i : sel_in[i]] = 1;
-      __syncthreads();
-      // Blocked arrangement for the scan: thread t owns tile rows [t*8, (t+1)*8).
-      constexpr int PER = TILE / THREADS;
-      uint32_t cntk = 0;
-#pragma unroll
-      for (int i = 0; i < PER; ++i) cntk += s_keep[tid * PER + i];
-      uint32_t total;
-      uint32_t pos = block_excl_sum<THREADS>(cntk, s_warp, &total);
-#pragma unroll
-      for (int i = 0; i < PER; ++i)
-        if (s_keep[tid * PER + i]) s_list[pos++] = (uint16_t)(tid * PER + i);
-      if (tid < 32) {
-        const uint64_t excl = lb_exclusive_warp(d.tile_status, tile, total, d.epoch, d.status);
-        if (tid == 0) {
-          s_base = excl;
-          if (tile == n_tiles - 1) *d.out_count = excl + total;
-        }
-      }
-      __syncthreads();
-      const uint64_t base = s_base;
+      const uint32_t total = n_sel;
+      const uint64_t base = lb_exclusive_warp(d.tile_status, tile, total, d.epoch, d.status);
+      if (lane == 0 && tile == n_tiles - 1) *d.out_count = base + total;
       // write phase: one output column at a time over the compacted rows
       const uint32_t lim = base >= d.out_capacity ? 0u
                            : (uint32_t)(d.out_capacity - base < (uint64_t)total ? d.out_capacity - base : total);
@@ -1004,9 +994,9 @@ __global__ void __launch_bounds__(kThreads) k_pipeline(const __grid_constant__ P
           // plain column: typed copy
           const ColAcc ca = col_acc(tc, pg.ins[0].arg);
 #pragma unroll 4
-          for (uint32_t p = tid; p < lim; p += THREADS) {
+          for (uint32_t p = lane; p < lim; p += 32) {
             Val v;
-            v.lo = acc_get(ca, tc, s_list[p]);
+            v.lo = acc_get(ca, tc, ident ? p : (uint32_t)sel_in[p]);
             v.hi = v.lo >> 63;
             store_val(out, ot, base + p, v);
           }
@@ -1017,27 +1007,29 @@ __global__ void __launch_bounds__(kThreads) k_pipeline(const __grid_constant__ P
           const Val kc{pg.ins[1].k, pg.ins[1].k2};
           const int16_t aop = pg.ins[2].op, aty = pg.ins[2].type;
 #pragma unroll 4
-          for (uint32_t p = tid; p < lim; p += THREADS) {
+          for (uint32_t p = lane; p < lim; p += 32) {
             Val v;
-            v.lo = acc_get(ca, tc, s_list[p]);
+            v.lo = acc_get(ca, tc, ident ? p : (uint32_t)sel_in[p]);
             v.hi = v.lo >> 63;
             store_val(out, ot, base + p, vm_arith(aop, aty, v, kc, st));
           }
         } else {
-          for (uint32_t p = tid; p < lim; p += THREADS) store_val(out, ot, base + p, vm_eval_t(pg, tc, s_list[p], st));
+          for (uint32_t p = lane; p < lim; p += 32)
+            store_val(out, ot, base + p, vm_eval_t(pg, tc, ident ? p : (uint32_t)sel_in[p], st));
         }
       }
       for (int s = 0; s < kMaxSrc; ++s)
         if ((d.out_rid_mask >> s) & 1u)
-          for (uint32_t p = tid; p < lim; p += THREADS) d.out_rids[s][base + p] = tc_rid(tc, s, s_list[p]);
+          for (uint32_t p = lane; p < lim; p += 32)
+            d.out_rids[s][base + p] = tc_rid(tc, s, ident ? p : (uint32_t)sel_in[p]);
     } else if (SINK == SK_BUILD) {
       const DBuild& bd = d.builds[d.sink_build];
-      // One slot reservation per tile: the tile's surviving rows take
+      // One slot reservation per warp-tile: its surviving rows take
       // consecutive slots.
-      if (tid == 0) s_base = n_sel ? (uint64_t)atomicAdd(bd.n_slots, n_sel) : 0;
-      __syncthreads();
-      const uint32_t sbase = (uint32_t)s_base;
-      for (uint32_t i = tid; i < n_sel; i += THREADS) {
+      uint32_t sbase = 0;
+      if (lane == 0 && n_sel) sbase = atomicAdd(bd.n_slots, n_sel);
+      sbase = __shfl_sync(0xFFFFFFFFu, sbase, 0);
+      for (uint32_t i = lane; i < n_sel; i += 32) {
         const uint32_t r = ident ? i : (uint32_t)sel_in[i];
         const uint32_t slot = sbase + i;
         const int64_t key = tc_get(tc, d.build_key_col, r);
@@ -1061,14 +1053,14 @@ __global__ void __launch_bounds__(kThreads) k_pipeline(const __grid_constant__ P
       const uint64_t gstride = tb.stride > 1 ? (uint64_t)tb.stride : 1;
       const uint64_t* const gkeys = tb.keys[0];
       const uint64_t gcap = tb.capacity;
-      for (uint32_t i0 = 0; i0 < n_sel; i0 += THREADS * B) {
+      for (uint32_t i0 = 0; i0 < n_sel; i0 += 32 * B) {
         uint32_t r[B];
         bool act[B];
         int sidx[B];
         uint64_t key[B], h[B], k0[B], g[B];
 #pragma unroll
         for (int b = 0; b < B; ++b) {
-          const uint32_t i = i0 + (uint32_t)b * THREADS + tid;
+          const uint32_t i = i0 + (uint32_t)b * 32 + lane;
           act[b] = i < n_sel;
           r[b] = act[b] ? (ident ? i : (uint32_t)sel_in[i]) : 0u;
           key[b] = act[b] ? (uint64_t)vm_eval_t(kp, tc, r[b], st).lo : 0;
@@ -1118,7 +1110,7 @@ __global__ void __launch_bounds__(kThreads) k_pipeline(const __grid_constant__ P
       }
     } else {
       uint8_t* const slot_hit = d.slot_hit;
-      for (uint32_t i = tid; i < n_sel; i += THREADS) {
+      for (uint32_t i = lane; i < n_sel; i += 32) {
         const uint32_t r = ident ? i : (uint32_t)sel_in[i];
         if (SINK == SK_AGG_SLOT) {
           const uint32_t g = s_slot[r];
@@ -1195,15 +1187,15 @@ __global__ void __launch_bounds__(kThreads) k_pipeline(const __grid_constant__ P
         }
       }
     }
-    // Every thread is done with `buf`, the selection and the sink scratch.
-    __syncthreads();
-    cur = s_tile[(k + 1) & 1];
-    ++k;
+    // Every lane is done with `buf` and the selection before they are reused.
+    __syncwarp();
+    cur = nx;
     b ^= 1;
   }
 
   // End-of-kernel work.
   if (SINK == SK_MATERIALIZE) {
+    __syncthreads();
     if (tid == 0) {
       if (n == 0 && blockIdx.x == 0) *d.out_count = 0;
       // The last CTA to finish resets the dynamic tile counter for the next launch.
@@ -1216,7 +1208,7 @@ __global__ void __launch_bounds__(kThreads) k_pipeline(const __grid_constant__ P
     }
   } else if (SINK == SK_AGG_SMEM) {
     __syncthreads();
-    for (int i = tid; i < sagg.cap; i += THREADS) {
+    for (int i = tid; i < sagg.cap; i += kThreads) {
       if (sagg.state[i] != 2u) continue;
       uint64_t kw[kMaxKeys];
 #pragma unroll
@@ -1233,7 +1225,6 @@ __global__ void __launch_bounds__(kThreads) k_pipeline(const __grid_constant__ P
     }
   } else if (SINK == SK_AGG_SCALAR) {
     // Block reduction of the register partials, then one atomic per CTA.
-    const int lane = tid & 31, warp = tid >> 5;
 #pragma unroll
     for (int a = 0; a < kMaxAggs; ++a) {
       if (a >= d.n_aggs) break;
@@ -1262,7 +1253,7 @@ __global__ void __launch_bounds__(kThreads) k_pipeline(const __grid_constant__ P
     __syncthreads();
     if (tid < d.n_aggs) {
       const DAgg& ag = d.aggs[tid];
-      for (int w = 0; w < THREADS / 32; ++w)
+      for (int w = 0; w < kWarps; ++w)
         agg_merge(ag.fn, (unsigned long long*)ag.lo, (long long*)ag.hi, s_red[tid][w], s_redhi[tid][w]);
     }
   }
@@ -1281,32 +1272,10 @@ static int sm_count() {
   return g_sm_count;
 }
 
-size_t pipeline_tile_rows() { return kTile; }
-
-static int probed_sources(const PipeDesc& d) {
-  int nq = 0;
-  for (int s = 0; s < kMaxSrc; ++s) {
-    if (s == d.drive_src) continue;
-    bool used = false;
-    for (int p = 0; p < d.n_probes; ++p) used |= ((d.probes[p].fill_mask >> s) & 1u) != 0;
-    nq += used;
-  }
-  return nq;
-}
 
 size_t pipeline_smem_bytes(const PipeDesc& d) {
-  constexpr size_t TILE = kTile;
-  size_t s = 2ull * TILE * stream_bytes_per_row(d);  // stream buffers
-  s += 2 * TILE * 2;                                  // selection vectors
-  s += TILE * 4;                                      // probe slots
-  s += (size_t)probed_sources(d) * TILE * 4;          // probed row ids
-  if (d.sink == SK_MATERIALIZE) s += TILE + 2 * TILE;  // keep flags + compacted list
-  if (d.sink == SK_AGG_SMEM) {
-    size_t n128 = 0;
-    for (int a = 0; a < d.n_aggs; ++a) n128 += d.aggs[a].fn == A_SUM_I128;
-    s += (size_t)d.smem_capacity * (4 + 8 * d.table.n_keys + 8 * d.n_aggs + 8 * n128);
-  }
-  return s;
+  return (size_t)sink_area_bytes(d) +
+         (size_t)kWarps * warp_area_bytes(stream_bytes_per_row(d), probed_source_count(d));
 }
 
 // Occupancy per (sink, dynamic smem) is computed once and cached: these
@@ -1342,7 +1311,7 @@ static cudaError_t launch_sink(const PipeDesc& d, uint64_t n_hint, cudaStream_t 
     }
   }
   // Grid = resident CTAs per SM x SM count (a persistent grid-stride grid).
-  uint64_t tiles = (n_hint + kTile - 1) / kTile;
+  uint64_t tiles = (n_hint + (uint64_t)kTile * kWarps - 1) / ((uint64_t)kTile * kWarps);
   uint64_t max_grid = (uint64_t)sm_count() * (uint64_t)blocks_per_sm;
   uint64_t grid = tiles < max_grid ? tiles : max_grid;
   if (grid == 0) grid = 1;
@@ -1354,7 +1323,7 @@ cudaError_t launch_pipeline(const PipeDesc& d, uint64_t n_hint, cudaStream_t s) 
   if (d.tuple_input) return cudaErrorInvalidValue;  // every pipeline scans a base table
   switch (d.sink) {
     case SK_BUILD: return launch_sink<SK_BUILD>(d, n_hint, s);
-    case SK_MATERIALIZE: return launch_sink<SK_MATERIALIZE>(d, n_hint, s);
+    case SK_MATERIALIZE: return launch_pipeline_materialize(d, n_hint, s);
     case SK_AGG_HASH: return launch_sink<SK_AGG_HASH>(d, n_hint, s);
     case SK_AGG_SMEM: return launch_sink<SK_AGG_SMEM>(d, n_hint, s);
     case SK_AGG_SLOT: return launch_sink<SK_AGG_SLOT>(d, n_hint, s);

@@ -14,6 +14,10 @@ size_t pipeline_tile_rows();
 size_t pipeline_smem_bytes(const PipeDesc& d);
 // n_hint bounds the tuples (grid sizing when the count lives on the device).
 cudaError_t launch_pipeline(const PipeDesc& d, uint64_t n_hint, cudaStream_t s);
+// Order-preserving compaction (SK_MATERIALIZE) runs a kernel with CTA-wide
+// tiles of pipeline_tile_rows() rows (k_pipeline_cta.cu); launch_pipeline
+// dispatches to it.
+cudaError_t launch_pipeline_materialize(const PipeDesc& d, uint64_t n_hint, cudaStream_t s);
 
 // ---- aggregate finalize (k_misc.cu)
 // Order-preserving list of READY slots of a hash aggregate table.
