@@ -247,7 +247,7 @@ struct PipeDesc {
   int32_t slot_probe;               // AGG_SLOT: probe whose slot is the group
   uint8_t* slot_hit;                // AGG_SLOT: 1 when the group saw a row
   int32_t smem_capacity;            // AGG_SMEM: slots per CTA table
-  int32_t pad2;
+  int32_t smem_probes;              // AGG_SMEM one-key tables: slots probed before the global table
 
   uint32_t* status;                 // DevStatus bits
 };

@@ -804,8 +804,10 @@ struct Compiler {
     if (d.tuple_input) return;
     uint32_t budget = 16;  // bytes per tuple: 64 KB of double-buffered tiles
     if (d.sink == SK_AGG_SMEM) {
+      // keep the CTA within about 110 KB so two fit on an SM: stream
+      // buffers take 2 x 2048 bytes per streamed byte of a row
       size_t table = pipeline_smem_bytes(d);
-      budget = table >= 150 * 1024 ? 0 : (uint32_t)std::min<size_t>(16, (150 * 1024 - table) / (2 * 2048));
+      budget = table >= 110 * 1024 ? 0 : (uint32_t)std::min<size_t>(16, (110 * 1024 - table) / (2 * 2048));
     }
     uint32_t used = 0;
     auto try_stream = [&](int col) {
@@ -1173,7 +1175,7 @@ struct Compiler {
       }
       // a one-key hash table keeps one more group: the key equal to the
       // empty-slot sentinel
-      cas_table = !scalar && rep_src < 0 && plan.group_keys.size() == 1;
+      cas_table = !scalar && rep_src < 0 && plan.group_keys.size() == 1 && groups + 1 < (1ull << 31);
       plan_states(cas_table ? groups + 1 : groups, root_rows, scalar, !cas_table);
     }
 
@@ -1375,9 +1377,21 @@ struct Compiler {
     }
     fill_aggs(pb, true);
     // Few groups: each CTA aggregates in shared memory and merges into the
-    // global table at the end. Many: rows update the global table directly.
+    // global table at the end. Many: rows update the global table directly;
+    // with one key, a small shared-memory table in front of it keeps each
+    // CTA's most frequent keys (the first to arrive), so a skewed key's rows
+    // meet in shared memory instead of contending on one global entry.
     pb.d.sink = SK_AGG_HASH;
-    if (est_groups <= 1536) {
+    if (cas_table) {
+      pb.d.sink = SK_AGG_SMEM;
+      const bool whole = est_groups <= 1536;
+      pb.d.smem_capacity = whole ? (int)(est_groups * 3 / 2 + 64) : 1024;
+      pb.d.smem_probes = whole ? pb.d.smem_capacity : 2;
+      if (pipeline_smem_bytes(pb.d) > 160 * 1024) {
+        pb.d.sink = SK_AGG_HASH;
+        pb.d.smem_capacity = 0;
+      }
+    } else if (est_groups <= 1536) {
       pb.d.sink = SK_AGG_SMEM;
       pb.d.smem_capacity = (int)std::max<uint64_t>(256, est_groups * 4 / 3 + 64);
       if (pipeline_smem_bytes(pb.d) > 150 * 1024) {

@@ -335,6 +335,86 @@ __device__ __forceinline__ int smem_agg_find(const PipeDesc& d, SmemAgg& s, cons
   return -1;
 }
 
+// One-key shared-memory table of a CTA (AGG_SMEM with DAggTable::cas): the
+// same entry layout as the global table (word 0 the key, word 1 + a state
+// a, then the high words of 128-bit sums), keys claimed by CAS, states
+// started at their identities, updates by shared-memory reductions.
+struct SmemCas {
+  uint64_t* e;
+  uint32_t cap;
+  uint32_t stride;
+};
+
+__device__ __forceinline__ void smem_cas_init(const PipeDesc& d, SmemCas& s, uint8_t* base) {
+  s.e = (uint64_t*)base;
+  s.cap = (uint32_t)d.smem_capacity;
+  s.stride = d.table.stride > 1 ? (uint32_t)d.table.stride : 1;
+  const uint32_t words = s.cap * s.stride;
+  for (uint32_t i = threadIdx.x; i < words; i += blockDim.x) {
+    const uint32_t w = i % s.stride;
+    uint64_t v = 0;
+    if (w == 0) {
+      v = (uint64_t)kEmptyKey;
+    } else if ((int)w <= d.n_aggs) {
+      switch (d.aggs[w - 1].fn) {
+        case A_MIN_I: v = 0x7FFFFFFFFFFFFFFFULL; break;
+        case A_MAX_I: v = 0x8000000000000000ULL; break;
+        case A_MIN_F: v = ~0ULL; break;
+        default: v = 0; break;
+      }
+    }
+    s.e[i] = v;
+  }
+}
+
+// Entry of key in the table, probing at most `limit` slots; -1 when it is
+// not there and cannot be claimed (or the key is the empty sentinel).
+__device__ __forceinline__ int smem_cas_find(const SmemCas& s, uint64_t key, uint32_t limit) {
+  if ((int64_t)key == kEmptyKey) return -1;
+  uint32_t idx = (uint32_t)hash_slot(key_hash1(key), (uint64_t)s.cap);
+  for (uint32_t probe = 0; probe < limit; ++probe) {
+    uint64_t* kp = s.e + (size_t)idx * s.stride;
+    const uint64_t k = *(volatile uint64_t*)kp;
+    if (k == key) return (int)idx;
+    if ((int64_t)k == kEmptyKey) {
+      const unsigned long long prev =
+          atomicCAS((unsigned long long*)kp, (unsigned long long)kEmptyKey, (unsigned long long)key);
+      if (prev == (unsigned long long)kEmptyKey || prev == key) return (int)idx;
+    }
+    if (++idx == s.cap) idx = 0;
+  }
+  return -1;
+}
+
+// Applies one value to a state word in shared memory (address `a` in the
+// shared window), without waiting for the result where the op allows.
+__device__ __forceinline__ void smem_apply(int32_t fn, uint32_t a, uint32_t a_hi, Val v, int32_t vt) {
+  switch (fn) {
+    case A_COUNT: asm volatile("red.shared.add.u64 [%0], %1;" ::"r"(a), "l"(1ULL) : "memory"); break;
+    case A_SUM_I: asm volatile("red.shared.add.u64 [%0], %1;" ::"r"(a), "l"((uint64_t)v.lo) : "memory"); break;
+    case A_SUM_I128: {
+      uint64_t old;
+      const uint64_t add = (uint64_t)v.lo;
+      asm volatile("atom.shared.add.u64 %0, [%1], %2;" : "=l"(old) : "r"(a), "l"(add) : "memory");
+      const int64_t hadd = (vt == P_I128 ? v.hi : (v.lo >> 63)) + ((old + add) < old ? 1 : 0);
+      if (hadd) asm volatile("red.shared.add.u64 [%0], %1;" ::"r"(a_hi), "l"((uint64_t)hadd) : "memory");
+      break;
+    }
+    case A_SUM_F:
+      asm volatile("red.shared.add.f64 [%0], %1;" ::"r"(a), "d"(val_as_f64(v, vt)) : "memory");
+      break;
+    case A_MIN_I: asm volatile("red.shared.min.s64 [%0], %1;" ::"r"(a), "l"(v.lo) : "memory"); break;
+    case A_MAX_I: asm volatile("red.shared.max.s64 [%0], %1;" ::"r"(a), "l"(v.lo) : "memory"); break;
+    case A_MIN_F:
+      asm volatile("red.shared.min.u64 [%0], %1;" ::"r"(a), "l"(ord_f64(val_as_f64(v, vt))) : "memory");
+      break;
+    case A_MAX_F:
+      asm volatile("red.shared.max.u64 [%0], %1;" ::"r"(a), "l"(ord_f64(val_as_f64(v, vt))) : "memory");
+      break;
+    default: break;
+  }
+}
+
 // ------------------------------------------------------------ the kernel
 constexpr int kWarps = 8;                 // warps per CTA, each an independent tile processor
 constexpr int kThreads = kWarps * 32;
@@ -676,6 +756,10 @@ constexpr int kTileFetch = 1;  // warp-tiles taken per fetch of the dynamic tile
 // rounded to 128.
 __host__ __device__ inline uint32_t sink_area_bytes(const PipeDesc& d) {
   if (d.sink != SK_AGG_SMEM) return 0;
+  if (d.table.cas) {
+    const uint32_t stride = d.table.stride > 1 ? (uint32_t)d.table.stride : 1;
+    return ((uint32_t)d.smem_capacity * stride * 8 + 127) & ~127u;
+  }
   uint32_t n128 = 0;
   for (int a = 0; a < d.n_aggs; ++a) n128 += d.aggs[a].fn == A_SUM_I128;
   const uint32_t b = (uint32_t)d.smem_capacity * (4 + 8 * (uint32_t)d.table.n_keys + 8 * (uint32_t)d.n_aggs + 8 * n128);
@@ -758,7 +842,11 @@ __global__ void __launch_bounds__(kThreads, (SINK == SK_AGG_SCALAR || SINK == SK
   uint32_t* const s_srid = s_slot + TILE;
 
   SmemAgg sagg;
-  if (SINK == SK_AGG_SMEM) smem_agg_init(d, sagg, smem);
+  SmemCas scas;
+  if (SINK == SK_AGG_SMEM) {
+    if (d.table.cas) smem_cas_init(d, scas, smem);
+    else smem_agg_init(d, sagg, smem);
+  }
   uint64_t plo[SINK == SK_AGG_SCALAR ? kMaxAggs : 1];
   int64_t phi[SINK == SK_AGG_SCALAR ? kMaxAggs : 1];
   if (SINK == SK_AGG_SCALAR) {
@@ -1043,16 +1131,20 @@ __global__ void __launch_bounds__(kThreads, (SINK == SK_AGG_SCALAR || SINK == SK
         build_insert(bd, key, slot, st);
       }
     } else if ((SINK == SK_AGG_HASH || SINK == SK_AGG_SMEM) && d.table.cas) {
-      // One 64-bit group key: kAggBatch rows per thread at a time. Keys held
-      // in the CTA's shared-memory table are updated there; for the others
-      // the first probed global key words are read together, and states are
-      // updated with atomics whose results are not waited for.
+      // One 64-bit group key. Phase 1 finds every surviving row's group
+      // (kAggBatch rows per lane in flight; keys held in the CTA's
+      // shared-memory table stay there) and parks it in s_slot; phase 2
+      // applies one aggregate at a time over the rows, with the column
+      // access resolved once per aggregate, and updates global states with
+      // atomics whose results are not waited for.
       constexpr int B = kAggBatch;
       const DAggTable& tb = d.table;
       const VmProg& kp = d.progs[d.key_prog[0]];
       const uint64_t gstride = tb.stride > 1 ? (uint64_t)tb.stride : 1;
       const uint64_t* const gkeys = tb.keys[0];
       const uint64_t gcap = tb.capacity;
+      const bool key_col = kp.fast.shape == 1 && kp.fast.leaf[0].op == VM_COL && !kp.fast.leaf_cast[0].on;
+      const ColAcc kca = col_acc(tc, key_col ? kp.fast.leaf[0].arg : 0);
       for (uint32_t i0 = 0; i0 < n_sel; i0 += 32 * B) {
         uint32_t r[B];
         bool act[B];
@@ -1063,15 +1155,12 @@ __global__ void __launch_bounds__(kThreads, (SINK == SK_AGG_SCALAR || SINK == SK
           const uint32_t i = i0 + (uint32_t)b * 32 + lane;
           act[b] = i < n_sel;
           r[b] = act[b] ? (ident ? i : (uint32_t)sel_in[i]) : 0u;
-          key[b] = act[b] ? (uint64_t)vm_eval_t(kp, tc, r[b], st).lo : 0;
+          key[b] = !act[b] ? 0 : key_col ? (uint64_t)acc_get(kca, tc, r[b]) : (uint64_t)vm_eval_t(kp, tc, r[b], st).lo;
         }
 #pragma unroll
         for (int b = 0; b < B; ++b) {
           sidx[b] = -1;
-          if (SINK == SK_AGG_SMEM && act[b]) {
-            const uint64_t kw[kMaxKeys] = {key[b], 0, 0, 0};
-            sidx[b] = smem_agg_find(d, sagg, kw, st);
-          }
+          if (SINK == SK_AGG_SMEM && act[b]) sidx[b] = smem_cas_find(scas, key[b], (uint32_t)d.smem_probes);
         }
 #pragma unroll
         for (int b = 0; b < B; ++b) {
@@ -1083,28 +1172,48 @@ __global__ void __launch_bounds__(kThreads, (SINK == SK_AGG_SCALAR || SINK == SK
           g[b] = kNoGroup;
           if (act[b] && sidx[b] < 0)
             g[b] = ((int64_t)key[b] != kEmptyKey && k0[b] == key[b]) ? h[b] : agg_find_cas(tb, key[b], h[b], st);
+          if (act[b])
+            s_slot[i0 + (uint32_t)b * 32 + lane] =
+                sidx[b] >= 0 ? (0x80000000u | (uint32_t)sidx[b]) : (g[b] == kNoGroup ? 0xFFFFFFFFu : (uint32_t)g[b]);
         }
-        for (int a = 0; a < d.n_aggs; ++a) {
-          const DAgg& ag = d.aggs[a];
-          const int32_t vt = ag.prog >= 0 ? d.progs[ag.prog].out_type : P_I64;
-          Val v[B];
-#pragma unroll
-          for (int b = 0; b < B; ++b) {
-            v[b] = Val{0, 0};
-            if (ag.prog >= 0 && (sidx[b] >= 0 || g[b] != kNoGroup)) v[b] = vm_eval_t(d.progs[ag.prog], tc, r[b], st);
+      }
+      __syncwarp();
+      for (int a = 0; a < d.n_aggs; ++a) {
+        const DAgg& ag = d.aggs[a];
+        const int32_t fn = ag.fn;
+        unsigned long long* const alo = (unsigned long long*)ag.lo;
+        long long* const ahi = (long long*)ag.hi;
+        const VmProg* const pg = ag.prog >= 0 ? &d.progs[ag.prog] : nullptr;
+        const int32_t vt = pg ? pg->out_type : P_I64;
+        const bool vcol = pg && pg->fast.shape == 1 && pg->fast.leaf[0].op == VM_COL && !pg->fast.leaf_cast[0].on;
+        const ColAcc vca = col_acc(tc, vcol ? pg->fast.leaf[0].arg : 0);
+        const bool vsigned = vcol && (pg->fast.leaf[0].type == P_I32 || pg->fast.leaf[0].type == P_I64);
+        // shared-window addresses of this state's words in entry 0
+        uint32_t s_lo = 0, s_hi = 0;
+        if (SINK == SK_AGG_SMEM) {
+          int hw = 0;
+          for (int q = 0; q < a; ++q) hw += d.aggs[q].fn == A_SUM_I128;
+          s_lo = smem_u32(scas.e + 1 + a);
+          s_hi = smem_u32(scas.e + 1 + d.n_aggs + hw);
+        }
+#pragma unroll 4
+        for (uint32_t p = lane; p < n_sel; p += 32) {
+          const uint32_t code = s_slot[p];
+          if (code == 0xFFFFFFFFu) continue;
+          const uint32_t rr = ident ? p : (uint32_t)sel_in[p];
+          Val v{0, 0};
+          if (vcol) {
+            v.lo = acc_get(vca, tc, rr);
+            v.hi = vsigned ? (v.lo >> 63) : 0;
+          } else if (pg) {
+            v = vm_eval_t(*pg, tc, rr, st);
           }
-#pragma unroll
-          for (int b = 0; b < B; ++b) {
-            if (SINK == SK_AGG_SMEM && sidx[b] >= 0) {
-              long long* hp = sagg.hi_index[a] >= 0
-                                  ? (long long*)(sagg.hi + (size_t)sagg.hi_index[a] * sagg.cap + sidx[b])
-                                  : nullptr;
-              agg_apply(ag.fn, (unsigned long long*)(sagg.lo + (size_t)a * sagg.cap + sidx[b]), hp, v[b], vt);
-            } else if (g[b] != kNoGroup) {
-              const uint64_t o = g[b] * gstride;
-              agg_apply_g(ag.fn, (unsigned long long*)(ag.lo + o), (long long*)(ag.hi ? ag.hi + o : nullptr), v[b],
-                          vt);
-            }
+          if (SINK == SK_AGG_SMEM && (code & 0x80000000u)) {
+            const uint32_t eo = (code & 0x7FFFFFFFu) * scas.stride * 8;
+            smem_apply(fn, s_lo + eo, s_hi + eo, v, vt);
+          } else {
+            const uint64_t o = (uint64_t)code * gstride;
+            agg_apply_g(fn, alo + o, ahi ? ahi + o : nullptr, v, vt);
           }
         }
       }
@@ -1204,6 +1313,23 @@ __global__ void __launch_bounds__(kThreads, (SINK == SK_AGG_SCALAR || SINK == SK
       if (done == gridDim.x - 1) {
         d.tile_counter[0] = 0;
         d.tile_counter[1] = 0;
+      }
+    }
+  } else if (SINK == SK_AGG_SMEM && d.table.cas) {
+    __syncthreads();
+    const uint64_t gstride = d.table.stride > 1 ? (uint64_t)d.table.stride : 1;
+    for (uint32_t i = tid; i < scas.cap; i += kThreads) {
+      const uint64_t* ent = scas.e + (size_t)i * scas.stride;
+      const uint64_t key = ent[0];
+      if ((int64_t)key == kEmptyKey) continue;
+      const uint64_t g = agg_find_cas(d.table, key, hash_slot(key_hash1(key), d.table.capacity), st);
+      if (g == kNoGroup) continue;
+      const uint64_t o = g * gstride;
+      int hw = 0;
+      for (int a = 0; a < d.n_aggs; ++a) {
+        const DAgg& ag = d.aggs[a];
+        const int64_t hv = ag.fn == A_SUM_I128 ? (int64_t)ent[1 + d.n_aggs + hw++] : 0;
+        agg_merge(ag.fn, (unsigned long long*)(ag.lo + o), (long long*)(ag.hi ? ag.hi + o : nullptr), ent[1 + a], hv);
       }
     }
   } else if (SINK == SK_AGG_SMEM) {
