@@ -785,6 +785,17 @@ __host__ __device__ inline int probed_source_count(const PipeDesc& d) {
   return nq;
 }
 
+// Decoded fused opening of a pipeline (see the kernel).
+struct FusedOpen {
+  int32_t on, empty, neg, want_slot;
+  uint32_t foff, koff;
+  int32_t lo, hi;
+  int64_t kmin;
+  uint64_t cap;
+  const uint32_t* bits;
+  const uint32_t* map;
+};
+
 // One CTA of kWarps warps; every warp is an independent tile processor. A
 // warp streams its own kTile-row tiles into its own double buffer (one TMA
 // bulk copy per streamed column, its own mbarriers), runs the ops and the
@@ -797,6 +808,7 @@ __global__ void __launch_bounds__(kThreads, (SINK == SK_AGG_SCALAR || SINK == SK
   constexpr int TILE = kTile;
   extern __shared__ __align__(128) uint8_t smem[];
   __shared__ __align__(8) uint64_t s_mbar[kWarps][2];
+  __shared__ FusedOpen s_fz;
   __shared__ uint64_t s_red[SINK == SK_AGG_SCALAR ? kMaxAggs : 1][kWarps];
   __shared__ int64_t s_redhi[SINK == SK_AGG_SCALAR ? kMaxAggs : 1][kWarps];
 
@@ -900,6 +912,43 @@ __global__ void __launch_bounds__(kThreads, (SINK == SK_AGG_SCALAR || SINK == SK
                (uint32_t)TILE * (uint32_t)S.width[i], &s_mbar[warp][b]);
   };
 
+  // The common opening of a join pipeline — a range filter on a streamed
+  // INTEGER/DATE column, then a dense-join probe keyed by a streamed INTEGER
+  // column — runs fused per lane over its own rows: no selection vector
+  // between the two, and the probe loads of all of a lane's rows in flight
+  // together. Decoded once per CTA into shared memory (s_fz).
+  if (tid == 0) {
+    s_fz.on = 0;
+    if (d.n_ops >= 2 && d.ops[0].kind == OPK_FILTER && d.ops[1].kind == OPK_PROBE) {
+      const DPred& p = d.preds[d.ops[0].idx];
+      const DCol& c = d.cols[p.col];
+      const int si = c.src == d.drive_src ? stream_index(S, p.col) : -1;
+      const DProbe& pr = d.probes[d.ops[1].idx];
+      const DBuild& bd = d.builds[pr.build];
+      const DCol& kc = d.cols[pr.key_col];
+      const int sk = kc.src == d.drive_src ? stream_index(S, pr.key_col) : -1;
+      const uint32_t fill = pr.fill_mask & ~(1u << d.drive_src);
+      if (si >= 0 && c.ptype == P_I32 && S.width[si] == 4 && sk >= 0 && kc.ptype == P_I32 && S.width[sk] == 4 &&
+          bd.kind == B_DENSE && fill == 0) {
+        const IntRange rg = to_range(p);
+        s_fz.on = 1;
+        s_fz.foff = S.off[si];
+        s_fz.koff = S.off[sk];
+        s_fz.empty = (rg.none || rg.lo > rg.hi || rg.lo > (int64_t)INT32_MAX || rg.hi < (int64_t)INT32_MIN) ? 1 : 0;
+        s_fz.lo = (int32_t)(rg.lo < (int64_t)INT32_MIN ? (int64_t)INT32_MIN : rg.lo);
+        s_fz.hi = (int32_t)(rg.hi > (int64_t)INT32_MAX ? (int64_t)INT32_MAX : rg.hi);
+        s_fz.neg = rg.neg ? 1 : 0;
+        s_fz.kmin = bd.key_min;
+        s_fz.cap = bd.capacity;
+        s_fz.bits = bd.dense_bits;
+        s_fz.map = bd.dense_map;
+        s_fz.want_slot = d.ops[1].idx == d.slot_probe ? 1 : 0;
+      }
+    }
+  }
+  __syncthreads();
+  const bool fz = s_fz.on != 0;
+
   uint64_t cur = fetch(0, true);
   if (lane == 0 && S.n && cur < n_tiles) issue(cur, 0);
   uint32_t parity = 0;
@@ -941,7 +990,60 @@ __global__ void __launch_bounds__(kThreads, (SINK == SK_AGG_SCALAR || SINK == SK
     bool ident = true;
     uint16_t* sel_in = selA;
     uint16_t* sel_out = selB;
-    for (int o = 0; o < d.n_ops && n_sel > 0; ++o) {
+    int o0 = 0;
+    if (fz) {
+      constexpr int U = TILE / 32;
+      const uint32_t b0 = (uint32_t)lane * U;
+      int32_t fv[U], kv[U];
+#pragma unroll
+      for (int q = 0; q < U / 4; ++q) {
+        ((uint4*)fv)[q] = ((const uint4*)(buf + s_fz.foff))[lane * (U / 4) + q];
+        ((uint4*)kv)[q] = ((const uint4*)(buf + s_fz.koff))[lane * (U / 4) + q];
+      }
+      uint32_t w[U], mv[U];
+      uint64_t kk[U];
+      const bool fz_empty = s_fz.empty != 0, fz_neg = s_fz.neg != 0;
+      const int32_t fz_lo = s_fz.lo, fz_hi = s_fz.hi;
+      const int64_t fz_kmin = s_fz.kmin;
+      const uint64_t fz_cap = s_fz.cap;
+      const uint32_t* const fz_bits = s_fz.bits;
+      const uint32_t* const fz_map = s_fz.map;
+      const bool fz_want_slot = s_fz.want_slot != 0;
+#pragma unroll
+      for (int j = 0; j < U; ++j) {
+        const bool pass = ((!fz_empty && fv[j] >= fz_lo && fv[j] <= fz_hi) != fz_neg) && b0 + j < nrow;
+        kk[j] = (uint64_t)((int64_t)kv[j] - fz_kmin);
+        const bool inb = pass && kk[j] < fz_cap;
+        w[j] = inb ? __ldg(fz_bits + (kk[j] >> 5)) : 0u;
+        mv[j] = inb ? __ldg(fz_map + kk[j]) : 0u;
+      }
+      uint32_t km = 0;
+#pragma unroll
+      for (int j = 0; j < U; ++j) {
+        if ((w[j] >> (kk[j] & 31)) & 1u) {
+          km |= 1u << j;
+          if (fz_want_slot) s_slot[b0 + j] = mv[j] - 1u;
+        }
+      }
+      const uint32_t c = __popc(km);
+      uint32_t incl = c;
+#pragma unroll
+      for (int q = 1; q < 32; q <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, q);
+        if (lane >= q) incl += y;
+      }
+      uint32_t pos = incl - c;
+#pragma unroll
+      for (int j = 0; j < U; ++j)
+        if ((km >> j) & 1u) sel_out[pos++] = (uint16_t)(b0 + j);
+      n_sel = __shfl_sync(0xFFFFFFFFu, incl, 31);
+      __syncwarp();
+      ident = false;
+      sel_in = sel_out;
+      sel_out = selA;
+      o0 = 2;
+    }
+    for (int o = o0; o < d.n_ops && n_sel > 0; ++o) {
       const PipeOp op = d.ops[o];
       uint32_t kept = 0;
       if (op.kind == OPK_FILTER) {

@@ -723,7 +723,7 @@ cudaError_t launch_topk(const SortItem* keys, const uint32_t* idx, const uint64_
     SortItem* pk = (SortItem*)temp;
     uint32_t* pi = (uint32_t*)(pk + (uint64_t)ctas * k);
     k_topk_warp<256><<<ctas, 256, 0, s>>>(keys, idx, count, n_max, k, pk, pi, nullptr, 0);
-    k_topk_warp<1024><<<1, 1024, 0, s>>>(pk, pi, nullptr, (uint64_t)ctas * k, k, nullptr, out_idx, out_count, 1, remap);
+    k_topk_warp<256><<<1, 256, 0, s>>>(pk, pi, nullptr, (uint64_t)ctas * k, k, nullptr, out_idx, out_count, 1, remap);
     return cudaGetLastError();
   }
   if (k <= 128) return topk_b<512>(keys, idx, count, n_max, k, out_idx, out_count, temp, s);
