@@ -827,7 +827,9 @@ struct Compiler {
       if (o == 0 || reach >= kStreamAbove) try_stream(col);
       reach *= op.kind == OPK_FILTER ? (o < (int)pb.op_sel.size() ? pb.op_sel[o] : 0.5) : 0.25;
     }
-    if (reach >= kStreamAbove)
+    // A build's key column is streamed at a lower reach: its read sits on the
+    // critical path of the sink (the map store depends on it).
+    if (reach >= kStreamAbove || (d.sink == SK_BUILD && reach >= 0.05))
       for (int c : sink) try_stream(c);
   }
 
