@@ -1474,34 +1474,16 @@ struct Compiler {
     const int K = (int)plan.limit;
     uint32_t* og = (uint32_t*)scratch((uint64_t)K * 4);
     uint64_t* oc = (uint64_t*)scratch(8);
-    // live groups (order-preserving), their ORDER BY images from the states,
-    // a warp top-K over the images, the winners mapped back to group ids
-    uint32_t* gidx = (uint32_t*)scratch(cap * 4);
-    uint64_t* gcnt = (uint64_t*)scratch(8);
-    compact_step(flag ? (const void*)flag : (const void*)state, cap, n_dev, gidx, gcnt, state != nullptr);
-    SortItem* keys = (SortItem*)scratch(cap * sizeof(SortItem));
-    uint32_t* kidx = (uint32_t*)scratch(cap * 4);
-    Step e;
-    e.k = Step::ENCODE_STATES;
-    e.tfs = ts;
-    e.idx = gidx;
-    e.count = gcnt;
-    e.n_max = cap;
-    e.keys = keys;
-    e.kidx = kidx;
-    P.steps.push_back(e);
-    P.kernels += 1;
+    // one fused top-K straight over the live groups' states (each warp
+    // gathers live groups, keys them and keeps a warp list), then one
+    // merge pass; the winners come out as group ids
     Step t;
-    t.k = Step::TOPK;
-    t.keys = keys;
-    t.kidx = kidx;
-    t.count = gcnt;
-    t.n_max = cap;
+    t.k = Step::TOPK_FINAL;
+    t.tfs = ts;
     t.topk = K;
     t.out_idx = og;
     t.out_count = oc;
-    t.remap = gidx;
-    t.temp = scratch(topk_temp_bytes(cap, K));
+    t.temp = scratch(topk_final_temp_bytes(cap, K));
     P.steps.push_back(t);
     P.kernels += 2;
     std::vector<FinalOut> vis;

@@ -587,63 +587,91 @@ __device__ __forceinline__ bool u256_gt(const U256& a, const Cand& b) {
   return false;
 }
 
-template <int THREADS, int U>
+template <int THREADS, int R>
 __global__ void __launch_bounds__(THREADS) k_topk_final(const __grid_constant__ TopkFinalSpec spec, int K,
                                                         SortItem* __restrict__ out_keys,
                                                         uint32_t* __restrict__ out_idx) {
   constexpr int WARPS = THREADS / 32;
   __shared__ Cand s_l[WARPS][32];
+  __shared__ uint32_t s_live[WARPS][32 * R + 32];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint32_t lt = (1u << lane) - 1u;
   const uint64_t n = spec.n_dev ? (*spec.n_dev < spec.n_max ? *spec.n_dev : spec.n_max) : spec.n_max;
   const uint64_t per = (n + gridDim.x - 1) / gridDim.x;
   const uint64_t lo = (uint64_t)blockIdx.x * per;
   const uint64_t hi = lo + per < n ? lo + per : n;
+  uint32_t* const wb = s_live[warp];
   Cand L = cand_inf();
-  for (uint64_t base = lo + (uint64_t)warp * 32 * U; base < hi; base += (uint64_t)THREADS * U) {
-    bool v[U];
-    uint64_t g[U];
+  // Offers the live groups wb[0 .. m): the first ORDER BY part alone drops
+  // most of them; the others get their full key.
+  auto process = [&](uint32_t m) {
+    const bool in = (uint32_t)lane < m;
+    const uint64_t g = in ? wb[lane] : 0;
+    bool v = in;
+    const Cand thr = cand_shfl(L, K - 1);
+    U256 k{{0, 0, 0, 0}};
+    if (v) {
+      uint64_t vlo, vhi;
+      final_value(spec.part[0], g, vlo, vhi);
+      key_part(k, spec.ptype[0], spec.desc[0] != 0, vlo, vhi);
+      U256 probe = k;
+      shl_or(probe, spec.total_bits - spec.bits0, 0, 0);
+      if (u256_gt(probe, thr)) v = false;
+    }
+    Cand c = cand_inf();
+    if (v) {
+      for (int p = 1; p < spec.n_parts; ++p) {
+        uint64_t vlo, vhi;
+        final_value(spec.part[p], g, vlo, vhi);
+        key_part(k, spec.ptype[p], spec.desc[p] != 0, vlo, vhi);
+      }
+      c.w[0] = k.w[0]; c.w[1] = k.w[1]; c.w[2] = k.w[2]; c.w[3] = k.w[3];
+      c.ix = (uint32_t)g;
+    }
+    warp_offer_batch(L, c, v, K, lane);
+  };
+  // Each warp walks its part of the range R groups per lane at a time,
+  // gathers the live ones in wb (ballots, no divergence later) and offers
+  // them 32 at a time.
+  uint32_t cnt = 0;
+  for (uint64_t base = lo + (uint64_t)warp * 32 * R; base < hi; base += (uint64_t)THREADS * R) {
+    bool live[R];
 #pragma unroll
-    for (int u = 0; u < U; ++u) {
-      g[u] = base + (uint64_t)u * 32 + lane;
-      v[u] = g[u] < hi;
+    for (int r = 0; r < R; ++r) {
+      const uint64_t g = base + (uint64_t)r * 32 + lane;
+      live[r] = g < hi;
     }
     if (spec.flag) {
 #pragma unroll
-      for (int u = 0; u < U; ++u) v[u] = v[u] && spec.flag[g[u]] != 0;
+      for (int r = 0; r < R; ++r) live[r] = live[r] && spec.flag[base + (uint64_t)r * 32 + lane] != 0;
     }
     if (spec.state) {
 #pragma unroll
-      for (int u = 0; u < U; ++u) v[u] = v[u] && spec.state[g[u]] == 2u;
-    }
-    const Cand thr = cand_shfl(L, K - 1);
-    U256 k[U];
-#pragma unroll
-    for (int u = 0; u < U; ++u) {
-      k[u] = U256{{0, 0, 0, 0}};
-      if (v[u]) {
-        uint64_t vlo, vhi;
-        final_value(spec.part[0], g[u], vlo, vhi);
-        key_part(k[u], spec.ptype[0], spec.desc[0] != 0, vlo, vhi);
-        U256 probe = k[u];
-        shl_or(probe, spec.total_bits - spec.bits0, 0, 0);
-        if (u256_gt(probe, thr)) v[u] = false;
-      }
+      for (int r = 0; r < R; ++r) live[r] = live[r] && spec.state[base + (uint64_t)r * 32 + lane] == 2u;
     }
 #pragma unroll
-    for (int u = 0; u < U; ++u) {
-      Cand c = cand_inf();
-      if (v[u]) {
-        for (int p = 1; p < spec.n_parts; ++p) {
-          uint64_t vlo, vhi;
-          final_value(spec.part[p], g[u], vlo, vhi);
-          key_part(k[u], spec.ptype[p], spec.desc[p] != 0, vlo, vhi);
-        }
-        c.w[0] = k[u].w[0]; c.w[1] = k[u].w[1]; c.w[2] = k[u].w[2]; c.w[3] = k[u].w[3];
-        c.ix = (uint32_t)g[u];
-      }
-      warp_offer_batch(L, c, v[u], K, lane);
+    for (int r = 0; r < R; ++r) {
+      const uint32_t m = __ballot_sync(0xFFFFFFFFu, live[r]);
+      if (live[r]) wb[cnt + __popc(m & lt)] = (uint32_t)(base + (uint64_t)r * 32 + lane);
+      cnt += __popc(m);
+    }
+    __syncwarp();
+    while (cnt >= 32) {
+      process(32);
+      __syncwarp();
+      const uint32_t rest = cnt - 32;
+      uint32_t x[R + 1];
+#pragma unroll
+      for (int q = 0; q <= R; ++q) x[q] = (uint32_t)(q * 32 + lane) < rest ? wb[32 + q * 32 + lane] : 0u;
+      __syncwarp();
+#pragma unroll
+      for (int q = 0; q <= R; ++q)
+        if ((uint32_t)(q * 32 + lane) < rest) wb[q * 32 + lane] = x[q];
+      cnt = rest;
+      __syncwarp();
     }
   }
+  if (cnt) process(cnt);
   block_merge_lists<WARPS>(L, s_l, warp, lane);
   if (warp == 0) {
     if (lane < K) {
@@ -655,8 +683,8 @@ __global__ void __launch_bounds__(THREADS) k_topk_final(const __grid_constant__ 
   }
 }
 
-constexpr int kTfThreads = 512;  // first pass
-constexpr int kTfItems = 2;      // groups per lane per step
+constexpr int kTfThreads = 256;  // first pass
+constexpr int kTfItems = 4;      // groups per lane per step
 static unsigned topk_final_ctas(uint64_t n_max) {
   static int per_sm = 0;
   if (!per_sm) {
