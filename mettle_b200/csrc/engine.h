@@ -184,7 +184,7 @@ class Arena {
 
 // ------------------------------------------------------------ program
 struct Step {
-  enum Kind { MEMSET, FILL, PIPELINE, COMPACT_FLAGS, COMPACT_READY, FINALIZE, ENCODE, RADIX, TOPK, TOPK_FINAL, ENCODE_STATES, GATHER } k;
+  enum Kind { MEMSET, FILL, PIPELINE, COMPACT_FLAGS, COMPACT_READY, FINALIZE, ENCODE, RADIX, TOPK, TOPK_FINAL, GATHER } k;
   std::string name;  // for per-step profiles, e.g. "pipeline:agg_slot:lineitem"
   // MEMSET / FILL (u64 words)
   void* ptr = nullptr;
@@ -220,7 +220,7 @@ struct Step {
   const void* gin = nullptr;
   int width = 0;
   void* gout = nullptr;
-  // TOPK_FINAL / ENCODE_STATES
+  // TOPK_FINAL
   TopkFinalSpec tfs;
   const uint32_t* remap = nullptr;  // TOPK: write remap[i] for winner i
 };

@@ -1673,7 +1673,6 @@ static const char* step_kind_name(Step::Kind k) {
     case Step::RADIX: return "radix_sort";
     case Step::TOPK: return "topk";
     case Step::TOPK_FINAL: return "topk_states";
-    case Step::ENCODE_STATES: return "encode_states";
     case Step::GATHER: return "gather";
   }
   return "step";
@@ -1713,9 +1712,6 @@ void run_program(Ctx& ctx, Program& p, cudaStream_t s) {
       case Step::TOPK:
         CK(launch_topk(st.keys, st.kidx, st.count, st.n_max, st.topk, st.out_idx, st.out_count, st.temp, p.status,
                        s, st.remap));
-        break;
-      case Step::ENCODE_STATES:
-        CK(launch_encode_states(st.tfs, st.idx, st.count, st.n_max, st.keys, st.kidx, s));
         break;
       case Step::TOPK_FINAL: CK(launch_topk_final(st.tfs, st.topk, st.out_idx, st.out_count, st.temp, s)); break;
       case Step::GATHER: CK(launch_gather_width(st.gin, st.width, st.idx, st.count, st.n_max, st.gout, s)); break;

@@ -57,82 +57,6 @@ __global__ void k_encode(const __grid_constant__ SortKeySpec spec, const uint64_
   }
 }
 
-// ORDER BY images of aggregate groups straight from their states: for
-// i < *count, group g = gidx[i]; each part is a FinalOut evaluated at g.
-__global__ void k_encode_states(const __grid_constant__ TopkFinalSpec spec, const uint32_t* __restrict__ gidx,
-                                const uint64_t* count, uint64_t n_max, SortItem* __restrict__ keys,
-                                uint32_t* __restrict__ idx) {
-  const uint64_t n = count ? (*count < n_max ? *count : n_max) : n_max;
-  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
-    const uint64_t g = gidx ? gidx[i] : i;
-    U256 k{{0, 0, 0, 0}};
-    for (int p = 0; p < spec.n_parts; ++p) {
-      uint64_t lo, hi;
-      final_value(spec.part[p], g, lo, hi);
-      key_part(k, spec.ptype[p], spec.desc[p] != 0, lo, hi);
-    }
-    SortItem it;
-    it.w[0] = k.w[0]; it.w[1] = k.w[1]; it.w[2] = k.w[2]; it.w[3] = k.w[3];
-    keys[i] = it;
-    idx[i] = (uint32_t)i;
-  }
-}
-
-// ORDER BY images of the live groups (flag byte nonzero, or table state
-// READY) straight from their states, in any order: a warp-aggregated cursor
-// places them, and idx holds the group id itself, so ties still go to the
-// lower group id as with an order-preserving compaction.
-__global__ void k_encode_live(const __grid_constant__ TopkFinalSpec spec, SortItem* __restrict__ keys,
-                              uint32_t* __restrict__ idx, unsigned long long* __restrict__ count) {
-  const uint64_t n = spec.n_dev ? (*spec.n_dev < spec.n_max ? *spec.n_dev : spec.n_max) : spec.n_max;
-  const int lane = threadIdx.x & 31;
-  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-  for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x; base < n; base += stride) {
-    const uint64_t g = base + threadIdx.x;
-    bool live = g < n;
-    if (live && spec.flag) live = spec.flag[g] != 0;
-    if (live && spec.state) live = spec.state[g] == 2u;
-    const uint32_t m = __ballot_sync(0xFFFFFFFFu, live);
-    if (!m) continue;
-    unsigned long long pos = 0;
-    if (lane == 0) pos = atomicAdd(count, (unsigned long long)__popc(m));
-    pos = __shfl_sync(0xFFFFFFFFu, pos, 0) + __popc(m & ((1u << lane) - 1u));
-    if (!live) continue;
-    U256 k{{0, 0, 0, 0}};
-    for (int p = 0; p < spec.n_parts; ++p) {
-      uint64_t lo, hi;
-      final_value(spec.part[p], g, lo, hi);
-      key_part(k, spec.ptype[p], spec.desc[p] != 0, lo, hi);
-    }
-    SortItem it;
-    it.w[0] = k.w[0]; it.w[1] = k.w[1]; it.w[2] = k.w[2]; it.w[3] = k.w[3];
-    keys[pos] = it;
-    idx[pos] = (uint32_t)g;
-  }
-}
-
-cudaError_t launch_encode_live(const TopkFinalSpec& spec, SortItem* keys, uint32_t* idx, uint64_t* count,
-                               cudaStream_t s) {
-  if (spec.n_parts <= 0 || spec.n_parts > kMaxOrder) return cudaErrorInvalidValue;
-  uint64_t b = (spec.n_max + 255) / 256;
-  uint64_t cap = (uint64_t)sms() * 8;
-  if (b > cap) b = cap;
-  if (!b) b = 1;
-  k_encode_live<<<(unsigned)b, 256, 0, s>>>(spec, keys, idx, (unsigned long long*)count);
-  return cudaGetLastError();
-}
-
-cudaError_t launch_encode_states(const TopkFinalSpec& spec, const uint32_t* gidx, const uint64_t* count,
-                                 uint64_t n_max, SortItem* keys, uint32_t* idx, cudaStream_t s) {
-  if (spec.n_parts <= 0 || spec.n_parts > kMaxOrder) return cudaErrorInvalidValue;
-  uint64_t b = (n_max + 255) / 256;
-  uint64_t cap = (uint64_t)sms() * 8;
-  if (b > cap) b = cap;
-  if (!b) b = 1;
-  k_encode_states<<<(unsigned)b, 256, 0, s>>>(spec, gidx, count, n_max, keys, idx);
-  return cudaGetLastError();
-}
-
 cudaError_t launch_encode_keys(const SortKeySpec& spec, const uint64_t* count, uint64_t n_max, SortItem* keys,
                                uint32_t* idx, cudaStream_t s) {
   uint64_t b = (n_max + 255) / 256;

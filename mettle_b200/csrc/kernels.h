@@ -111,15 +111,6 @@ struct TopkFinalSpec {
   uint64_t n_max;
 };
 size_t topk_final_temp_bytes(uint64_t n_max, int k);
-// ORDER BY images of the live groups of spec (flag / state / n_dev as in
-// TopkFinalSpec), in any order, with idx = the group id; *count (zeroed by
-// the caller) gets their number.
-cudaError_t launch_encode_live(const TopkFinalSpec& spec, SortItem* keys, uint32_t* idx, uint64_t* count,
-                               cudaStream_t s);
-// ORDER BY images (and indices i) of the groups gidx[i], i < *count, from
-// their states, the parts as in TopkFinalSpec (flag/state/n_dev unused).
-cudaError_t launch_encode_states(const TopkFinalSpec& spec, const uint32_t* gidx, const uint64_t* count,
-                                 uint64_t n_max, SortItem* keys, uint32_t* idx, cudaStream_t s);
 cudaError_t launch_topk_final(const TopkFinalSpec& spec, int k, uint32_t* out_g, uint64_t* out_count, void* temp,
                               cudaStream_t s);
 
