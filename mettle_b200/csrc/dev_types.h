@@ -174,6 +174,8 @@ enum SinkKind : int32_t {
   SK_AGG_SMEM = 4,     // per-CTA shared-memory tables merged into AGG_HASH
   SK_AGG_SLOT = 5,     // dense states indexed by a build slot
   SK_AGG_SCALAR = 6,   // one group (no GROUP BY)
+  SK_PART_COUNT = 7,   // count the surviving rows per key partition, per CTA
+  SK_PART_SCATTER = 8, // write (key, values) records into their partitions
 };
 
 // Hash aggregate table (SoA). State word: 0 empty, 1 claimed, 2 ready.
@@ -248,6 +250,25 @@ struct PipeDesc {
   uint8_t* slot_hit;                // AGG_SLOT: 1 when the group saw a row
   int32_t smem_capacity;            // AGG_SMEM: slots per CTA table
   int32_t smem_probes;              // AGG_SMEM one-key tables: slots probed before the global table
+
+  // PART_COUNT / PART_SCATTER: the key's partition is the top part_bits of
+  // its hash; counts/offsets are [CTA][partition] (the grid is fixed to
+  // part_ctas CTAs so both launches give every CTA the same tiles); a
+  // record is part_words u64 words (1, 2 or 4): the key, then value slot v
+  // of each aggregate (part_val[a], -1 when it takes no value), zero padded.
+  int32_t part_bits;
+  int32_t part_words;
+  int32_t part_nvals;               // inputs per record (value slots in use)
+  int32_t part_combine;             // few keys per partition: combine a warp's records of one key
+  int32_t part_ctas;
+  uint32_t part_chunk;              // records per CTA of the per-partition aggregation
+  int32_t part_val[kMaxAggs];
+  int32_t part_src[kMaxAggs];       // aggregate whose program computes value slot v
+  uint32_t* part_counts;
+  uint32_t* part_offsets;           // per [CTA][partition], relative to part_start
+  uint32_t* part_start;             // first record of each partition (P + 1 entries)
+  uint32_t* part_chunk_start;       // first chunk of each partition (P + 1 entries)
+  uint64_t* part_records;
 
   uint32_t* status;                 // DevStatus bits
 };

@@ -184,7 +184,10 @@ class Arena {
 
 // ------------------------------------------------------------ program
 struct Step {
-  enum Kind { MEMSET, FILL, PIPELINE, COMPACT_FLAGS, COMPACT_READY, FINALIZE, ENCODE, RADIX, TOPK, TOPK_FINAL, GATHER } k;
+  enum Kind {
+    MEMSET, FILL, PIPELINE, COMPACT_FLAGS, COMPACT_READY, FINALIZE, ENCODE, RADIX, TOPK, TOPK_FINAL, GATHER,
+    PART_SCAN, PART_AGG  // partitioned aggregation (descriptor in `pipe`)
+  } k;
   std::string name;  // for per-step profiles, e.g. "pipeline:agg_slot:lineitem"
   // MEMSET / FILL (u64 words)
   void* ptr = nullptr;

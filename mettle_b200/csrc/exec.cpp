@@ -790,9 +790,10 @@ struct Compiler {
     PipeDesc& d = pb.d;
     std::vector<int> sink;
     if (d.sink == SK_BUILD) sink.push_back(d.build_key_col);
-    if (d.sink == SK_AGG_HASH || d.sink == SK_AGG_SMEM)
+    if (d.sink == SK_AGG_HASH || d.sink == SK_AGG_SMEM || d.sink == SK_PART_COUNT || d.sink == SK_PART_SCATTER)
       for (int k = 0; k < d.table.n_keys; ++k) prog_cols(d.progs[d.key_prog[k]], sink);
-    if (d.sink == SK_AGG_HASH || d.sink == SK_AGG_SMEM || d.sink == SK_AGG_SLOT || d.sink == SK_AGG_SCALAR)
+    if (d.sink == SK_AGG_HASH || d.sink == SK_AGG_SMEM || d.sink == SK_AGG_SLOT || d.sink == SK_AGG_SCALAR ||
+        d.sink == SK_PART_SCATTER)
       for (int a = 0; a < d.n_aggs; ++a)
         if (d.aggs[a].prog >= 0) prog_cols(d.progs[d.aggs[a].prog], sink);
     if (d.sink == SK_MATERIALIZE)
@@ -803,6 +804,9 @@ struct Compiler {
     d.n_stream = 0;
     if (d.tuple_input) return;
     uint32_t budget = 16;  // bytes per tuple: 64 KB of double-buffered tiles
+    // the scatter pass reads every input of the records: 80 KB still lets
+    // two of its CTAs share an SM
+    if (d.sink == SK_PART_SCATTER) budget = 20;
     if (d.sink == SK_AGG_SMEM) {
       // keep the CTA within about 110 KB so two fit on an SM: stream
       // buffers take 2 x 2048 bytes per streamed byte of a row
@@ -860,7 +864,8 @@ struct Compiler {
   }
 
   void push_pipeline(PipeBuilder& pb, uint64_t n_hint) {
-    static const char* sinks[] = {"none", "build", "materialize", "agg_hash", "agg_smem", "agg_slot", "agg_scalar"};
+    static const char* sinks[] = {"none",       "build",      "materialize", "agg_hash",    "agg_smem",
+                                  "agg_slot",   "agg_scalar", "part_count",  "part_scatter"};
     plan_columns(pb);
     Step s;
     s.k = Step::PIPELINE;
@@ -869,6 +874,92 @@ struct Compiler {
     s.name = std::string("pipeline:") + sinks[pb.d.sink] + ":" + plan.sources[pb.d.drive_src].name;
     P.steps.push_back(s);
     P.kernels += 1;
+  }
+
+  // Partitioned one-key aggregation, for all but a few groups: the rows'
+  // keys and aggregate inputs are written out grouped by key partition (a
+  // count pass, a scan and a scatter pass over the same pipeline), then
+  // CTAs aggregate one partition's chunk each in shared memory and merge
+  // their groups into the global table, so rows update shared memory
+  // instead of contending for global atomics, and each CTA's table holds
+  // one partition's keys only. Returns false (nothing queued) when the
+  // aggregate does not
+  // qualify: few groups, a 128-bit input, more distinct inputs than a record
+  // holds, more partitions than the count pass supports, or records that do
+  // not fit the scratch region. On success pb.d.sink is SK_PART_COUNT.
+  bool push_partitioned(PipeBuilder& pb, uint64_t est, uint64_t rows) {
+    if (est <= 8 || rows == 0 || rows >= (1ull << 31)) return false;
+    PipeDesc d = pb.d;
+    int nv = 0;
+    int slot_prog[kMaxAggs];
+    for (int a = 0; a < d.n_aggs; ++a) {
+      d.part_val[a] = -1;
+      const int pi = d.aggs[a].prog;
+      if (pi < 0) continue;
+      if (d.progs[pi].out_type == P_I128) return false;
+      int f = -1;
+      for (int j = 0; j < nv && f < 0; ++j)
+        if (memcmp(&d.progs[slot_prog[j]], &d.progs[pi], sizeof(VmProg)) == 0) f = j;
+      if (f < 0) {
+        if (nv == part_max_values()) return false;
+        f = nv++;
+        slot_prog[f] = pi;
+        d.part_src[f] = a;
+      }
+      d.part_val[a] = f;
+    }
+    // the partition CTA's table: up to 2048 entries within about 100 KB, so
+    // two CTAs share an SM
+    d.smem_capacity = 1;
+    const uint64_t entry = part_agg_smem_bytes(d);
+    const uint64_t cap = std::min<uint64_t>(2048, (100 * 1024) / entry);
+    if (cap < 256) return false;
+    // partitions: on average at most half a table of groups each
+    int bits = 1;
+    while ((cap / 2) << bits < est) ++bits;
+    if (bits > part_max_bits()) return false;
+    const uint64_t np = 1ull << bits;
+    const uint64_t words = nv == 0 ? 1 : nv == 1 ? 2 : 4;  // 16-byte aligned records
+    const uint64_t rec_bytes = rows * words * 8;
+    if (rec_bytes + (64ull << 20) > ctx.arena.largest_free()) return false;
+    const int ctas = pipeline_part_ctas();
+    d.part_bits = bits;
+    d.part_words = (int32_t)words;
+    d.part_nvals = nv;
+    d.part_combine = est / np < 128 ? 1 : 0;
+    d.part_ctas = ctas;
+    d.smem_capacity = (int32_t)cap;
+    d.smem_probes = 0;
+    // records per CTA: half a partition's average, but small enough for
+    // eight CTAs per SM, and at least 4096
+    const uint64_t min_ctas = 4ull * (uint64_t)pipeline_part_ctas();
+    d.part_chunk = (uint32_t)std::max<uint64_t>(
+        4096, std::min<uint64_t>((rows + 2 * np - 1) / (2 * np), (rows + min_ctas - 1) / min_ctas));
+    d.part_records = (uint64_t*)scratch(rec_bytes);
+    d.part_counts = (uint32_t*)scratch((uint64_t)ctas * np * 4);
+    d.part_offsets = (uint32_t*)scratch((uint64_t)ctas * np * 4);
+    d.part_start = (uint32_t*)scratch((np + 1) * 4);
+    d.part_chunk_start = (uint32_t*)scratch((np + 1) * 4);
+    pb.d = d;
+    PipeBuilder scatter = pb;
+    pb.d.sink = SK_PART_COUNT;
+    push_pipeline(pb, rows);
+    Step sc;
+    sc.k = Step::PART_SCAN;
+    sc.pipe = d;
+    sc.name = "part_scan";
+    P.steps.push_back(sc);
+    P.kernels += 1;
+    scatter.d.sink = SK_PART_SCATTER;
+    push_pipeline(scatter, rows);
+    Step sa;
+    sa.k = Step::PART_AGG;
+    sa.pipe = d;
+    sa.name = "part_agg";
+    sa.n_hint = rows;
+    P.steps.push_back(sa);
+    P.kernels += 1;
+    return true;
   }
 
   // Aggregate state descriptors for the sink (shared with the rep build).
@@ -1384,7 +1475,9 @@ struct Compiler {
     // CTA's most frequent keys (the first to arrive), so a skewed key's rows
     // meet in shared memory instead of contending on one global entry.
     pb.d.sink = SK_AGG_HASH;
-    if (cas_table) {
+    if (cas_table && push_partitioned(pb, est_groups, root_rows)) {
+      // count, scan, scatter and per-partition aggregation are queued
+    } else if (cas_table) {
       pb.d.sink = SK_AGG_SMEM;
       const bool whole = est_groups <= 1536;
       pb.d.smem_capacity = whole ? (int)(est_groups * 3 / 2 + 64) : 1024;
@@ -1401,7 +1494,7 @@ struct Compiler {
         pb.d.smem_capacity = 0;
       }
     }
-    push_pipeline(pb, root_rows);
+    if (pb.d.sink != SK_PART_COUNT) push_pipeline(pb, root_rows);
     std::vector<FinalOut> fo;
     for (size_t i = 0; i < plan.outputs.size(); ++i) {
       const BOut& o = plan.outputs[i];
@@ -1674,6 +1767,8 @@ static const char* step_kind_name(Step::Kind k) {
     case Step::TOPK: return "topk";
     case Step::TOPK_FINAL: return "topk_states";
     case Step::GATHER: return "gather";
+    case Step::PART_SCAN: return "part_scan";
+    case Step::PART_AGG: return "part_agg";
   }
   return "step";
 }
@@ -1715,6 +1810,8 @@ void run_program(Ctx& ctx, Program& p, cudaStream_t s) {
         break;
       case Step::TOPK_FINAL: CK(launch_topk_final(st.tfs, st.topk, st.out_idx, st.out_count, st.temp, s)); break;
       case Step::GATHER: CK(launch_gather_width(st.gin, st.width, st.idx, st.count, st.n_max, st.gout, s)); break;
+      case Step::PART_SCAN: CK(launch_part_scan(st.pipe, s)); break;
+      case Step::PART_AGG: CK(launch_part_agg(st.pipe, st.n_hint, s)); break;
     }
     if (p.profile) CK(cudaEventRecord(p.prof_ev[2 * i + 1], s));
   }

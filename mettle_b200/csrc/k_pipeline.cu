@@ -335,10 +335,27 @@ __device__ __forceinline__ int smem_agg_find(const PipeDesc& d, SmemAgg& s, cons
   return -1;
 }
 
+// Aggregate inputs in one record of the partitioned aggregation: a record
+// is the key and up to three inputs, padded to 1, 2 or 4 words.
+constexpr int kPartMaxVals = 3;
+
+// Words between entries of a CTA's one-key shared-memory table: the entry's
+// words (key, states, high words of 128-bit sums) rounded up to an odd
+// count, so that the same state of 16 consecutive entries sits in 16
+// different bank pairs and a warp's updates to random groups rarely collide
+// on a bank (the global table's 32-byte rounding would put every entry's
+// state on the same few banks).
+__host__ __device__ inline uint32_t smem_cas_stride(const PipeDesc& d) {
+  uint32_t words = 1u + (uint32_t)d.n_aggs;
+  for (int a = 0; a < d.n_aggs; ++a) words += d.aggs[a].fn == A_SUM_I128;
+  return words | 1u;
+}
+
 // One-key shared-memory table of a CTA (AGG_SMEM with DAggTable::cas): the
-// same entry layout as the global table (word 0 the key, word 1 + a state
-// a, then the high words of 128-bit sums), keys claimed by CAS, states
-// started at their identities, updates by shared-memory reductions.
+// global table's word order within an entry (word 0 the key, word 1 + a
+// state a, then the high words of 128-bit sums) at the odd stride above,
+// keys claimed by CAS, states started at their identities, updates by
+// shared-memory reductions.
 struct SmemCas {
   uint64_t* e;
   uint32_t cap;
@@ -348,7 +365,7 @@ struct SmemCas {
 __device__ __forceinline__ void smem_cas_init(const PipeDesc& d, SmemCas& s, uint8_t* base) {
   s.e = (uint64_t*)base;
   s.cap = (uint32_t)d.smem_capacity;
-  s.stride = d.table.stride > 1 ? (uint32_t)d.table.stride : 1;
+  s.stride = smem_cas_stride(d);
   const uint32_t words = s.cap * s.stride;
   for (uint32_t i = threadIdx.x; i < words; i += blockDim.x) {
     const uint32_t w = i % s.stride;
@@ -369,9 +386,11 @@ __device__ __forceinline__ void smem_cas_init(const PipeDesc& d, SmemCas& s, uin
 
 // Entry of key in the table, probing at most `limit` slots; -1 when it is
 // not there and cannot be claimed (or the key is the empty sentinel).
-__device__ __forceinline__ int smem_cas_find(const SmemCas& s, uint64_t key, uint32_t limit) {
+// hshift drops the hash bits that the keys in the table share (their
+// partition), so that those keys still spread over the whole table.
+__device__ __forceinline__ int smem_cas_find(const SmemCas& s, uint64_t key, uint32_t limit, int hshift = 0) {
   if ((int64_t)key == kEmptyKey) return -1;
-  uint32_t idx = (uint32_t)hash_slot(key_hash1(key), (uint64_t)s.cap);
+  uint32_t idx = (uint32_t)hash_slot(key_hash1(key) << hshift, (uint64_t)s.cap);
   for (uint32_t probe = 0; probe < limit; ++probe) {
     uint64_t* kp = s.e + (size_t)idx * s.stride;
     const uint64_t k = *(volatile uint64_t*)kp;
@@ -386,31 +405,85 @@ __device__ __forceinline__ int smem_cas_find(const SmemCas& s, uint64_t key, uin
   return -1;
 }
 
+__device__ __forceinline__ int64_t lds_s64(uint32_t a) {
+  int64_t x;
+  asm volatile("ld.volatile.shared.s64 %0, [%1];" : "=l"(x) : "r"(a));
+  return x;
+}
+
+// Adds x to the 64-bit word at shared address a as two 32-bit atomics: the
+// low half's add returns the old value, from which the carry into the high
+// half follows, so the word ends as the exact 64-bit sum modulo 2^64 however
+// the adds interleave (each carry is counted by the add that wrapped).
+__device__ __forceinline__ void smem_add64_split(uint32_t a, uint64_t x) {
+  const uint32_t lo = (uint32_t)x;
+  uint32_t old;
+  asm volatile("atom.shared.add.u32 %0, [%1], %2;" : "=r"(old) : "r"(a), "r"(lo));
+  const uint32_t hi = (uint32_t)(x >> 32) + ((uint32_t)(old + lo) < old ? 1u : 0u);
+  if (hi) asm volatile("red.shared.add.u32 [%0], %1;" ::"r"(a + 4), "r"(hi));
+}
+
 // Applies one value to a state word in shared memory (address `a` in the
 // shared window), without waiting for the result where the op allows.
+// These asm statements carry no memory clobber: the table is read back as
+// plain memory only after a CTA barrier, and without the clobber the
+// compiler keeps the global loads of later rows in flight across updates.
+// COUNT and 64-bit SUM use 32-bit atomics; MIN and MAX read the state first
+// and update only when the value improves on it (a stale read only costs
+// an update that changes nothing).
 __device__ __forceinline__ void smem_apply(int32_t fn, uint32_t a, uint32_t a_hi, Val v, int32_t vt) {
   switch (fn) {
-    case A_COUNT: asm volatile("red.shared.add.u64 [%0], %1;" ::"r"(a), "l"(1ULL) : "memory"); break;
-    case A_SUM_I: asm volatile("red.shared.add.u64 [%0], %1;" ::"r"(a), "l"((uint64_t)v.lo) : "memory"); break;
+    case A_COUNT: smem_add64_split(a, 1ULL); break;
+    case A_SUM_I: smem_add64_split(a, (uint64_t)v.lo); break;
     case A_SUM_I128: {
       uint64_t old;
       const uint64_t add = (uint64_t)v.lo;
-      asm volatile("atom.shared.add.u64 %0, [%1], %2;" : "=l"(old) : "r"(a), "l"(add) : "memory");
+      asm volatile("atom.shared.add.u64 %0, [%1], %2;" : "=l"(old) : "r"(a), "l"(add));
       const int64_t hadd = (vt == P_I128 ? v.hi : (v.lo >> 63)) + ((old + add) < old ? 1 : 0);
-      if (hadd) asm volatile("red.shared.add.u64 [%0], %1;" ::"r"(a_hi), "l"((uint64_t)hadd) : "memory");
+      if (hadd) asm volatile("red.shared.add.u64 [%0], %1;" ::"r"(a_hi), "l"((uint64_t)hadd));
       break;
     }
     case A_SUM_F:
-      asm volatile("red.shared.add.f64 [%0], %1;" ::"r"(a), "d"(val_as_f64(v, vt)) : "memory");
+      asm volatile("red.shared.add.f64 [%0], %1;" ::"r"(a), "d"(val_as_f64(v, vt)));
       break;
-    case A_MIN_I: asm volatile("red.shared.min.s64 [%0], %1;" ::"r"(a), "l"(v.lo) : "memory"); break;
-    case A_MAX_I: asm volatile("red.shared.max.s64 [%0], %1;" ::"r"(a), "l"(v.lo) : "memory"); break;
-    case A_MIN_F:
-      asm volatile("red.shared.min.u64 [%0], %1;" ::"r"(a), "l"(ord_f64(val_as_f64(v, vt))) : "memory");
+    case A_MIN_I:
+      if ((int64_t)v.lo < lds_s64(a)) asm volatile("red.shared.min.s64 [%0], %1;" ::"r"(a), "l"(v.lo));
       break;
-    case A_MAX_F:
-      asm volatile("red.shared.max.u64 [%0], %1;" ::"r"(a), "l"(ord_f64(val_as_f64(v, vt))) : "memory");
+    case A_MAX_I:
+      if ((int64_t)v.lo > lds_s64(a)) asm volatile("red.shared.max.s64 [%0], %1;" ::"r"(a), "l"(v.lo));
       break;
+    case A_MIN_F: {
+      const uint64_t u = ord_f64(val_as_f64(v, vt));
+      if (u < (uint64_t)lds_s64(a)) asm volatile("red.shared.min.u64 [%0], %1;" ::"r"(a), "l"(u));
+      break;
+    }
+    case A_MAX_F: {
+      const uint64_t u = ord_f64(val_as_f64(v, vt));
+      if (u > (uint64_t)lds_s64(a)) asm volatile("red.shared.max.u64 [%0], %1;" ::"r"(a), "l"(u));
+      break;
+    }
+    default: break;
+  }
+}
+
+// Calls f(FnC<fn>{}) with the aggregate function as a compile-time constant,
+// so that a loop over rows inside f is compiled once per function.
+template <int N>
+struct FnC {
+  static constexpr int value = N;
+};
+
+template <class F>
+__device__ __forceinline__ void dispatch_fn(int32_t fn, F& f) {
+  switch (fn) {
+    case A_COUNT: f(FnC<A_COUNT>{}); break;
+    case A_SUM_I: f(FnC<A_SUM_I>{}); break;
+    case A_SUM_I128: f(FnC<A_SUM_I128>{}); break;
+    case A_SUM_F: f(FnC<A_SUM_F>{}); break;
+    case A_MIN_I: f(FnC<A_MIN_I>{}); break;
+    case A_MAX_I: f(FnC<A_MAX_I>{}); break;
+    case A_MIN_F: f(FnC<A_MIN_F>{}); break;
+    case A_MAX_F: f(FnC<A_MAX_F>{}); break;
     default: break;
   }
 }
@@ -755,11 +828,9 @@ constexpr int kTileFetch = 1;  // warp-tiles taken per fetch of the dynamic tile
 // Bytes of the CTA-wide shared-memory sink area (the AGG_SMEM table),
 // rounded to 128.
 __host__ __device__ inline uint32_t sink_area_bytes(const PipeDesc& d) {
+  if (d.sink == SK_PART_COUNT || d.sink == SK_PART_SCATTER) return ((4u << d.part_bits) + 127) & ~127u;
   if (d.sink != SK_AGG_SMEM) return 0;
-  if (d.table.cas) {
-    const uint32_t stride = d.table.stride > 1 ? (uint32_t)d.table.stride : 1;
-    return ((uint32_t)d.smem_capacity * stride * 8 + 127) & ~127u;
-  }
+  if (d.table.cas) return ((uint32_t)d.smem_capacity * smem_cas_stride(d) * 8 + 127) & ~127u;
   uint32_t n128 = 0;
   for (int a = 0; a < d.n_aggs; ++a) n128 += d.aggs[a].fn == A_SUM_I128;
   const uint32_t b = (uint32_t)d.smem_capacity * (4 + 8 * (uint32_t)d.table.n_keys + 8 * (uint32_t)d.n_aggs + 8 * n128);
@@ -858,6 +929,13 @@ __global__ void __launch_bounds__(kThreads, (SINK == SK_AGG_SCALAR || SINK == SK
   if (SINK == SK_AGG_SMEM) {
     if (d.table.cas) smem_cas_init(d, scas, smem);
     else smem_agg_init(d, sagg, smem);
+  }
+  // key partitions: per-CTA counters, or this CTA's write cursors
+  if (SINK == SK_PART_COUNT || SINK == SK_PART_SCATTER) {
+    uint32_t* const s_part = (uint32_t*)smem;
+    const uint32_t np = 1u << d.part_bits;
+    for (uint32_t p = tid; p < np; p += kThreads)
+      s_part[p] = SINK == SK_PART_COUNT ? 0u : d.part_start[p] + d.part_offsets[(size_t)blockIdx.x * np + p];
   }
   uint64_t plo[SINK == SK_AGG_SCALAR ? kMaxAggs : 1];
   int64_t phi[SINK == SK_AGG_SCALAR ? kMaxAggs : 1];
@@ -1212,6 +1290,36 @@ __global__ void __launch_bounds__(kThreads, (SINK == SK_AGG_SCALAR || SINK == SK
         if ((d.out_rid_mask >> s) & 1u)
           for (uint32_t p = lane; p < lim; p += 32)
             d.out_rids[s][base + p] = tc_rid(tc, s, ident ? p : (uint32_t)sel_in[p]);
+    } else if (SINK == SK_PART_COUNT || SINK == SK_PART_SCATTER) {
+      // The key's partition is the top part_bits of its hash.
+      uint32_t* const s_part = (uint32_t*)smem;
+      const VmProg& kp = d.progs[d.key_prog[0]];
+      const int shift = 64 - d.part_bits;
+      const int nv = d.part_nvals;
+      for (uint32_t i = lane; i < n_sel; i += 32) {
+        const uint32_t r = ident ? i : (uint32_t)sel_in[i];
+        const uint64_t key = (uint64_t)vm_eval_t(kp, tc, r, st).lo;
+        const uint32_t p = (uint32_t)(key_hash1(key) >> shift);
+        if (SINK == SK_PART_COUNT) {
+          atomicAdd(&s_part[p], 1u);
+        } else {
+          // 1, 2 or 4 words: the key, then the inputs (zero padded), written
+          // with 16-byte stores
+          uint64_t wv[kPartMaxVals + 1];
+          wv[0] = key;
+#pragma unroll
+          for (int v = 0; v < kPartMaxVals; ++v)
+            wv[1 + v] = v < nv ? (uint64_t)vm_eval_t(d.progs[d.aggs[d.part_src[v]].prog], tc, r, st).lo : 0;
+          const uint32_t pos = atomicAdd(&s_part[p], 1u);
+          uint64_t* const rec = d.part_records + (uint64_t)pos * (uint64_t)d.part_words;
+          if (d.part_words == 1) {
+            rec[0] = key;
+          } else {
+            *(ulonglong2*)rec = make_ulonglong2(wv[0], wv[1]);
+            if (d.part_words == 4) *(ulonglong2*)(rec + 2) = make_ulonglong2(wv[2], wv[3]);
+          }
+        }
+      }
     } else if (SINK == SK_BUILD) {
       const DBuild& bd = d.builds[d.sink_build];
       // One slot reservation per warp-tile: its surviving rows take
@@ -1405,7 +1513,12 @@ __global__ void __launch_bounds__(kThreads, (SINK == SK_AGG_SCALAR || SINK == SK
   }
 
   // End-of-kernel work.
-  if (SINK == SK_MATERIALIZE) {
+  if (SINK == SK_PART_COUNT) {
+    __syncthreads();
+    const uint32_t np = 1u << d.part_bits;
+    const uint32_t* const s_part = (const uint32_t*)smem;
+    for (uint32_t p = tid; p < np; p += kThreads) d.part_counts[(size_t)blockIdx.x * np + p] = s_part[p];
+  } else if (SINK == SK_MATERIALIZE) {
     __syncthreads();
     if (tid == 0) {
       if (n == 0 && blockIdx.x == 0) *d.out_count = 0;
@@ -1488,6 +1601,321 @@ __global__ void __launch_bounds__(kThreads, (SINK == SK_AGG_SCALAR || SINK == SK
   if (st) atomicOr(d.status, st);
 }
 
+// ------------------------------------------------- partitioned aggregation
+// A one-key aggregate over many groups runs in three passes instead of
+// updating a global table per row: the pipeline counts each CTA's surviving
+// rows per key partition (SK_PART_COUNT), k_part_scan turns the counts into
+// write positions, the pipeline writes each row's key and aggregate inputs
+// into its partition (SK_PART_SCATTER, the same tiles per CTA), and
+// k_part_agg aggregates one partition per CTA in a shared-memory table
+// before merging its groups into the global table. A partition is the top
+// part_bits of the key's hash, so a partition's groups also occupy one
+// contiguous stretch of the global table.
+
+// One CTA. counts and offsets are [CTA][partition]; offsets become each
+// CTA's first position within the partition, start[p] the partition's first
+// record (start[P] = all records), and chunk_start[p] the first of the
+// partition's ceil(records / chunk) chunks (chunk_start[P] = all chunks).
+constexpr int kScanThreads = 1024;
+constexpr int kMaxPartBits = 13;
+
+// Exclusive scan of s_vals[0, np) into out[0, np], out[np] = the total.
+__device__ void block_scan_excl(const uint32_t* s_vals, uint32_t np, uint32_t* out, uint32_t* s_warp) {
+  const uint32_t per = (np + kScanThreads - 1) / kScanThreads;
+  const uint32_t b = threadIdx.x * per;
+  uint32_t sum = 0;
+  for (uint32_t i = 0; i < per; ++i)
+    if (b + i < np) sum += s_vals[b + i];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t incl = sum;
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+    if (lane >= o) incl += y;
+  }
+  if (lane == 31) s_warp[warp] = incl;
+  __syncthreads();
+  if (warp == 0) {
+    uint32_t w = s_warp[lane];
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, w, o);
+      if (lane >= o) w += y;
+    }
+    s_warp[lane] = w;  // inclusive over warps
+  }
+  __syncthreads();
+  uint32_t run = (warp ? s_warp[warp - 1] : 0u) + incl - sum;
+  for (uint32_t i = 0; i < per; ++i)
+    if (b + i < np) {
+      out[b + i] = run;
+      run += s_vals[b + i];
+    }
+  if (threadIdx.x == 0) out[np] = s_warp[kScanThreads / 32 - 1];
+  __syncthreads();  // s_warp and s_vals may be reused
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_part_scan(const uint32_t* __restrict__ counts,
+                                                             uint32_t* __restrict__ offsets,
+                                                             uint32_t* __restrict__ start,
+                                                             uint32_t* __restrict__ chunk_start, int n_ctas,
+                                                             int part_bits, uint32_t chunk) {
+  __shared__ uint32_t s_tot[1 << kMaxPartBits];
+  __shared__ uint32_t s_warp[kScanThreads / 32];
+  const uint32_t np = 1u << part_bits;
+  for (uint32_t p = threadIdx.x; p < np; p += kScanThreads) {
+    uint32_t run = 0;
+#pragma unroll 8
+    for (int c = 0; c < n_ctas; ++c) {
+      const size_t i = (size_t)c * np + p;
+      const uint32_t v = counts[i];
+      offsets[i] = run;
+      run += v;
+    }
+    s_tot[p] = run;
+  }
+  __syncthreads();
+  block_scan_excl(s_tot, np, start, s_warp);
+  for (uint32_t p = threadIdx.x; p < np; p += kScanThreads) s_tot[p] = (s_tot[p] + chunk - 1) / chunk;
+  __syncthreads();
+  block_scan_excl(s_tot, np, chunk_start, s_warp);
+}
+
+// A row's value in its state's domain (COUNT 1, SUM_F a double's bits,
+// MIN_F/MAX_F the order-preserving image): the one-word states (all but
+// A_SUM_I128) combine these with state_combine and merge them once.
+__device__ __forceinline__ uint64_t lane_state_value(int32_t fn, Val v, int32_t vt) {
+  switch (fn) {
+    case A_COUNT: return 1;
+    case A_SUM_F: return (uint64_t)__double_as_longlong(val_as_f64(v, vt));
+    case A_MIN_F:
+    case A_MAX_F: return ord_f64(val_as_f64(v, vt));
+    default: return (uint64_t)v.lo;
+  }
+}
+
+__device__ __forceinline__ uint64_t state_combine(int32_t fn, uint64_t x, uint64_t y) {
+  switch (fn) {
+    case A_SUM_F:
+      return (uint64_t)__double_as_longlong(
+          __dadd_rn(__longlong_as_double((long long)x), __longlong_as_double((long long)y)));
+    case A_MIN_I: return (int64_t)y < (int64_t)x ? y : x;
+    case A_MAX_I: return (int64_t)y > (int64_t)x ? y : x;
+    case A_MIN_F: return y < x ? y : x;
+    case A_MAX_F: return y > x ? y : x;
+    default: return x + y;  // COUNT, SUM_I (mod 2^64)
+  }
+}
+
+// Combines x over each group of lanes that share a key (`peers`: the lanes
+// of this lane's group, this lane included; 0 for a lane outside every
+// group); the group's lowest lane ends with the group's total. Each round
+// every lane still collecting adds the value of the next higher lane of its
+// group that is still collecting, and the lanes at odd ranks within their
+// group drop out, so a group of n lanes takes ceil(log2 n) rounds.
+__device__ __forceinline__ uint64_t peer_combine(int32_t fn, unsigned peers, uint64_t x, uint32_t lane) {
+  unsigned rank = __popc(peers & ((1u << lane) - 1u));  // lanes of the group below this one
+  unsigned rest = peers & ~((2u << lane) - 1u);          // lanes of the group above this one
+  while (__any_sync(0xFFFFFFFFu, rest != 0)) {
+    const int next = __ffs(rest) - 1;
+    const uint64_t y = __shfl_sync(0xFFFFFFFFu, x, next < 0 ? (int)lane : next);
+    if (next >= 0) x = state_combine(fn, x, y);
+    const unsigned done = __ballot_sync(0xFFFFFFFFu, (rank & 1u) != 0);
+    rest &= ~done;
+    rank >>= 1;
+  }
+  return x;
+}
+
+// Merges a one-word partial state into a shared-memory state word.
+__device__ __forceinline__ void smem_merge(int32_t fn, uint32_t a, uint64_t x) {
+  switch (fn) {
+    case A_COUNT:
+    case A_SUM_I: smem_add64_split(a, x); break;
+    case A_SUM_F: asm volatile("red.shared.add.f64 [%0], %1;" ::"r"(a), "d"(__longlong_as_double((long long)x))); break;
+    case A_MIN_I:
+      if ((int64_t)x < lds_s64(a)) asm volatile("red.shared.min.s64 [%0], %1;" ::"r"(a), "l"(x));
+      break;
+    case A_MAX_I:
+      if ((int64_t)x > lds_s64(a)) asm volatile("red.shared.max.s64 [%0], %1;" ::"r"(a), "l"(x));
+      break;
+    case A_MIN_F:
+      if (x < (uint64_t)lds_s64(a)) asm volatile("red.shared.min.u64 [%0], %1;" ::"r"(a), "l"(x));
+      break;
+    case A_MAX_F:
+      if (x > (uint64_t)lds_s64(a)) asm volatile("red.shared.max.u64 [%0], %1;" ::"r"(a), "l"(x));
+      break;
+    default: break;
+  }
+}
+
+constexpr int kPartAggThreads = 512;
+constexpr int kPartBatch = 4;  // records per thread with loads in flight together
+
+// One CTA per chunk: a partition's records split into pieces of at most
+// d.part_chunk, so that a large partition (a skewed key's) is shared by
+// several CTAs while a CTA sees one partition's keys only. The records go
+// into a shared-memory table (the layout of SmemCas, capacity
+// d.smem_capacity); a record whose key finds no entry within kPartProbes
+// slots goes to the global table directly. Then every entry is merged into
+// the global table.
+constexpr uint32_t kPartProbes = 64;
+
+__global__ void __launch_bounds__(kPartAggThreads) k_part_agg(const __grid_constant__ PipeDesc d) {
+  extern __shared__ __align__(128) uint8_t smem[];
+  const uint32_t np = 1u << d.part_bits;
+  const uint32_t cb = blockIdx.x;
+  if (cb >= d.part_chunk_start[np]) return;  // the whole CTA leaves, before any barrier
+  // the chunk's partition: chunk_start[lo] <= cb < chunk_start[hi]
+  uint32_t lo = 0, hi = np;
+  while (hi - lo > 1) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (d.part_chunk_start[mid] <= cb) lo = mid;
+    else hi = mid;
+  }
+  const uint32_t pend = d.part_start[lo + 1];
+  const uint32_t psize = pend - d.part_start[lo];
+  const uint32_t rb = d.part_start[lo] + (cb - d.part_chunk_start[lo]) * d.part_chunk;
+  const uint32_t re = pend - rb < d.part_chunk ? pend : rb + d.part_chunk;
+  SmemCas s;
+  smem_cas_init(d, s, smem);
+  __syncthreads();
+  uint32_t st = 0;
+  const int W = d.part_words;
+  const int na = d.n_aggs;
+  const DAggTable& tb = d.table;
+  const uint64_t gstride = tb.stride > 1 ? (uint64_t)tb.stride : 1;
+  const uint32_t estride = s.stride * 8;
+  constexpr int B = kPartBatch;
+  const uint32_t lane = threadIdx.x & 31;
+  // Records of one key are combined within a warp before updating where a
+  // warp often holds several of them: in a partition over twice the average
+  // size (a skewed key's), or when partitions have few keys. Every state must
+  // be one word.
+  bool warp_ok = d.part_combine != 0 || psize > 2 * (d.part_start[np] >> d.part_bits) + 1024;
+  for (int a = 0; a < na; ++a) warp_ok &= d.aggs[a].fn != A_SUM_I128;
+  for (uint32_t i0 = rb; i0 < re; i0 += kPartAggThreads * B) {
+    uint64_t key[B];
+    uint64_t val[B][kPartMaxVals];
+    bool act[B];
+#pragma unroll
+    for (int q = 0; q < B; ++q) {
+      const uint32_t i = i0 + (uint32_t)q * kPartAggThreads + threadIdx.x;
+      act[q] = i < re;
+      const uint64_t* rec = d.part_records + (uint64_t)(act[q] ? i : rb) * (uint64_t)W;
+      key[q] = 0;
+#pragma unroll
+      for (int v = 0; v < kPartMaxVals; ++v) val[q][v] = 0;
+      if (act[q]) {
+        if (W == 1) {
+          key[q] = __ldcs(rec);
+        } else {
+          const ulonglong2 x = __ldcs((const ulonglong2*)rec);
+          key[q] = x.x;
+          val[q][0] = x.y;
+          if (W == 4) {
+            const ulonglong2 y = __ldcs((const ulonglong2*)rec + 1);
+            val[q][1] = y.x;
+            val[q][2] = y.y;
+          }
+        }
+      }
+    }
+    // Records of one key in the same warp (a skewed key's) are combined in
+    // registers first: only the lowest lane of each key's group updates.
+    bool upd[B];      // this lane's record updates an entry
+    bool comb[B];     // (warp-uniform) batch q combines records of a key first
+    unsigned peers[B];
+    bool any_comb = false;
+#pragma unroll
+    for (int q = 0; q < B; ++q) {
+      upd[q] = act[q];
+      comb[q] = false;
+      peers[q] = 0;
+      if (warp_ok) {
+        // every lane takes part in the warp votes (key[q] is 0 where the lane has no record)
+        const unsigned am = __ballot_sync(0xFFFFFFFFu, act[q]);
+        const unsigned same = __match_any_sync(0xFFFFFFFFu, key[q]);
+        peers[q] = act[q] ? (same & am) : 0u;
+        // combining pays for itself once some key holds four lanes
+        comb[q] = __any_sync(0xFFFFFFFFu, __popc(peers[q]) >= 4);
+        // when combining, only the lowest lane of each key's group updates
+        if (comb[q]) upd[q] = act[q] && (peers[q] & ((1u << lane) - 1u)) == 0;
+        any_comb |= comb[q];
+      }
+    }
+    // the updating records' entries: shared-memory index, else the global group
+    int idx[B];
+    uint64_t g[B];
+#pragma unroll
+    for (int q = 0; q < B; ++q) {
+      idx[q] = -1;
+      g[q] = kNoGroup;
+      if (upd[q]) {
+        idx[q] = smem_cas_find(s, key[q], kPartProbes, d.part_bits);
+        if (idx[q] < 0) g[q] = agg_find_cas(tb, key[q], hash_slot(key_hash1(key[q]), tb.capacity), st);
+      }
+    }
+    // one aggregate at a time over the batch, compiled per function
+    int hw = 0;
+    for (int a = 0; a < na; ++a) {
+      const DAgg& ag = d.aggs[a];
+      const int vs = d.part_val[a];
+      const int32_t vt = vs >= 0 ? d.progs[ag.prog].out_type : P_I64;
+      Val v[B];
+#pragma unroll
+      for (int q = 0; q < B; ++q) {
+        const uint64_t x = vs == 0 ? val[q][0] : vs == 1 ? val[q][1] : vs == 2 ? val[q][2] : 0;
+        v[q].lo = (int64_t)x;
+        v[q].hi = v[q].lo >> 63;
+      }
+      const uint32_t sa = smem_u32(s.e + 1 + a), sh = smem_u32(s.e + 1 + na + hw);
+      unsigned long long* const glo = (unsigned long long*)ag.lo;
+      long long* const ghi = (long long*)ag.hi;
+      if (any_comb) {
+        // warp_ok holds: every state is one word
+#pragma unroll
+        for (int q = 0; q < B; ++q) {
+          if (!comb[q]) continue;  // warp-uniform
+          const uint64_t x = peer_combine(ag.fn, peers[q], lane_state_value(ag.fn, v[q], vt), lane);
+          if (idx[q] >= 0) smem_merge(ag.fn, sa + (uint32_t)idx[q] * estride, x);
+          else if (g[q] != kNoGroup) agg_merge(ag.fn, glo + g[q] * gstride, nullptr, x, 0);
+        }
+      }
+      auto apply = [&](auto fnc) {
+        constexpr int FN = decltype(fnc)::value;
+#pragma unroll
+        for (int q = 0; q < B; ++q) {
+          if (comb[q]) continue;
+          if (idx[q] >= 0) {
+            const uint32_t eo = (uint32_t)idx[q] * estride;
+            smem_apply(FN, sa + eo, sh + eo, v[q], vt);
+          } else if (g[q] != kNoGroup) {
+            const uint64_t o = g[q] * gstride;
+            agg_apply_g(FN, glo + o, ghi ? ghi + o : nullptr, v[q], vt);
+          }
+        }
+      };
+      dispatch_fn(ag.fn, apply);
+      hw += ag.fn == A_SUM_I128;
+    }
+  }
+  __syncthreads();
+  for (uint32_t i = threadIdx.x; i < s.cap; i += kPartAggThreads) {
+    const uint64_t* ent = s.e + (size_t)i * s.stride;
+    const uint64_t key = ent[0];
+    if ((int64_t)key == kEmptyKey) continue;
+    const uint64_t gg = agg_find_cas(tb, key, hash_slot(key_hash1(key), tb.capacity), st);
+    if (gg == kNoGroup) continue;
+    const uint64_t o = gg * gstride;
+    int hw2 = 0;
+    for (int a = 0; a < na; ++a) {
+      const DAgg& ag = d.aggs[a];
+      const int64_t hv = ag.fn == A_SUM_I128 ? (int64_t)ent[1 + na + hw2++] : 0;
+      agg_merge(ag.fn, (unsigned long long*)(ag.lo + o), (long long*)(ag.hi ? ag.hi + o : nullptr), ent[1 + a], hv);
+    }
+  }
+  if (st) atomicOr(d.status, st);
+}
+
 // ------------------------------------------------------------ launch
 static int g_sm_count = 0;
 static int sm_count() {
@@ -1510,7 +1938,7 @@ size_t pipeline_smem_bytes(const PipeDesc& d) {
 // queries cost host time on every launch otherwise.
 static std::mutex g_occ_mu;
 static std::map<std::pair<int, size_t>, int> g_occ;
-static size_t g_smem_set[8];
+static size_t g_smem_set[9];
 
 template <int SINK>
 static cudaError_t launch_sink(const PipeDesc& d, uint64_t n_hint, cudaStream_t s) {
@@ -1543,7 +1971,45 @@ static cudaError_t launch_sink(const PipeDesc& d, uint64_t n_hint, cudaStream_t 
   uint64_t max_grid = (uint64_t)sm_count() * (uint64_t)blocks_per_sm;
   uint64_t grid = tiles < max_grid ? tiles : max_grid;
   if (grid == 0) grid = 1;
+  // both partition passes must give every CTA the same tiles
+  if (SINK == SK_PART_COUNT || SINK == SK_PART_SCATTER) grid = (uint64_t)d.part_ctas;
   kern<<<(unsigned)grid, kThreads, smem, s>>>(d);
+  return cudaGetLastError();
+}
+
+int part_max_bits() { return kMaxPartBits; }
+int part_max_values() { return kPartMaxVals; }
+
+// Both partition passes run this many CTAs (they must cover the same tiles):
+// two per SM, which the scatter pass's shared memory allows.
+int pipeline_part_ctas() { return 2 * sm_count(); }
+
+cudaError_t launch_part_scan(const PipeDesc& d, cudaStream_t s) {
+  if (d.part_bits < 1 || d.part_bits > kMaxPartBits) return cudaErrorInvalidValue;
+  if (d.part_chunk == 0) return cudaErrorInvalidValue;
+  k_part_scan<<<1, kScanThreads, 0, s>>>(d.part_counts, d.part_offsets, d.part_start, d.part_chunk_start, d.part_ctas,
+                                         d.part_bits, d.part_chunk);
+  return cudaGetLastError();
+}
+
+size_t part_agg_smem_bytes(const PipeDesc& d) { return (size_t)d.smem_capacity * smem_cas_stride(d) * 8; }
+
+cudaError_t launch_part_agg(const PipeDesc& d, uint64_t n_hint, cudaStream_t s) {
+  if (d.part_chunk == 0) return cudaErrorInvalidValue;
+  static std::mutex mu;
+  static size_t smem_set = 0;
+  const size_t smem = part_agg_smem_bytes(d);
+  {
+    std::lock_guard<std::mutex> g(mu);
+    if (smem > smem_set) {
+      cudaError_t e = cudaFuncSetAttribute(k_part_agg, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      if (e != cudaSuccess) return e;
+      smem_set = smem;
+    }
+  }
+  // at most records / chunk + one partial chunk per partition
+  const uint64_t grid = n_hint / d.part_chunk + (1ull << d.part_bits);
+  k_part_agg<<<(unsigned)grid, kPartAggThreads, smem, s>>>(d);
   return cudaGetLastError();
 }
 
@@ -1556,6 +2022,8 @@ cudaError_t launch_pipeline(const PipeDesc& d, uint64_t n_hint, cudaStream_t s) 
     case SK_AGG_SMEM: return launch_sink<SK_AGG_SMEM>(d, n_hint, s);
     case SK_AGG_SLOT: return launch_sink<SK_AGG_SLOT>(d, n_hint, s);
     case SK_AGG_SCALAR: return launch_sink<SK_AGG_SCALAR>(d, n_hint, s);
+    case SK_PART_COUNT: return launch_sink<SK_PART_COUNT>(d, n_hint, s);
+    case SK_PART_SCATTER: return launch_sink<SK_PART_SCATTER>(d, n_hint, s);
     default: return cudaErrorInvalidValue;
   }
 }

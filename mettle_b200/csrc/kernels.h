@@ -18,6 +18,18 @@ cudaError_t launch_pipeline(const PipeDesc& d, uint64_t n_hint, cudaStream_t s);
 // tiles of pipeline_tile_rows() rows (k_pipeline_cta.cu); launch_pipeline
 // dispatches to it.
 cudaError_t launch_pipeline_materialize(const PipeDesc& d, uint64_t n_hint, cudaStream_t s);
+// Partitioned one-key aggregation (k_pipeline.cu): the SK_PART_COUNT and
+// SK_PART_SCATTER pipelines run pipeline_part_ctas() CTAs; between them
+// launch_part_scan turns the per-CTA partition counts into write positions;
+// launch_part_agg then aggregates the records into d.table: one CTA per
+// chunk of at most d.part_chunk records of one partition, with a
+// shared-memory table of d.smem_capacity entries; n_hint bounds the records.
+int part_max_bits();
+int part_max_values();
+int pipeline_part_ctas();
+size_t part_agg_smem_bytes(const PipeDesc& d);
+cudaError_t launch_part_scan(const PipeDesc& d, cudaStream_t s);
+cudaError_t launch_part_agg(const PipeDesc& d, uint64_t n_hint, cudaStream_t s);
 
 // ---- aggregate finalize (k_misc.cu)
 // Order-preserving list of READY slots of a hash aggregate table.

@@ -156,6 +156,115 @@ def test_c3_all_groups_exact(conn):
     assert np.array_equal(r.columns[3], want["min_v"]) and np.array_equal(r.columns[4], want["max_v"])
 
 
+def _grouped(keys, cols):
+    """Per distinct key (ascending): COUNT and, per column, SUM / MIN / MAX / SUM(|x|)."""
+    o = np.argsort(keys, kind="stable")
+    ks = keys[o]
+    starts = np.flatnonzero(np.r_[True, ks[1:] != ks[:-1]])
+    out = {"k": ks[starts], "cnt": np.diff(np.r_[starts, len(ks)])}
+    for name, c in cols.items():
+        cs = c[o]
+        out[name + "_sum"] = np.add.reduceat(cs, starts)
+        out[name + "_min"] = np.minimum.reduceat(cs, starts)
+        out[name + "_max"] = np.maximum.reduceat(cs, starts)
+        out[name + "_abs"] = np.add.reduceat(np.abs(cs), starts)
+    return out
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("groups", [3000, 40_000])
+def test_group_by_many_groups_edge_keys(conn, groups):
+    """Group counts past the shared-memory table take the partitioned
+    aggregation; keys include the empty-slot sentinel (-1) and both int64
+    extremes, rows pass a filter, and a DOUBLE column feeds SUM/MIN/MAX."""
+    init(conn)
+    r = np.random.default_rng(groups)
+    n = 1_000_000
+    k = r.integers(-(groups // 2), groups // 2, n).astype(np.int64)
+    k[::97] = -1
+    k[::1009] = np.iinfo(np.int64).min
+    k[::1013] = np.iinfo(np.int64).max
+    v = r.integers(-10**12, 10**12, n).astype(np.int64)
+    x = r.standard_normal(n)
+    conn.create_table("t", {"k": (L.T_BIGINT, k), "v": (L.T_BIGINT, v), "x": (L.T_DOUBLE, x)})
+    conn.gpu_register_table("t")
+    res = conn.gpu_processing("SELECT k, COUNT(*), SUM(v), MIN(v), MAX(v), SUM(x), MIN(x), MAX(x) FROM t "
+                              "WHERE v > -500000000000 GROUP BY k ORDER BY k")
+    m = v > -500_000_000_000
+    want = _grouped(k[m], {"v": v[m], "x": x[m]})
+    rows = res.fetchall()
+    assert len(rows) == len(want["k"])
+    got = list(zip(*rows))
+    assert np.array_equal(np.array(got[0], np.int64), want["k"])
+    assert np.array_equal(np.array(got[1], np.int64), want["cnt"])
+    assert [int(s) for s in got[2]] == [int(s) for s in want["v_sum"]]
+    assert np.array_equal(np.array(got[3], np.int64), want["v_min"])
+    assert np.array_equal(np.array(got[4], np.int64), want["v_max"])
+    assert np.all(np.abs(np.array(got[5]) - want["x_sum"]) <= 1e-12 * want["x_abs"] + 1e-300)
+    assert np.array_equal(np.array(got[6]), want["x_min"]) and np.array_equal(np.array(got[7]), want["x_max"])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("groups,dist", [(12, "uniform"), (100, "uniform"), (20_000, "zipf"), (300_000, "zipf")])
+def test_group_by_repeated_keys_in_a_warp(conn, groups, dist):
+    """Few groups, or a skewed key, put several records of one key in the
+    same warp of the per-partition aggregation, which combines them before
+    updating; every group must still see every row."""
+    init(conn)
+    r = np.random.default_rng(groups)
+    n = 2_000_000
+    if dist == "zipf":
+        k = (r.zipf(1.1, n) % groups).astype(np.int64) * 104729 - 7
+    else:
+        k = r.integers(0, groups, n).astype(np.int64) * 104729 - 7
+    v = r.integers(-10**9, 10**9, n).astype(np.int64)
+    x = r.standard_normal(n)
+    conn.create_table("t", {"k": (L.T_BIGINT, k), "v": (L.T_BIGINT, v), "x": (L.T_DOUBLE, x)})
+    conn.gpu_register_table("t")
+    res = conn.gpu_processing("SELECT k, COUNT(*), SUM(v), MIN(v), MAX(v), SUM(x), MIN(x), MAX(x) FROM t "
+                              "GROUP BY k ORDER BY k")
+    want = _grouped(k, {"v": v, "x": x})
+    rows = res.fetchall()
+    assert len(rows) == len(want["k"])
+    got = list(zip(*rows))
+    assert np.array_equal(np.array(got[0], np.int64), want["k"])
+    assert np.array_equal(np.array(got[1], np.int64), want["cnt"])
+    assert [int(s) for s in got[2]] == [int(s) for s in want["v_sum"]]
+    assert np.array_equal(np.array(got[3], np.int64), want["v_min"])
+    assert np.array_equal(np.array(got[4], np.int64), want["v_max"])
+    assert np.all(np.abs(np.array(got[5]) - want["x_sum"]) <= 1e-12 * want["x_abs"] + 1e-300)
+    assert np.array_equal(np.array(got[6]), want["x_min"]) and np.array_equal(np.array(got[7]), want["x_max"])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("sql_aggs,cols", [
+    ("COUNT(*)", ()),                                          # records hold the key alone
+    ("COUNT(*), SUM(a)", "a"),                                 # key and one input
+    ("COUNT(*), SUM(a), SUM(b), SUM(c)", "abc"),               # key, three inputs
+    ("COUNT(*), SUM(a), SUM(b), SUM(c), SUM(d), SUM(e)", "abcde"),  # more inputs than a record holds
+])
+def test_group_by_many_groups_record_shapes(conn, sql_aggs, cols):
+    init(conn)
+    r = np.random.default_rng(7)
+    n = 600_000
+    k = r.integers(0, 50_000, n).astype(np.int64) * 7919
+    data = {"k": (L.T_BIGINT, k)}
+    vals = {c: r.integers(-1000, 1000, n).astype(np.int64) for c in "abcde"}
+    for c in "abcde":
+        data[c] = (L.T_BIGINT, vals[c])
+    conn.create_table("t", data)
+    conn.gpu_register_table("t")
+    res = conn.gpu_processing(f"SELECT k, {sql_aggs} FROM t GROUP BY k ORDER BY k")
+    want = _grouped(k, {c: vals[c] for c in cols})
+    rows = res.fetchall()
+    assert len(rows) == len(want["k"])
+    got = list(zip(*rows))
+    assert np.array_equal(np.array(got[0], np.int64), want["k"])
+    assert np.array_equal(np.array(got[1], np.int64), want["cnt"])
+    for i, c in enumerate(cols):
+        assert [int(s) for s in got[2 + i]] == [int(s) for s in want[c + "_sum"]]
+
+
 # ------------------------------------------------------------------ config 4
 def q3_check(conn, t, limit=10):
     r = conn.gpu_processing(W.q3_sql(t.date, limit=limit))
