@@ -874,7 +874,7 @@ struct FusedOpen {
 // warps of the CTA inside the tile loop: a slow tile (a long sink chain, a
 // look-back) stalls only its warp while the others keep the SM busy.
 template <int SINK>
-__global__ void __launch_bounds__(kThreads, (SINK == SK_AGG_SCALAR || SINK == SK_AGG_SMEM) ? 2 : 3)
+__global__ void __launch_bounds__(kThreads, (SINK == SK_AGG_SCALAR || SINK == SK_AGG_SMEM || SINK == SK_PART_SCATTER) ? 2 : 3)
     k_pipeline(const __grid_constant__ PipeDesc d) {
   constexpr int TILE = kTile;
   extern __shared__ __align__(128) uint8_t smem[];
@@ -1291,33 +1291,64 @@ __global__ void __launch_bounds__(kThreads, (SINK == SK_AGG_SCALAR || SINK == SK
           for (uint32_t p = lane; p < lim; p += 32)
             d.out_rids[s][base + p] = tc_rid(tc, s, ident ? p : (uint32_t)sel_in[p]);
     } else if (SINK == SK_PART_COUNT || SINK == SK_PART_SCATTER) {
-      // The key's partition is the top part_bits of its hash.
+      // The key's partition is the top part_bits of its hash. With few
+      // partitions, a warp's rows of one partition reserve their positions
+      // with one shared-memory atomic (their leader's).
       uint32_t* const s_part = (uint32_t*)smem;
       const VmProg& kp = d.progs[d.key_prog[0]];
       const int shift = 64 - d.part_bits;
       const int nv = d.part_nvals;
-      for (uint32_t i = lane; i < n_sel; i += 32) {
-        const uint32_t r = ident ? i : (uint32_t)sel_in[i];
-        const uint64_t key = (uint64_t)vm_eval_t(kp, tc, r, st).lo;
-        const uint32_t p = (uint32_t)(key_hash1(key) >> shift);
-        if (SINK == SK_PART_COUNT) {
-          atomicAdd(&s_part[p], 1u);
-        } else {
-          // 1, 2 or 4 words: the key, then the inputs (zero padded), written
-          // with 16-byte stores
-          uint64_t wv[kPartMaxVals + 1];
-          wv[0] = key;
+      const bool grouped = d.part_bits <= 8;
+      auto plain = [](const VmProg& pg) {
+        return pg.fast.shape == 1 && pg.fast.leaf[0].op == VM_COL && !pg.fast.leaf_cast[0].on;
+      };
+      const bool kcol = plain(kp);
+      const ColAcc kca = col_acc(tc, kcol ? kp.fast.leaf[0].arg : 0);
+      const VmProg* vp[kPartMaxVals];
+      bool vcol[kPartMaxVals];
+      ColAcc vca[kPartMaxVals];
 #pragma unroll
-          for (int v = 0; v < kPartMaxVals; ++v)
-            wv[1 + v] = v < nv ? (uint64_t)vm_eval_t(d.progs[d.aggs[d.part_src[v]].prog], tc, r, st).lo : 0;
-          const uint32_t pos = atomicAdd(&s_part[p], 1u);
-          uint64_t* const rec = d.part_records + (uint64_t)pos * (uint64_t)d.part_words;
-          if (d.part_words == 1) {
-            rec[0] = key;
-          } else {
-            *(ulonglong2*)rec = make_ulonglong2(wv[0], wv[1]);
-            if (d.part_words == 4) *(ulonglong2*)(rec + 2) = make_ulonglong2(wv[2], wv[3]);
+      for (int v = 0; v < kPartMaxVals; ++v) {
+        vp[v] = (SINK == SK_PART_SCATTER && v < nv) ? &d.progs[d.aggs[d.part_src[v]].prog] : nullptr;
+        vcol[v] = vp[v] && plain(*vp[v]);
+        vca[v] = col_acc(tc, vcol[v] ? vp[v]->fast.leaf[0].arg : 0);
+      }
+      for (uint32_t i0 = 0; i0 < n_sel; i0 += 32) {
+        const uint32_t i = i0 + lane;
+        const bool act = i < n_sel;
+        const uint32_t r = act ? (ident ? i : (uint32_t)sel_in[i]) : 0u;
+        uint64_t key = 0;
+        if (act) key = kcol ? (uint64_t)acc_get(kca, tc, r) : (uint64_t)vm_eval_t(kp, tc, r, st).lo;
+        const uint32_t p = act ? (uint32_t)(key_hash1(key) >> shift) : 0xFFFFFFFFu;
+        uint32_t pos = 0;
+        if (grouped) {
+          // all lanes vote; lanes without a row form their own group, whose leader adds nothing
+          const unsigned peers = __match_any_sync(0xFFFFFFFFu, p);
+          const int leader = __ffs(peers) - 1;
+          uint32_t base = 0;
+          if (act && (int)lane == leader) base = atomicAdd(&s_part[p], (uint32_t)__popc(peers));
+          if (SINK == SK_PART_SCATTER) {
+            base = __shfl_sync(0xFFFFFFFFu, base, leader);
+            pos = base + (uint32_t)__popc(peers & ((1u << lane) - 1u));
           }
+        } else if (act) {
+          if (SINK == SK_PART_COUNT) atomicAdd(&s_part[p], 1u);
+          else pos = atomicAdd(&s_part[p], 1u);
+        }
+        if (SINK == SK_PART_COUNT || !act) continue;
+        // 1, 2 or 4 words: the key, then the inputs (zero padded), written
+        // with 16-byte stores
+        uint64_t wv[kPartMaxVals + 1];
+        wv[0] = key;
+#pragma unroll
+        for (int v = 0; v < kPartMaxVals; ++v)
+          wv[1 + v] = !vp[v] ? 0 : vcol[v] ? (uint64_t)acc_get(vca[v], tc, r) : (uint64_t)vm_eval_t(*vp[v], tc, r, st).lo;
+        uint64_t* const rec = d.part_records + (uint64_t)pos * (uint64_t)d.part_words;
+        if (d.part_words == 1) {
+          rec[0] = key;
+        } else {
+          *(ulonglong2*)rec = make_ulonglong2(wv[0], wv[1]);
+          if (d.part_words == 4) *(ulonglong2*)(rec + 2) = make_ulonglong2(wv[2], wv[3]);
         }
       }
     } else if (SINK == SK_BUILD) {
