@@ -1743,6 +1743,12 @@ __device__ __forceinline__ uint64_t state_combine(int32_t fn, uint64_t x, uint64
 // group that is still collecting, and the lanes at odd ranks within their
 // group drop out, so a group of n lanes takes ceil(log2 n) rounds.
 __device__ __forceinline__ uint64_t peer_combine(int32_t fn, unsigned peers, uint64_t x, uint32_t lane) {
+  // one key across the whole warp: a butterfly leaves the total in every lane
+  if (__all_sync(0xFFFFFFFFu, peers == 0xFFFFFFFFu)) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x = state_combine(fn, x, __shfl_xor_sync(0xFFFFFFFFu, x, o));
+    return x;
+  }
   unsigned rank = __popc(peers & ((1u << lane) - 1u));  // lanes of the group below this one
   unsigned rest = peers & ~((2u << lane) - 1u);          // lanes of the group above this one
   while (__any_sync(0xFFFFFFFFu, rest != 0)) {
@@ -1790,7 +1796,7 @@ constexpr int kPartBatch = 4;  // records per thread with loads in flight togeth
 // the global table.
 constexpr uint32_t kPartProbes = 64;
 
-__global__ void __launch_bounds__(kPartAggThreads) k_part_agg(const __grid_constant__ PipeDesc d) {
+__global__ void __launch_bounds__(kPartAggThreads, 2) k_part_agg(const __grid_constant__ PipeDesc d) {
   extern __shared__ __align__(128) uint8_t smem[];
   const uint32_t np = 1u << d.part_bits;
   const uint32_t cb = blockIdx.x;
@@ -1855,8 +1861,7 @@ __global__ void __launch_bounds__(kPartAggThreads) k_part_agg(const __grid_const
     bool upd[B];      // this lane's record updates an entry
     bool comb[B];     // (warp-uniform) batch q combines records of a key first
     unsigned peers[B];
-    bool any_comb = false;
-#pragma unroll
+  #pragma unroll
     for (int q = 0; q < B; ++q) {
       upd[q] = act[q];
       comb[q] = false;
@@ -1870,7 +1875,6 @@ __global__ void __launch_bounds__(kPartAggThreads) k_part_agg(const __grid_const
         comb[q] = __any_sync(0xFFFFFFFFu, __popc(peers[q]) >= 4);
         // when combining, only the lowest lane of each key's group updates
         if (comb[q]) upd[q] = act[q] && (peers[q] & ((1u << lane) - 1u)) == 0;
-        any_comb |= comb[q];
       }
     }
     // the updating records' entries: shared-memory index, else the global group
@@ -1901,21 +1905,18 @@ __global__ void __launch_bounds__(kPartAggThreads) k_part_agg(const __grid_const
       const uint32_t sa = smem_u32(s.e + 1 + a), sh = smem_u32(s.e + 1 + na + hw);
       unsigned long long* const glo = (unsigned long long*)ag.lo;
       long long* const ghi = (long long*)ag.hi;
-      if (any_comb) {
-        // warp_ok holds: every state is one word
-#pragma unroll
-        for (int q = 0; q < B; ++q) {
-          if (!comb[q]) continue;  // warp-uniform
-          const uint64_t x = peer_combine(ag.fn, peers[q], lane_state_value(ag.fn, v[q], vt), lane);
-          if (idx[q] >= 0) smem_merge(ag.fn, sa + (uint32_t)idx[q] * estride, x);
-          else if (g[q] != kNoGroup) agg_merge(ag.fn, glo + g[q] * gstride, nullptr, x, 0);
-        }
-      }
       auto apply = [&](auto fnc) {
         constexpr int FN = decltype(fnc)::value;
 #pragma unroll
         for (int q = 0; q < B; ++q) {
-          if (comb[q]) continue;
+          if (comb[q]) {  // warp-uniform; only when every state is one word
+            if (FN != A_SUM_I128) {
+              const uint64_t x = peer_combine(FN, peers[q], lane_state_value(FN, v[q], vt), lane);
+              if (idx[q] >= 0) smem_merge(FN, sa + (uint32_t)idx[q] * estride, x);
+              else if (g[q] != kNoGroup) agg_merge(FN, glo + g[q] * gstride, nullptr, x, 0);
+            }
+            continue;
+          }
           if (idx[q] >= 0) {
             const uint32_t eo = (uint32_t)idx[q] * estride;
             smem_apply(FN, sa + eo, sh + eo, v[q], vt);
