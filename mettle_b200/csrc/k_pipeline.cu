@@ -1337,7 +1337,7 @@ __global__ void __launch_bounds__(kThreads, (SINK == SK_AGG_SCALAR || SINK == SK
         }
         if (SINK == SK_PART_COUNT || !act) continue;
         // 1, 2 or 4 words: the key, then the inputs (zero padded), written
-        // with 16-byte stores
+        // with one 16- or 32-byte store
         uint64_t wv[kPartMaxVals + 1];
         wv[0] = key;
 #pragma unroll
@@ -1347,8 +1347,12 @@ __global__ void __launch_bounds__(kThreads, (SINK == SK_AGG_SCALAR || SINK == SK
         if (d.part_words == 1) {
           rec[0] = key;
         } else {
-          *(ulonglong2*)rec = make_ulonglong2(wv[0], wv[1]);
-          if (d.part_words == 4) *(ulonglong2*)(rec + 2) = make_ulonglong2(wv[2], wv[3]);
+          if (d.part_words == 4)  // one 32-byte store (records are 32-byte aligned)
+            asm volatile("st.global.v4.u64 [%0], {%1, %2, %3, %4};" ::"l"(rec), "l"(wv[0]), "l"(wv[1]), "l"(wv[2]),
+                         "l"(wv[3])
+                         : "memory");
+          else
+            *(ulonglong2*)rec = make_ulonglong2(wv[0], wv[1]);
         }
       }
     } else if (SINK == SK_BUILD) {
@@ -1845,13 +1849,14 @@ __global__ void __launch_bounds__(kPartAggThreads, 2) k_part_agg(const __grid_co
         if (W == 1) {
           key[q] = __ldcs(rec);
         } else {
-          const ulonglong2 x = __ldcs((const ulonglong2*)rec);
-          key[q] = x.x;
-          val[q][0] = x.y;
-          if (W == 4) {
-            const ulonglong2 y = __ldcs((const ulonglong2*)rec + 1);
-            val[q][1] = y.x;
-            val[q][2] = y.y;
+          if (W == 4) {  // one 32-byte load
+            asm volatile("ld.global.cs.v4.u64 {%0, %1, %2, %3}, [%4];"
+                         : "=l"(key[q]), "=l"(val[q][0]), "=l"(val[q][1]), "=l"(val[q][2])
+                         : "l"(rec));
+          } else {
+            const ulonglong2 x = __ldcs((const ulonglong2*)rec);
+            key[q] = x.x;
+            val[q][0] = x.y;
           }
         }
       }
