@@ -1789,7 +1789,7 @@ __device__ __forceinline__ void smem_merge(int32_t fn, uint32_t a, uint64_t x) {
 }
 
 constexpr int kPartAggThreads = 512;
-constexpr int kPartBatch = 4;  // records per thread with loads in flight together
+constexpr int kPartBatch = 2;  // records per thread with loads in flight together
 
 // One CTA per chunk: a partition's records split into pieces of at most
 // d.part_chunk, so that a large partition (a skewed key's) is shared by
