@@ -237,6 +237,37 @@ def test_group_by_repeated_keys_in_a_warp(conn, groups, dist):
 
 
 @pytest.mark.gpu
+def test_group_by_probed_column_many_groups(conn):
+    """A one-key aggregate whose key and input come through a join: the
+    partition passes read the probed table's columns by row id."""
+    init(conn)
+    r = np.random.default_rng(31)
+    n_ord, n_item = 200_000, 1_500_000
+    o_id = r.permutation(n_ord).astype(np.int32)
+    o_cust = r.integers(0, 30_000, n_ord).astype(np.int64)
+    i_order = r.integers(0, n_ord + 50_000, n_item).astype(np.int32)  # some match no order
+    i_val = r.integers(-1000, 100_000, n_item).astype(np.int64)
+    conn.create_table("orders", {"o_id": (L.T_INTEGER, o_id), "o_cust": (L.T_BIGINT, o_cust)})
+    conn.create_table("items", {"i_order": (L.T_INTEGER, i_order), "i_val": (L.T_BIGINT, i_val)})
+    conn.gpu_register_table("orders")
+    conn.gpu_register_table("items")
+    res = conn.gpu_processing("SELECT o_cust, COUNT(*), SUM(i_val), MAX(i_val) FROM orders, items "
+                              "WHERE i_order = o_id AND i_val > 0 GROUP BY o_cust ORDER BY o_cust")
+    cust_of = np.full(n_ord + 50_000, -1, np.int64)
+    cust_of[o_id] = o_cust
+    c = cust_of[i_order]
+    m = (c >= 0) & (i_val > 0)
+    want = _grouped(c[m], {"v": i_val[m]})
+    rows = res.fetchall()
+    assert len(rows) == len(want["k"])
+    got = list(zip(*rows))
+    assert np.array_equal(np.array(got[0], np.int64), want["k"])
+    assert np.array_equal(np.array(got[1], np.int64), want["cnt"])
+    assert [int(s) for s in got[2]] == [int(s) for s in want["v_sum"]]
+    assert np.array_equal(np.array(got[3], np.int64), want["v_max"])
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("sql_aggs,cols", [
     ("COUNT(*)", ()),                                          # records hold the key alone
     ("COUNT(*), SUM(a)", "a"),                                 # key and one input
