@@ -164,20 +164,25 @@ def profile_traffic(name: str) -> float | None:
 
 # ------------------------------------------------------------------ workloads
 class Workload:
-    """A benchmark configuration: tables, SQL, fact rows, algorithmic bytes."""
+    """A benchmark configuration: tables, SQL, fact rows, algorithmic bytes.
+    `scale` shrinks the tables (profiling runs on a small case); `groups` and
+    `dist` pick the config-3 key distribution; `keys` the config-4 join keys."""
 
-    def __init__(self, name: str):
+    def __init__(self, name: str, scale: float = 1.0, groups: int | None = None, dist: str | None = None,
+                 keys: str = "dense"):
         self.name = name
         if name == "c4":
-            self.t = W.q3()
+            self.t = W.q3(n_cust=int(1_500_000 * scale), n_ord=int(15_000_000 * scale), keys=keys)
             self.sql = W.q3_sql(self.t.date)
             self.rows = self.t.lineitem_rows
             self.bytes = W.q3_bytes(self.t)
             self.dom_step = "pipeline:agg_slot:lineitem"
-            self.dom_bytes = self.rows * (4 + 8 + 8 + 4)
+            kw = self.t.orders["o_orderkey"].dtype.itemsize
+            self.dom_bytes = self.rows * (kw + 8 + 8 + 4)
             self.desc = (f"c4 join->filter->group->top-10: customer {len(self.t.customer['c_custkey'])}, "
                          f"orders {len(self.t.orders['o_orderkey'])}, lineitem {self.rows} rows; "
-                         "DECIMAL(15,2) as int64 cents, revenue exact int128 at scale 4")
+                         "DECIMAL(15,2) as int64 cents, revenue exact int128 at scale 4"
+                         + ("" if keys == "dense" else f"; {keys} join keys (open-addressing hash joins)"))
         elif name == "c1":
             self.d = W.numbers(1_000_000)
             self.sql = W.C1_SQL
@@ -188,31 +193,34 @@ class Workload:
             self.dom_bytes = 4 * self.rows + sel * 8
             self.desc = "c1 numbers 1M rows: SELECT value, value*10 WHERE value > 500000 ORDER BY value"
         elif name == "c2":
-            self.d = W.scan(100_000_000)
+            self.rows = int(100_000_000 * scale)
+            self.d = W.scan(self.rows)
             self.sql = W.scan_sql("a", "<", 0.5)
-            self.rows = 100_000_000
             sel = int((self.d["a"] < int(0.5 * 2**31)).sum())
             self.bytes = 4 * self.rows + sel * (28 - 4) + sel * 28
             self.dom_step = "pipeline:materialize:t"
             self.dom_bytes = self.bytes
-            self.desc = "c2 scan 1e8 rows (a,b,c,d,e): SELECT a, b+5, c*10, d, e WHERE a < 2^30 (50%)"
+            self.desc = f"c2 scan {self.rows} rows (a,b,c,d,e): SELECT a, b+5, c*10, d, e WHERE a < 2^30 (50%)"
         elif name == "c3":
-            g = int(os.environ.get("C3_GROUPS", "1000000"))
-            dist = os.environ.get("C3_DIST", "uniform")
-            self.d = W.groupby(200_000_000, groups=g, dist=dist)
+            g = groups or int(os.environ.get("C3_GROUPS", "1000000"))
+            dist = dist or os.environ.get("C3_DIST", "uniform")
+            self.rows = int(200_000_000 * scale)
+            self.d = W.groupby(self.rows, groups=g, dist=dist)
             self.sql = W.C3_SQL
-            self.rows = 200_000_000
             self.bytes = 20 * self.rows
             self.dom_step = "pipeline:agg_"
             self.dom_bytes = self.bytes
-            # Many groups take the partitioned aggregation: a count pass
-            # (reads k), a scatter pass (reads k, v, f; writes 32-byte
-            # records of key, v, f and padding) and a per-partition
-            # aggregation (reads the records). The slowest of them is the
-            # dominant kernel.
+            # The query reads 20 B per row (k, v, f). Many groups take the
+            # partitioned aggregation, whose kernels move intermediate records
+            # too (count pass: reads k; scatter pass: reads k, v, f and writes
+            # a 32-byte record; per-partition aggregation: reads the record);
+            # those per-kernel figures are reported as diagnostics, while the
+            # roofline fraction is the query's 20 B per row over the whole
+            # query's time.
             self.dom_candidates = [("pipeline:agg_", self.bytes), ("pipeline:part_count", 8 * self.rows),
                                    ("pipeline:part_scatter", 52 * self.rows), ("part_agg", 32 * self.rows)]
-            self.desc = f"c3 group-by 2e8 rows, G={g} {dist}: SUM/COUNT/MIN/MAX/AVG x2, top-100"
+            self.query_frac_is_roofline = True
+            self.desc = f"c3 group-by {self.rows} rows, G={g} {dist}: SUM/COUNT/MIN/MAX/AVG x2, top-100"
         else:
             raise SystemExit(f"unknown config {name}")
 
@@ -252,6 +260,8 @@ class Workload:
     def cpu_run(self):
         import oracle as orc
         if self.name == "c4":
+            if self.t.orders["o_orderkey"].dtype == np.int64:
+                return orc.q3_numpy(self.t, limit=10)
             return orc.q3(self.t, segment_code=1, limit=10)
         if self.name == "c1":
             rows = orc.filter_rows([(self.d["value"], ">", 500000)])
@@ -269,16 +279,24 @@ class Workload:
         rows = res.fetchall()
         if self.name == "c4":
             got = [(r[0], int(r[1].scaleb(4)), r[3]) for r in rows]
+            if isinstance(want, list):
+                return got == [(k, rev, p) for k, rev, _, p in want]
             exp = list(zip(want["key"].tolist(), want["revenue"], want["prio"].tolist()))
             return got == exp
         if self.name == "c1":
             return np.array_equal(res.columns[0], want[0]) and np.array_equal(res.columns[1], want[1])
         if self.name == "c2":
             return all(np.array_equal(res.columns[i], want[i]) for i in range(5))
+        # every column: integers and AVG(BIGINT) (DuckDB's extended-precision
+        # quotient) exact, FLOAT sums and averages within 1e-6 relative
         ok = len(rows) == len(want["k"])
         for i, r in enumerate(rows[: len(want["k"])]):
-            ok &= r[0] == want["k"][i] and r[1] == want["sum_v"][i] and r[2] == want["cnt"][i]
-            ok &= abs(r[6] - want["sum_f"][i]) <= 1e-6 * abs(want["sum_f"][i])
+            k, sum_v, cnt, min_v, max_v, avg_v, sum_f, min_f, max_f, avg_f = r
+            ok &= k == want["k"][i] and sum_v == want["sum_v"][i] and cnt == want["cnt"][i]
+            ok &= min_v == want["min_v"][i] and max_v == want["max_v"][i] and avg_v == want["avg_v"][i]
+            ok &= abs(sum_f - want["sum_f"][i]) <= 1e-6 * abs(want["sum_f"][i])
+            ok &= np.float32(min_f) == want["min_f"][i] and np.float32(max_f) == want["max_f"][i]
+            ok &= abs(avg_f - want["avg_f"][i]) <= 1e-6 * abs(want["avg_f"][i])
         return bool(ok)
 
 
@@ -345,16 +363,22 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
-def run_mettle(args):
-    ws, rank, local = dist_env()
-    import torch
-    torch.cuda.set_device(local)
-    dist = dist_init(ws)
-    from mettle_b200 import Connection
-    wl = Workload(args.config)
-    conn = Connection(device=local)
+def _budget_sql(wl) -> str:
     gb = max(8, int(wl.bytes * 3 / 2**30) + 8)
-    conn.execute(f"CALL gpu_buffer_init('{gb} GB', '{gb} GB', pinned_memory_size = '{2 * gb} GB')")
+    return f"CALL gpu_buffer_init('{gb} GB', '{gb} GB', pinned_memory_size = '{2 * gb} GB')"
+
+
+def measure(wl, args, dist, local: int, with_e2e: bool, cpu_seconds: float) -> dict:
+    """One configuration's bench figures: K launches of the prepared
+    statement timed with CUDA events on the launching stream (max over
+    ranks), parity of the measured statement against the oracle, per-step
+    device times, the roofline of the dominant kernel, and optionally the
+    end-to-end figure through the public API with host buffers."""
+    import torch
+    from mettle_b200 import Connection
+    ws, rank, _ = dist_env()
+    conn = Connection(device=local)
+    conn.execute(_budget_sql(wl))
     wl.register(conn, upload=True)
     stmt = conn.prepare(wl.sql)
     # A dedicated (non-default) stream: the library enqueues on it and the
@@ -367,6 +391,7 @@ def run_mettle(args):
     stmt.launch(sp)
     first = stmt.fetch()
     parity = wl.parity(first) if rank == 0 else None
+    del first
 
     for _ in range(args.warmup):
         stmt.launch(sp)
@@ -408,61 +433,121 @@ def run_mettle(args):
             per[p].append(sum(t for n, t in steps if n.startswith(p)))
     stmt.set_profiling(False)
     dom_prefix, dom_bytes = max(cands, key=lambda c: statistics.mean(per[c[0]]))
-    wl.dom_step, wl.dom_bytes = dom_prefix, dom_bytes
     dom_ms = statistics.mean(per[dom_prefix])
     peak, peak_src = measured_peak()
-    achieved = wl.dom_bytes / (dom_ms / 1e3) / 1e9
-    traffic = profile_traffic(f"{wl.name}:{wl.dom_step}")
-    query_gbs = wl.bytes / (ms / args.steps / 1e3) / 1e9
-
-    # ---- e2e through the public API with host buffers
-    import os as _os
-    _os.environ["METTLE_DISABLE_QUERY_CACHE"] = "1"
-    pinned = [torch.from_numpy(a).pin_memory() for a in wl.host_arrays()]
-    wl.replace_arrays([p.numpy() for p in pinned])
-    h2d = sum(a.nbytes for a in wl.host_arrays())
-    e2e_steps = max(3, min(args.steps, 10))
-    r = None
-    conn2 = Connection(device=local)
-    conn2.execute(f"CALL gpu_buffer_init('{gb} GB', '{gb} GB', pinned_memory_size = '{2 * gb} GB')")
-    wl.register(conn2, upload=False, borrow=True)
-    r = conn2.gpu_processing(wl.sql)  # warm (plans, stats)
-    barrier(dist, local)
-    t0 = time.perf_counter()
-    for _ in range(e2e_steps):
-        wl.register(conn2, upload=False, borrow=True)  # new table version: H2D on first use
-        r = conn2.gpu_processing(wl.sql)
-    e2e_s = (time.perf_counter() - t0) / e2e_steps
-    e2e_s = reduce_max(dist, e2e_s, f"cuda:{local}")
-    d2h = sum(c.nbytes for c in r.columns) + 12
-    e2e_value = reduce_sum(dist, float(wl.rows), f"cuda:{local}") / e2e_s
-
-    cpu = cpu_baseline(wl, args.cpu_seconds) if (rank == 0 and ws == 1 and args.cpu_seconds > 0) else None
-
-    if rank == 0:
-        line = {
-            "metric": "pipeline rows/s", "value": value, "unit": "rows/s", "n_gpus": ws, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "int64", "data": "synthetic",
-            "config": {"workload": wl.desc, "l2": "inputs larger than L2 (126 MB); no flush",
-                       "parallelism": f"replicas x{ws}" if ws > 1 else "1 GPU"},
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                         "traffic": traffic, "kernel": wl.dom_step, "kernel_ms": dom_ms,
-                         "algorithmic_bytes": wl.dom_bytes, "peak_source": peak_src,
-                         "query_gbs": query_gbs, "query_frac": query_gbs / peak,
-                         "query_algorithmic_bytes": wl.bytes},
-            "cpu_baseline": cpu,
-            "e2e": {"value": e2e_value, "unit": "rows/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                    "ms_per_step": e2e_s * 1e3, "steps": e2e_steps},
-            "gpu_launches": kernels * args.steps,
-            "clocks": clocks,
-            "parity": parity,
-            "step_ms": {k: v / prof_runs for k, v in sorted(totals.items(), key=lambda kv: -kv[1])[:8]},
-        }
-        print(json.dumps(line), flush=True)
+    achieved = dom_bytes / (dom_ms / 1e3) / 1e9
+    traffic = profile_traffic(f"{wl.name}:{dom_prefix}")
+    query_ms = ms / args.steps
+    query_gbs = wl.bytes / (query_ms / 1e3) / 1e9
+    roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "traffic": traffic, "kernel": dom_prefix, "kernel_ms": dom_ms, "algorithmic_bytes": dom_bytes,
+            "peak_source": peak_src, "query_gbs": query_gbs, "query_frac": query_gbs / peak,
+            "query_algorithmic_bytes": wl.bytes}
+    if getattr(wl, "query_frac_is_roofline", False):
+        # the query's own bytes over the whole query's time; the dominant
+        # kernel's figure (which counts intermediate records) is a diagnostic
+        roof.update({"achieved": query_gbs, "frac": query_gbs / peak, "kernel": "whole query",
+                     "kernel_ms": query_ms, "algorithmic_bytes": wl.bytes,
+                     "dominant_kernel": {"name": dom_prefix, "ms": dom_ms, "bytes": dom_bytes,
+                                         "frac": achieved / peak}})
+    out = {"value": value, "ms_per_step": query_ms, "roofline": roof, "gpu_launches": kernels * args.steps,
+           "clocks": clocks, "parity": parity,
+           "step_ms": {k: v / prof_runs for k, v in sorted(totals.items(), key=lambda kv: -kv[1])[:8]}}
     stmt.close()
     conn.close()
-    conn2.close()
+
+    # ---- e2e through the public API with host buffers
+    if with_e2e:
+        os.environ["METTLE_DISABLE_QUERY_CACHE"] = "1"
+        pinned = [torch.from_numpy(a).pin_memory() for a in wl.host_arrays()]
+        wl.replace_arrays([p.numpy() for p in pinned])
+        h2d = sum(a.nbytes for a in wl.host_arrays())
+        e2e_steps = max(3, min(args.steps, 10))
+        conn2 = Connection(device=local)
+        conn2.execute(_budget_sql(wl))
+        wl.register(conn2, upload=False, borrow=True)
+        r = conn2.gpu_processing(wl.sql)  # warm (plans, stats)
+        barrier(dist, local)
+        t0 = time.perf_counter()
+        for _ in range(e2e_steps):
+            wl.register(conn2, upload=False, borrow=True)  # new table version: H2D on first use
+            r = conn2.gpu_processing(wl.sql)
+        e2e_s = (time.perf_counter() - t0) / e2e_steps
+        e2e_s = reduce_max(dist, e2e_s, f"cuda:{local}")
+        d2h = sum(c.nbytes for c in r.columns) + 12
+        e2e_value = reduce_sum(dist, float(wl.rows), f"cuda:{local}") / e2e_s
+        out["e2e"] = {"value": e2e_value, "unit": "rows/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                      "ms_per_step": e2e_s * 1e3, "steps": e2e_steps}
+        del r
+        conn2.close()
+        os.environ.pop("METTLE_DISABLE_QUERY_CACHE", None)
+
+    out["cpu_baseline"] = (cpu_baseline(wl, cpu_seconds)
+                           if (rank == 0 and ws == 1 and cpu_seconds > 0) else None)
+    return out
+
+
+# Extra configurations measured beside the headline in the default run:
+# (key, config, kwargs).
+EXTRA_CONFIGS = [
+    ("c2_scan_a_lt_2e30", "c2", {}),
+    ("c3_groups_1e6_uniform", "c3", {"groups": 1_000_000, "dist": "uniform"}),
+    ("c3_groups_5e7_uniform", "c3", {"groups": 50_000_000, "dist": "uniform"}),
+]
+
+
+def run_profile(args):
+    """Runs one workload as a prepared statement a few times and prints the
+    per-step device times: a small case for a profiler to capture."""
+    from mettle_b200 import Connection
+    wl = Workload(args.config, scale=args.scale, keys=args.keys, groups=args.groups, dist=args.dist)
+    conn = Connection()
+    conn.execute(_budget_sql(wl))
+    wl.register(conn, upload=True)
+    st = conn.prepare(wl.sql)
+    st.set_profiling(True)
+    for i in range(args.launches):
+        st.launch()
+        res = st.fetch()
+        steps = st.step_times()
+        print(f"launch {i}: rows={res.rows} device_ms={st.device_ms():.3f} kernels={st.kernel_count()}")
+        for name, t in steps:
+            print(f"  {name:40s} {t:8.4f} ms")
+    st.close()
+    conn.close()
+
+
+def run_mettle(args):
+    ws, rank, local = dist_env()
+    import torch
+    torch.cuda.set_device(local)
+    dist = dist_init(ws)
+    wl = Workload(args.config, scale=args.scale, keys=args.keys, groups=args.groups, dist=args.dist)
+    m = measure(wl, args, dist, local, with_e2e=True, cpu_seconds=args.cpu_seconds)
+    desc = wl.desc
+    extra = {}
+    if args.config == "c4" and args.scale == 1.0 and args.keys == "dense" and not args.no_extra:
+        del wl
+        for key, cfg, kw in EXTRA_CONFIGS:
+            x = Workload(cfg, **kw)
+            r = measure(x, args, dist, local, with_e2e=False, cpu_seconds=min(args.cpu_seconds, 5.0))
+            extra[key] = {"workload": x.desc, "metric": "pipeline rows/s", "unit": "rows/s", **r}
+            del x
+    if rank == 0:
+        line = {
+            "metric": "pipeline rows/s", "value": m["value"], "unit": "rows/s", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": m["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "int64", "data": "synthetic",
+            "config": {"workload": desc,
+                       "l2": "inputs larger than L2 (126 MB); no flush",
+                       "parallelism": f"replicas x{ws}" if ws > 1 else "1 GPU"},
+            "roofline": m["roofline"], "cpu_baseline": m["cpu_baseline"], "e2e": m["e2e"],
+            "gpu_launches": m["gpu_launches"], "clocks": m["clocks"], "parity": m["parity"],
+            "step_ms": m["step_ms"],
+        }
+        if extra:
+            line["extra_configs"] = extra
+        print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()
 
@@ -668,8 +753,18 @@ def main():
     ap.add_argument("--c5-queries", type=int, default=2000)
     ap.add_argument("--c5-rates", type=float, nargs="+", default=[0.5, 1.0, 2.0])
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--scale", type=float, default=1.0, help="table size factor (profiling runs use a small case)")
+    ap.add_argument("--keys", default="dense", choices=["dense", "sparse32", "sparse64"],
+                    help="config-4 join keys: dense (direct-mapped joins) or sparse (hash joins)")
+    ap.add_argument("--launches", type=int, default=0,
+                    help="profile mode: run the prepared statement this many times and print per-step times")
+    ap.add_argument("--no-extra", action="store_true", help="measure the headline configuration only")
+    ap.add_argument("--groups", type=int, default=None, help="config-3 group count (default 10^6)")
+    ap.add_argument("--dist", default=None, choices=["uniform", "zipf"], help="config-3 key distribution")
     args = ap.parse_args()
-    if args.impl == "reference":
+    if args.launches > 0:
+        run_profile(args)
+    elif args.impl == "reference":
         run_reference(args)
     elif args.config == "c5":
         run_served(args)

@@ -230,13 +230,33 @@ int mtl_scalar_compare(mtl_ctx *ctx, int32_t op, int32_t type, const void *in, u
  * lower row number); out_count: the number written (min(n, k)). Both are
  * device pointers. stream: a cudaStream_t (NULL = the legacy default
  * stream); the call only enqueues work. Limits: 1 <= k <= 32,
- * n <= 2^32 - 2; a call that would need more scratch than the array holds is
- * rejected with MTL_INVALID and a message. The first call on a device looks
+ * n <= 2^32 - 2; sizes beyond them are rejected with MTL_INVALID and a
+ * message, and every size within them runs (the kernels' grid is capped so
+ * that their scratch fits the array). Each call clears the array's first
+ * 256 bytes on its stream before its kernels run. The first call on a device looks
  * up the array's address with that device current; make it before any
  * stream capture. All calls share the array: calls whose kernels overlap on
  * the GPU race and can return wrong rows. */
 int mtl_topk_noalloc(int32_t type, const void *values, uint64_t n, int32_t k, int32_t descending,
                      uint32_t *out_rows, uint64_t *out_count, void *stream);
+
+/* ------------------------------------------------- failure injection */
+/* Test hook for the failure paths, with no counterpart in the reference
+ * (its waits are host-side only). Nothing it does faults, traps or hangs the
+ * GPU: every device wait it shortens is bounded and ends in a status the
+ * host turns into an error, after which the context stays usable.
+ *   MTL_INJECT_NONE: clears any injection.
+ *   MTL_INJECT_LOOKBACK_STALL: in queries compiled from now on, the first
+ *     tile of every order-preserving compaction never publishes its prefix,
+ *     and a look-back wait gives up after `arg` polls (0: the default
+ *     limit); the query fails with MTL_DEVICE_ERROR ("a device wait
+ *     exceeded its iteration limit").
+ *   MTL_INJECT_HOLD_QUEUE: the serving loop starts no queued request until
+ *     the injection is cleared (mtl_request_wait then times out). */
+#define MTL_INJECT_NONE 0
+#define MTL_INJECT_LOOKBACK_STALL 1
+#define MTL_INJECT_HOLD_QUEUE 2
+int mtl_debug_inject(mtl_ctx *ctx, int32_t what, uint32_t arg);
 
 /* -------------------------------------------------------------- serving */
 typedef struct mtl_serve_stats {

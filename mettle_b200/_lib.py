@@ -120,6 +120,7 @@ SIGNATURES = [
                                      C.c_double, C.c_void_p]),
     ("mtl_serve_stats_get", C.c_int, [C.c_void_p, C.POINTER(ServeStats)]),
     ("mtl_serve_set_slots", C.c_int, [C.c_void_p, C.c_int32]),
+    ("mtl_debug_inject", C.c_int, [C.c_void_p, C.c_int32, C.c_uint32]),
     ("mtl_topk_noalloc", C.c_int, [C.c_int32, C.c_void_p, C.c_uint64, C.c_int32, C.c_int32, C.c_void_p,
                                    C.c_void_p, C.c_void_p]),
 ]

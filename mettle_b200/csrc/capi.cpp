@@ -32,6 +32,7 @@ double serve_latency_ms(Request* r);
 void serve_free(Request* r);
 void serve_stats(Ctx& ctx, mtl_serve_stats* out);
 int serve_set_slots(Ctx& ctx, int slots);
+void serve_wake(Ctx& ctx);
 }  // namespace mtl
 
 using namespace mtl;
@@ -835,6 +836,19 @@ int mtl_serve_stats_get(mtl_ctx* ctx, mtl_serve_stats* out) {
 int mtl_serve_set_slots(mtl_ctx* ctx, int32_t slots) {
   if (!ctx) return MTL_NOT_INITIALIZED;
   return serve_set_slots(ctx->c, slots);
+}
+
+int mtl_debug_inject(mtl_ctx* ctx, int32_t what, uint32_t arg) {
+  if (!ctx) return MTL_NOT_INITIALIZED;
+  if (what != MTL_INJECT_NONE && what != MTL_INJECT_LOOKBACK_STALL && what != MTL_INJECT_HOLD_QUEUE) {
+    set_last_error("mtl_debug_inject: unknown injection");
+    return MTL_INVALID;
+  }
+  Ctx& c = ctx->c;
+  c.inject_arg.store(arg);
+  c.inject_kind.store(what);
+  serve_wake(c);  // a held queue starts again once cleared
+  return MTL_OK;
 }
 
 }  // extern "C"

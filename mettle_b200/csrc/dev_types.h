@@ -241,6 +241,8 @@ struct PipeDesc {
   uint64_t* tile_status;            // look-back state, one word per tile
   uint32_t* tile_counter;           // dynamic tile ids + finished CTAs
   uint32_t epoch;                   // look-back epoch (no memset per launch)
+  uint32_t lb_spin_limit;           // polls before a look-back wait gives up (0: kSpinLimit)
+  int32_t lb_stall_first;           // failure injection: tile 0 never publishes its prefix
   // aggregates
   int32_t n_aggs;
   DAgg aggs[kMaxAggs];

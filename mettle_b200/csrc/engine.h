@@ -334,6 +334,9 @@ struct Ctx {
   int64_t grouped_topk_entries = 0;
   std::string last_mode;
   ServeState* serve = nullptr;  // owned; created by the first submit
+  // failure injection (mtl_debug_inject): MTL_INJECT_* and its argument
+  std::atomic<int> inject_kind{0};
+  std::atomic<uint32_t> inject_arg{0};
   ~Ctx();
 };
 

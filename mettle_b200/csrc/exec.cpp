@@ -914,10 +914,13 @@ struct Compiler {
     const uint64_t entry = part_agg_smem_bytes(d);
     const uint64_t cap = std::min<uint64_t>(2048, (100 * 1024) / entry);
     if (cap < 256) return false;
-    // partitions: on average at most half a table of groups each
+    // partitions: on average at most half a table of groups each; beyond
+    // the partition limit, partitions hold more groups than a table and
+    // the records of the keys a full table leaves out update the global
+    // table, within the partition's stretch of it (kept in L2)
     int bits = 1;
-    while ((cap / 2) << bits < est) ++bits;
-    if (bits > part_max_bits()) return false;
+    while ((cap / 2) << bits < est && bits < part_max_bits()) ++bits;
+    const bool overfull = (cap / 2) << bits < est;
     const uint64_t np = 1ull << bits;
     const uint64_t words = nv == 0 ? 1 : nv == 1 ? 2 : 4;  // 16-byte aligned records
     const uint64_t rec_bytes = rows * words * 8;
@@ -929,7 +932,7 @@ struct Compiler {
     d.part_combine = est / np < 128 ? 1 : 0;
     d.part_ctas = ctas;
     d.smem_capacity = (int32_t)cap;
-    d.smem_probes = 0;
+    d.smem_probes = overfull ? 8 : 0;  // 0: the kernel's default window
     // records per CTA: half a partition's average, but small enough for
     // eight CTAs per SM, and at least 4096
     const uint64_t min_ctas = 4ull * (uint64_t)pipeline_part_ctas();
@@ -1349,6 +1352,10 @@ struct Compiler {
       pb.d.tile_status = (uint64_t*)scratch(std::max<uint64_t>(tiles, 1) * 8);
       pb.d.tile_counter = (uint32_t*)scratch(8);
       pb.d.epoch = 1;
+      if (ctx.inject_kind.load() == MTL_INJECT_LOOKBACK_STALL) {
+        pb.d.lb_stall_first = 1;
+        pb.d.lb_spin_limit = ctx.inject_arg.load();
+      }
       memset_step(pb.d.tile_status, 0, std::max<uint64_t>(tiles, 1) * 8);
       memset_step(pb.d.tile_counter, 0, 8);
       push_pipeline(pb, root_rows);
@@ -1577,6 +1584,7 @@ struct Compiler {
     t.out_idx = og;
     t.out_count = oc;
     t.temp = scratch(topk_final_temp_bytes(cap, K));
+    memset_step(t.temp, 0, 256);  // the launch's cross-CTA state starts at zero
     P.steps.push_back(t);
     P.kernels += 2;
     std::vector<FinalOut> vis;

@@ -1248,7 +1248,8 @@ __global__ void __launch_bounds__(kThreads, (SINK == SK_AGG_SCALAR || SINK == SK
     // ---- sink over the surviving rows (sorted: ballots keep row order)
     if (SINK == SK_MATERIALIZE) {
       const uint32_t total = n_sel;
-      const uint64_t base = lb_exclusive_warp(d.tile_status, tile, total, d.epoch, d.status);
+      const uint64_t base = lb_exclusive_warp(d.tile_status, tile, total, d.epoch, d.status,
+                                              d.lb_spin_limit ? d.lb_spin_limit : kSpinLimit, !d.lb_stall_first);
       if (lane == 0 && tile == n_tiles - 1) *d.out_count = base + total;
       // write phase: one output column at a time over the compacted rows
       const uint32_t lim = base >= d.out_capacity ? 0u
@@ -1795,7 +1796,13 @@ constexpr int kPartBatch = 2;  // records per thread with loads in flight togeth
 // d.part_chunk, so that a large partition (a skewed key's) is shared by
 // several CTAs while a CTA sees one partition's keys only. The records go
 // into a shared-memory table (the layout of SmemCas, capacity
-// d.smem_capacity); a record whose key finds no entry within kPartProbes
+// d.smem_capacity); a record whose key finds no entry within d.smem_probes
+// (at most kPartProbes) slots of its home slot goes to the global table directly (a key is
+// claimed only within that window, so its records always take the same
+// route). Partitions with more groups than the table use a short window:
+// once the table is full, records of the keys left out go straight to the
+// global table, where a partition's groups share one stretch that stays in
+// L2 while its CTAs run.
 // slots goes to the global table directly. Then every entry is merged into
 // the global table.
 constexpr uint32_t kPartProbes = 64;
@@ -1825,6 +1832,8 @@ __global__ void __launch_bounds__(kPartAggThreads, 2) k_part_agg(const __grid_co
   const DAggTable& tb = d.table;
   const uint64_t gstride = tb.stride > 1 ? (uint64_t)tb.stride : 1;
   const uint32_t estride = s.stride * 8;
+  const uint32_t probes = d.smem_probes > 0 && (uint32_t)d.smem_probes < kPartProbes ? (uint32_t)d.smem_probes
+                                                                                     : kPartProbes;
   constexpr int B = kPartBatch;
   const uint32_t lane = threadIdx.x & 31;
   // Records of one key are combined within a warp before updating where a
@@ -1890,7 +1899,7 @@ __global__ void __launch_bounds__(kPartAggThreads, 2) k_part_agg(const __grid_co
       idx[q] = -1;
       g[q] = kNoGroup;
       if (upd[q]) {
-        idx[q] = smem_cas_find(s, key[q], kPartProbes, d.part_bits);
+        idx[q] = smem_cas_find(s, key[q], probes, d.part_bits);
         if (idx[q] < 0) g[q] = agg_find_cas(tb, key[q], hash_slot(key_hash1(key[q]), tb.capacity), st);
       }
     }

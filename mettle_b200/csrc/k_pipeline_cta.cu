@@ -990,7 +990,8 @@ __global__ void __launch_bounds__(kThreads) k_pipeline(const __grid_constant__ P
       for (int i = 0; i < PER; ++i)
         if (s_keep[tid * PER + i]) s_list[pos++] = (uint16_t)(tid * PER + i);
       if (tid < 32) {
-        const uint64_t excl = lb_exclusive_warp(d.tile_status, tile, total, d.epoch, d.status);
+        const uint64_t excl = lb_exclusive_warp(d.tile_status, tile, total, d.epoch, d.status,
+                                                d.lb_spin_limit ? d.lb_spin_limit : kSpinLimit, !d.lb_stall_first);
         if (tid == 0) {
           s_base = excl;
           if (tile == n_tiles - 1) *d.out_count = excl + total;

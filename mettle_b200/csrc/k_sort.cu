@@ -460,11 +460,13 @@ __global__ void __launch_bounds__(THREADS) k_topk_warp(const SortItem* __restric
                                                        const uint32_t* __restrict__ idx, const uint64_t* count,
                                                        uint64_t n_max, int K, SortItem* __restrict__ out_keys,
                                                        uint32_t* __restrict__ out_idx, uint64_t* out_count,
-                                                       int final_pass, const uint32_t* __restrict__ remap = nullptr) {
+                                                       int final_pass, const uint32_t* __restrict__ remap = nullptr,
+                                                       uint64_t* reset = nullptr) {
   constexpr int WARPS = THREADS / 32;
   __shared__ Cand s_l[WARPS][32];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const uint64_t n = count ? *count : n_max;
+  uint64_t n = count ? *count : n_max;
+  if (n > n_max) n = n_max;
   const uint64_t per = (n + gridDim.x - 1) / gridDim.x;
   const uint64_t lo = (uint64_t)blockIdx.x * per;
   const uint64_t hi = lo + per < n ? lo + per : n;
@@ -494,6 +496,12 @@ __global__ void __launch_bounds__(THREADS) k_topk_warp(const SortItem* __restric
       out_idx[(uint64_t)blockIdx.x * K + lane] = L.ix;
     }
   }
+  // Every thread read *count before the block merge's barriers: the
+  // cross-CTA state of the first pass can be cleared for the next launch.
+  if (reset && threadIdx.x == 0) {
+    reset[0] = 0;
+    reset[1] = 0;
+  }
 }
 
 // Fused aggregate top-K (K <= 32): the ORDER BY image of each live group is
@@ -502,8 +510,16 @@ __global__ void __launch_bounds__(THREADS) k_topk_warp(const SortItem* __restric
 // written. Ties are broken by the group index, which orders groups the same
 // way as the order-preserving compaction the unfused path uses. A group
 // whose first ORDER BY part alone already places it after the warp's current
-// K-th key is dropped before its other parts (often gathers through a
-// representative row) are read.
+// K-th key, or after the grid-wide cut below, is dropped before its other
+// parts (often gathers through a representative row) are read.
+//
+// Grid-wide cut: a warp whose list holds K groups knows that the K best keys
+// of the whole input start with at most the leading 64 key bits of its own
+// K-th entry, so every warp publishes that value (an atomic max of its
+// complement, so that a zero word means "no cut yet") and prunes against the
+// smallest one published. Each CTA then appends only the candidates that
+// can still win to one list (an atomic counter), and the merge pass reads
+// that list alone: its work no longer grows with the number of CTAs.
 __device__ __forceinline__ bool u256_gt(const U256& a, const Cand& b) {
 #pragma unroll
   for (int i = 0; i < 4; ++i)
@@ -511,8 +527,27 @@ __device__ __forceinline__ bool u256_gt(const U256& a, const Cand& b) {
   return false;
 }
 
+// The leading 64 bits of a key of `bits` significant bits (right aligned in
+// w[0..3], w[0] most significant); shorter keys are returned whole.
+__device__ __forceinline__ uint64_t key_top64(const uint64_t* w, int bits) {
+  if (bits <= 64) return w[3];
+  const int s = bits - 64;  // lowest bit of the leading 64
+  const int wi = 3 - (s >> 6), sh = s & 63;
+  uint64_t x = w[wi] >> sh;
+  if (sh) x |= w[wi - 1] << (64 - sh);
+  return x;
+}
+
+// Cross-CTA state of one fused top-K launch, at the start of its temp area;
+// it must be zero when the launch starts (the merge pass clears it again).
+struct TopkFinalState {
+  unsigned long long cut_inv;  // ~(smallest published cut); 0: none yet
+  unsigned long long n_cand;   // candidates appended
+};
+
 template <int THREADS, int R>
 __global__ void __launch_bounds__(THREADS) k_topk_final(const __grid_constant__ TopkFinalSpec spec, int K,
+                                                        TopkFinalState* __restrict__ gst,
                                                         SortItem* __restrict__ out_keys,
                                                         uint32_t* __restrict__ out_idx) {
   constexpr int WARPS = THREADS / 32;
@@ -524,11 +559,19 @@ __global__ void __launch_bounds__(THREADS) k_topk_final(const __grid_constant__ 
   const uint64_t per = (n + gridDim.x - 1) / gridDim.x;
   const uint64_t lo = (uint64_t)blockIdx.x * per;
   const uint64_t hi = lo + per < n ? lo + per : n;
+  const int tb = spec.total_bits;
   uint32_t* const wb = s_live[warp];
   Cand L = cand_inf();
+  uint64_t cut = ~0ULL;  // warp-uniform: no group whose leading bits exceed it can win
   // Offers the live groups wb[0 .. m): the first ORDER BY part alone drops
   // most of them; the others get their full key.
   auto process = [&](uint32_t m) {
+    {
+      uint64_t g = 0;
+      if (lane == 0) g = ~*(volatile unsigned long long*)&gst->cut_inv;
+      g = __shfl_sync(0xFFFFFFFFu, g, 0);
+      if (g < cut) cut = g;
+    }
     const bool in = (uint32_t)lane < m;
     const uint64_t g = in ? wb[lane] : 0;
     bool v = in;
@@ -539,8 +582,8 @@ __global__ void __launch_bounds__(THREADS) k_topk_final(const __grid_constant__ 
       final_value(spec.part[0], g, vlo, vhi);
       key_part(k, spec.ptype[0], spec.desc[0] != 0, vlo, vhi);
       U256 probe = k;
-      shl_or(probe, spec.total_bits - spec.bits0, 0, 0);
-      if (u256_gt(probe, thr)) v = false;
+      shl_or(probe, tb - spec.bits0, 0, 0);
+      if (u256_gt(probe, thr) || key_top64(probe.w, tb) > cut) v = false;
     }
     Cand c = cand_inf();
     if (v) {
@@ -553,6 +596,15 @@ __global__ void __launch_bounds__(THREADS) k_topk_final(const __grid_constant__ 
       c.ix = (uint32_t)g;
     }
     warp_offer_batch(L, c, v, K, lane);
+    // publish this warp's K-th key when it tightens the cut
+    const Cand kth = cand_shfl(L, K - 1);
+    if (kth.ix != 0xFFFFFFFFu) {
+      const uint64_t t = key_top64(kth.w, tb);
+      if (t < cut) {
+        if (lane == 0) atomicMax(&gst->cut_inv, ~t);
+        cut = t;
+      }
+    }
   };
   // Each warp walks its part of the range R groups per lane at a time,
   // gathers the live ones in wb (ballots, no divergence later) and offers
@@ -598,18 +650,28 @@ __global__ void __launch_bounds__(THREADS) k_topk_final(const __grid_constant__ 
   if (cnt) process(cnt);
   block_merge_lists<WARPS>(L, s_l, warp, lane);
   if (warp == 0) {
-    if (lane < K) {
+    // append the CTA's candidates that can still win
+    uint64_t gc = 0;
+    if (lane == 0) gc = ~*(volatile unsigned long long*)&gst->cut_inv;
+    gc = __shfl_sync(0xFFFFFFFFu, gc, 0);
+    const bool keep = lane < K && L.ix != 0xFFFFFFFFu && key_top64(L.w, tb) <= gc;
+    const uint32_t m = __ballot_sync(0xFFFFFFFFu, keep);
+    unsigned long long base = 0;
+    if (lane == 0 && m) base = atomicAdd(&gst->n_cand, (unsigned long long)__popc(m));
+    base = __shfl_sync(0xFFFFFFFFu, base, 0);
+    if (keep) {
+      const uint64_t at = base + (uint64_t)__popc(m & lt);
       SortItem it;
       it.w[0] = L.w[0]; it.w[1] = L.w[1]; it.w[2] = L.w[2]; it.w[3] = L.w[3];
-      out_keys[(uint64_t)blockIdx.x * K + lane] = it;
-      out_idx[(uint64_t)blockIdx.x * K + lane] = L.ix;
+      out_keys[at] = it;
+      out_idx[at] = L.ix;
     }
   }
 }
 
 constexpr int kTfThreads = 256;  // first pass
 constexpr int kTfItems = 4;      // groups per lane per step
-static unsigned topk_final_ctas(uint64_t n_max) {
+static unsigned topk_final_ctas(uint64_t n_max, unsigned max_ctas) {
   static int per_sm = 0;
   if (!per_sm) {
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_topk_final<kTfThreads, kTfItems>, kTfThreads, 0);
@@ -618,23 +680,33 @@ static unsigned topk_final_ctas(uint64_t n_max) {
   uint64_t ctas = (uint64_t)sms() * (uint64_t)per_sm;
   const uint64_t want = (n_max + kTfThreads * kTfItems * 4 - 1) / (kTfThreads * kTfItems * 4);
   if (want < ctas) ctas = want ? want : 1;
+  if (max_ctas && ctas > max_ctas) ctas = max_ctas;
   return (unsigned)ctas;
 }
 
-size_t topk_final_temp_bytes(uint64_t n_max, int k) {
-  return (size_t)topk_final_ctas(n_max) * (size_t)k * (sizeof(SortItem) + sizeof(uint32_t)) + 256;
+// temp: the cross-CTA state (256 bytes), then the candidate keys and indices.
+size_t topk_final_temp_bytes(uint64_t n_max, int k, unsigned max_ctas) {
+  return 256 + (size_t)topk_final_ctas(n_max, max_ctas) * (size_t)k * (sizeof(SortItem) + sizeof(uint32_t));
+}
+
+unsigned topk_final_max_ctas_for(size_t temp_bytes, int k) {
+  if (temp_bytes <= 256 || k <= 0) return 0;
+  return (unsigned)((temp_bytes - 256) / ((size_t)k * (sizeof(SortItem) + sizeof(uint32_t))));
 }
 
 cudaError_t launch_topk_final(const TopkFinalSpec& spec, int k, uint32_t* out_g, uint64_t* out_count, void* temp,
-                              cudaStream_t s) {
+                              cudaStream_t s, unsigned max_ctas) {
   if (k <= 0 || k > 32 || spec.n_parts <= 0 || spec.n_parts > kMaxOrder || spec.total_bits > 256 ||
       spec.bits0 <= 0 || spec.bits0 > spec.total_bits)
     return cudaErrorInvalidValue;
-  const unsigned ctas = topk_final_ctas(spec.n_max);
-  SortItem* pk = (SortItem*)temp;
+  const unsigned ctas = topk_final_ctas(spec.n_max, max_ctas);
+  if (ctas == 0) return cudaErrorInvalidValue;
+  TopkFinalState* gst = (TopkFinalState*)temp;
+  SortItem* pk = (SortItem*)((uint8_t*)temp + 256);
   uint32_t* pi = (uint32_t*)(pk + (uint64_t)ctas * k);
-  k_topk_final<kTfThreads, kTfItems><<<ctas, kTfThreads, 0, s>>>(spec, k, pk, pi);
-  k_topk_warp<1024><<<1, 1024, 0, s>>>(pk, pi, nullptr, (uint64_t)ctas * k, k, nullptr, out_g, out_count, 1);
+  k_topk_final<kTfThreads, kTfItems><<<ctas, kTfThreads, 0, s>>>(spec, k, gst, pk, pi);
+  k_topk_warp<1024><<<1, 1024, 0, s>>>(pk, pi, (const uint64_t*)&gst->n_cand, (uint64_t)ctas * k, k, nullptr, out_g,
+                                       out_count, 1, nullptr, (uint64_t*)gst);
   return cudaGetLastError();
 }
 

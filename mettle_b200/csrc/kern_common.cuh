@@ -387,13 +387,17 @@ __device__ __forceinline__ uint64_t lb_exclusive(uint64_t* status, uint64_t t, u
 // inspects predecessor t-1-i, so one round trip covers 32 tiles. Sums the
 // aggregates back to the nearest published prefix, publishes this tile's
 // inclusive prefix and returns its exclusive prefix (in every lane).
+// spin_limit bounds the polls of unpublished predecessors; publish_first =
+// false (failure injection only) keeps tile 0 from publishing, so that the
+// waits behind it run out.
 __device__ __forceinline__ uint64_t lb_exclusive_warp(uint64_t* status, uint64_t t, uint64_t c, uint32_t epoch,
-                                                      uint32_t* st_flags) {
+                                                      uint32_t* st_flags, uint32_t spin_limit = kSpinLimit,
+                                                      bool publish_first = true) {
   const int lane = threadIdx.x & 31;
   const uint64_t ep = (uint64_t)(epoch & 0xFFFFu);
   const uint64_t vmask = (1ULL << 46) - 1;
   if (t == 0) {
-    if (lane == 0) st_release(status, lb_word(epoch, kLbPre, c));
+    if (lane == 0 && publish_first) st_release(status, lb_word(epoch, kLbPre, c));
     return 0;
   }
   if (lane == 0) st_release(status + t, lb_word(epoch, kLbAgg, c));
@@ -416,7 +420,7 @@ __device__ __forceinline__ uint64_t lb_exclusive_warp(uint64_t* status, uint64_t
     const int limit = pre ? __ffs(pre) - 1 : 31;  // lanes 0..limit are summed
     const uint32_t upto = limit == 31 ? 0xFFFFFFFFu : ((1u << (limit + 1)) - 1u);
     if (none & upto) {
-      if (++spins > kSpinLimit) {
+      if (++spins > spin_limit) {
         if (lane == 0) atomicOr(st_flags, ST_SPIN_LIMIT);
         break;
       }

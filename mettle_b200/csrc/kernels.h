@@ -122,9 +122,15 @@ struct TopkFinalSpec {
   const uint64_t* n_dev;
   uint64_t n_max;
 };
-size_t topk_final_temp_bytes(uint64_t n_max, int k);
+// temp starts with 256 bytes of cross-CTA state that must be zero when the
+// launch starts (the launch leaves it zero again). max_ctas (0: no limit)
+// caps the first pass's grid, and with it the temp size; each CTA then
+// covers more groups.
+size_t topk_final_temp_bytes(uint64_t n_max, int k, unsigned max_ctas = 0);
+// The largest max_ctas whose temp fits in temp_bytes.
+unsigned topk_final_max_ctas_for(size_t temp_bytes, int k);
 cudaError_t launch_topk_final(const TopkFinalSpec& spec, int k, uint32_t* out_g, uint64_t* out_count, void* temp,
-                              cudaStream_t s);
+                              cudaStream_t s, unsigned max_ctas = 0);
 
 // ---- gathers for final materialization (k_misc.cu)
 // out[i] = in[idx[i]] for fixed width elements (4, 8 or 16 bytes).

@@ -11,10 +11,14 @@
 // * The array holds kScratchBytes (1 MiB) on every GPU that loads the
 //   library, for as long as the process lives.
 // * All calls share it, and it keeps whatever the last call left in it.
-//   Nothing in it has to start at zero: the first kernel writes every entry
-//   the second kernel reads. Calls whose kernels overlap on the GPU (on
-//   different streams, or from different host threads without ordering)
-//   race on the array and can return wrong rows; order them on one stream.
+//   Its first 256 bytes (the pruning cut and the candidate count shared by
+//   the CTAs of one call) must start at zero, so every call clears them on
+//   its stream before the kernels run; the candidate lists need no clearing.
+//   Calls whose kernels overlap on the GPU (on different streams, or from
+//   different host threads without ordering) race on the array and can
+//   return wrong rows; order them on one stream.
+// * The first kernel's grid is capped so that its candidate lists fit the
+//   array (each CTA then covers more rows), so every n up to 2^32 - 2 runs.
 // * The first call on each device looks up the array's device address with
 //   that device current. Make that first call before any stream capture
 //   begins on the device.
@@ -89,8 +93,9 @@ extern "C" int mtl_topk_noalloc(int32_t type, const void* values, uint64_t n, in
     mtl::set_last_error("mtl_topk_noalloc: null buffer");
     return MTL_INVALID;
   }
-  const size_t need = mtl::topk_final_temp_bytes(n, k);
-  if (need > kScratchBytes) {
+  const unsigned max_ctas = mtl::topk_final_max_ctas_for(kScratchBytes, k);
+  const size_t need = mtl::topk_final_temp_bytes(n, k, max_ctas);
+  if (max_ctas == 0 || need > kScratchBytes) {
     mtl::set_last_error("mtl_topk_noalloc: needs " + std::to_string(need) + " bytes of scratch; the fixed scratch holds " +
                         std::to_string(kScratchBytes));
     return MTL_INVALID;
@@ -111,7 +116,10 @@ extern "C" int mtl_topk_noalloc(int32_t type, const void* values, uint64_t n, in
   spec.part[0].kind = mtl::F_COPY_I64;
   spec.part[0].a = (const uint64_t*)values;
   spec.n_max = n;
-  cudaError_t e = mtl::launch_topk_final(spec, k, out_rows, out_count, scratch, (cudaStream_t)stream);
+  // the cross-CTA state starts at zero (a memset, not an allocation)
+  cudaError_t e = cudaMemsetAsync(scratch, 0, 256, (cudaStream_t)stream);
+  if (e == cudaSuccess)
+    e = mtl::launch_topk_final(spec, k, out_rows, out_count, scratch, (cudaStream_t)stream, max_ctas);
   if (e != cudaSuccess) {
     mtl::set_last_error(std::string("mtl_topk_noalloc: launch failed: ") + cudaGetErrorString(e));
     return MTL_DEVICE_ERROR;

@@ -186,7 +186,10 @@ static void worker(Ctx* ctx, ServeState* S, int slot) {
     std::vector<Request*> batch;
     {
       std::unique_lock<std::mutex> lk(S->mu);
-      S->cv.wait(lk, [&] { return S->stop || !S->queue.empty(); });
+      // (failure injection can hold the queue: nothing starts until it is cleared)
+      S->cv.wait(lk, [&] {
+        return S->stop || (!S->queue.empty() && ctx->inject_kind.load() != MTL_INJECT_HOLD_QUEUE);
+      });
       if (S->stop && S->queue.empty()) return;
       Request* r = S->queue.front();
       S->queue.pop_front();
@@ -306,6 +309,14 @@ void serve_stats(Ctx& ctx, mtl_serve_stats* out) {
   }
   out->admitted_bytes = S.admitted_bytes;
   out->batched_launches = S.batched;
+}
+
+// Wakes the workers (after a change of the queue-holding injection).
+void serve_wake(Ctx& ctx) {
+  std::lock_guard<std::recursive_mutex> g(ctx.mu);
+  if (!ctx.serve) return;
+  { std::lock_guard<std::mutex> q(ctx.serve->mu); }
+  ctx.serve->cv.notify_all();
 }
 
 int serve_set_slots(Ctx& ctx, int slots) {

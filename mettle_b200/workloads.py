@@ -128,16 +128,42 @@ class Q3Tables:
         return len(self.lineitem["l_orderkey"])
 
 
-def q3(n_cust: int = 1_500_000, n_ord: int = 15_000_000, seed_salt: int = 0) -> Q3Tables:
+def _sparse_keys(r: np.random.Generator, n: int, dtype) -> np.ndarray:
+    """n distinct keys spread over the whole range of dtype (both extremes
+    and -1 included when n allows), in random order."""
+    info = np.iinfo(dtype)
+    special = np.array([-1, info.min, info.max], dtype=np.int64)[: min(3, n)]
+    k = np.unique(r.integers(info.min, info.max, n + n // 8 + 16, dtype=np.int64, endpoint=True))
+    k = np.setdiff1d(k, special)
+    k = np.concatenate([special, r.choice(k, n - len(special), replace=False)])
+    r.shuffle(k)
+    return k.astype(dtype)
+
+
+def q3(n_cust: int = 1_500_000, n_ord: int = 15_000_000, seed_salt: int = 0, keys: str = "dense") -> Q3Tables:
+    """keys="dense": custkey 1..n_cust and orderkey 1..n_ord (the direct-mapped
+    joins); "sparse32" / "sparse64": distinct INTEGER / BIGINT keys spread over
+    the whole type range (-1 and both extremes included), so both joins take
+    the open-addressing hash tables."""
     r = rng(4, seed_salt)
+    if keys == "dense":
+        cust_keys = np.arange(1, n_cust + 1, dtype=np.int32)
+        order_keys = np.arange(1, n_ord + 1, dtype=np.int32)
+    elif keys in ("sparse32", "sparse64"):
+        dt = np.int32 if keys == "sparse32" else np.int64
+        kr = rng(40, seed_salt)
+        cust_keys = _sparse_keys(kr, n_cust, dt)
+        order_keys = _sparse_keys(kr, n_ord, dt)
+    else:
+        raise ValueError(keys)
     customer = {
-        "c_custkey": np.arange(1, n_cust + 1, dtype=np.int32),
+        "c_custkey": cust_keys,
         "c_mktsegment": r.integers(0, len(SEGMENTS), n_cust, dtype=np.int32),
     }
     orderdate = (DAY0 + r.integers(0, SPAN_DAYS, n_ord, dtype=np.int32)).astype(np.int32)
     orders = {
-        "o_orderkey": np.arange(1, n_ord + 1, dtype=np.int32),
-        "o_custkey": r.integers(1, n_cust + 1, n_ord, dtype=np.int32),
+        "o_orderkey": order_keys,
+        "o_custkey": cust_keys[r.integers(0, n_cust, n_ord)],
         "o_orderdate": orderdate,
         "o_shippriority": np.zeros(n_ord, dtype=np.int32),
     }
@@ -165,19 +191,21 @@ def q3_sql(date: int, segment: str = "BUILDING", limit: int = 10) -> str:
 
 def q3_bytes(t: Q3Tables) -> int:
     """Algorithmic bytes of one config-4 query: every column the query names, read once."""
-    return (len(t.customer["c_custkey"]) * (4 + 4) + len(t.orders["o_orderkey"]) * (4 + 4 + 4 + 4)
-            + t.lineitem_rows * (4 + 8 + 8 + 4))
+    kw = t.orders["o_orderkey"].dtype.itemsize
+    return (len(t.customer["c_custkey"]) * (kw + 4) + len(t.orders["o_orderkey"]) * (kw + kw + 4 + 4)
+            + t.lineitem_rows * (kw + 8 + 8 + 4))
 
 
 def register_q3(conn, t: Q3Tables, upload: bool = True, borrow: bool = False):
     from . import _lib as L
-    conn.create_table("customer", {"c_custkey": (L.T_INTEGER, t.customer["c_custkey"]),
+    kt = L.T_BIGINT if t.orders["o_orderkey"].dtype == np.int64 else L.T_INTEGER
+    conn.create_table("customer", {"c_custkey": (kt, t.customer["c_custkey"]),
                                    "c_mktsegment": (L.T_VARCHAR, t.customer["c_mktsegment"], SEGMENTS)})
-    conn.create_table("orders", {"o_orderkey": (L.T_INTEGER, t.orders["o_orderkey"]),
-                                 "o_custkey": (L.T_INTEGER, t.orders["o_custkey"]),
+    conn.create_table("orders", {"o_orderkey": (kt, t.orders["o_orderkey"]),
+                                 "o_custkey": (kt, t.orders["o_custkey"]),
                                  "o_orderdate": (L.T_DATE, t.orders["o_orderdate"]),
                                  "o_shippriority": (L.T_INTEGER, t.orders["o_shippriority"])})
-    conn.create_table("lineitem", {"l_orderkey": (L.T_INTEGER, t.lineitem["l_orderkey"]),
+    conn.create_table("lineitem", {"l_orderkey": (kt, t.lineitem["l_orderkey"]),
                                    "l_extendedprice": (L.T_DECIMAL, t.lineitem["l_extendedprice"], 2),
                                    "l_discount": (L.T_DECIMAL, t.lineitem["l_discount"], 2),
                                    "l_shipdate": (L.T_DATE, t.lineitem["l_shipdate"])})

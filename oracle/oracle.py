@@ -148,3 +148,37 @@ def q3(t, segment_code: int = 1, limit: int = 10) -> dict:
 
 def threads() -> int:
     return int(lib().orc_threads())
+
+
+def _lookup(keys: np.ndarray, probe: np.ndarray) -> np.ndarray:
+    """Row of each probe value in `keys` (distinct values), -1 when absent."""
+    o = np.argsort(keys, kind="stable")
+    s = keys[o]
+    if len(s) == 0:
+        return np.full(len(probe), -1, np.int64)
+    i = np.minimum(np.searchsorted(s, probe), len(s) - 1)
+    return np.where(s[i] == probe, o[i], -1)
+
+
+def q3_numpy(t, limit: int = 10, segment_code: int = 1) -> list[tuple]:
+    """Config-4 pipeline in numpy for keys of any integer width (orc_q3 takes
+    INTEGER keys only): rows (orderkey, revenue at scale 4, orderdate,
+    shippriority) ordered by revenue DESC, orderdate, orderkey. Same
+    relational result as orc_q3; revenue per order fits int64 here (at most
+    7 lines of at most 10,500,000 x 100)."""
+    c, o, li = t.customer, t.orders, t.lineitem
+    qual_cust = c["c_custkey"][c["c_mktsegment"] == segment_code]
+    om = (o["o_orderdate"] < t.date) & np.isin(o["o_custkey"], qual_cust)
+    ok = o["o_orderkey"][om]
+    row = _lookup(ok, li["l_orderkey"])
+    lm = (row >= 0) & (li["l_shipdate"] > t.date)
+    keys, inv = np.unique(li["l_orderkey"][lm], return_inverse=True)
+    rev = np.zeros(len(keys), np.int64)
+    np.add.at(rev, inv, li["l_extendedprice"][lm] * (100 - li["l_discount"][lm]))
+    orow = np.flatnonzero(om)[_lookup(ok, keys)]
+    date = o["o_orderdate"][orow]
+    prio = o["o_shippriority"][orow]
+    order = np.lexsort((keys, date, -rev))
+    if limit >= 0:
+        order = order[:limit]
+    return [(int(keys[i]), int(rev[i]), int(date[i]), int(prio[i])) for i in order]

@@ -156,6 +156,75 @@ def test_c3_all_groups_exact(conn):
     assert np.array_equal(r.columns[3], want["min_v"]) and np.array_equal(r.columns[4], want["max_v"])
 
 
+def _step_names(conn, sql):
+    """Names of the device steps a prepared statement runs."""
+    st = conn.prepare(sql)
+    try:
+        st.set_profiling(True)
+        st.launch()
+        st.fetch()
+        return [n for n, _ in st.step_times()]
+    finally:
+        st.close()
+
+
+def _check_c3_all_groups(res, want):
+    """Every group of the config-3 aggregate (ordered by k) against the oracle:
+    integers and AVG(BIGINT) exact, FLOAT sums and averages within 1e-6."""
+    assert res.rows == want["groups"] == len(want["k"])
+    k, sv, cnt, mnv, mxv, avg, sf, mnf, mxf, avgf = res.columns
+    assert np.array_equal(k, want["k"])
+    assert np.array_equal(sv[:, 0].view(np.uint64), want["sum_lo"])
+    assert np.array_equal(sv[:, 1], want["sum_hi"])
+    assert np.array_equal(cnt, want["cnt"])
+    assert np.array_equal(mnv, want["min_v"]) and np.array_equal(mxv, want["max_v"])
+    assert np.array_equal(avg, want["avg_v"])  # DuckDB's extended-precision quotient
+    assert np.all(np.abs(sf - want["sum_f"]) <= FLOAT_RTOL * np.abs(want["sum_f"]))
+    assert np.array_equal(mnf, want["min_f"]) and np.array_equal(mxf, want["max_f"])
+    assert np.all(np.abs(avgf - want["avg_f"]) <= FLOAT_RTOL * np.abs(want["avg_f"]))
+
+
+C3_ALL_GROUPS_SQL = ("SELECT k, SUM(v), COUNT(*), MIN(v), MAX(v), AVG(v), SUM(f), MIN(f), MAX(f), AVG(f) "
+                     "FROM t GROUP BY k ORDER BY k")
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n,groups,dist", [(20_000_000, 4_000_000, "uniform"), (40_000_000, 8_000_000, "zipf")])
+def test_c3_many_partitions_all_groups(conn, n, groups, dist):
+    """Millions of groups: the partitioned aggregation at thousands of
+    partitions (the scan over the partition totals covers several entries per
+    thread, and partitions hold more groups than a CTA's shared-memory table,
+    so records also reach the global table directly), uniform and Zipf.
+    Every group is compared on all ten aggregates, and the plan must have
+    taken the partitioned steps."""
+    init(conn, "16 GB", "16 GB")
+    d = W.groupby(n=n, groups=groups, dist=dist, seed_salt=3)
+    conn.create_table("t", {"k": (L.T_BIGINT, d["k"]), "v": (L.T_BIGINT, d["v"]), "f": (L.T_FLOAT, d["f"])})
+    conn.gpu_register_table("t", upload=True)
+    steps = _step_names(conn, C3_ALL_GROUPS_SQL)
+    assert "part_agg" in steps and "part_scan" in steps, steps
+    want = orc.groupby_c3(d["k"], d["v"], d["f"], limit=-1)
+    _check_c3_all_groups(conn.gpu_processing(C3_ALL_GROUPS_SQL), want)
+    # and the headline form: top-100 by SUM(v) with the key as the tie-break
+    r = conn.gpu_processing(W.C3_SQL)
+    top = orc.groupby_c3(d["k"], d["v"], d["f"], limit=100)
+    assert np.array_equal(r.columns[0], top["k"]) and np.array_equal(r.columns[2], top["cnt"])
+    assert np.array_equal(r.columns[5], top["avg_v"])
+
+
+@pytest.mark.gpu
+def test_c3_highest_cardinality_all_groups(conn):
+    """About four rows per group over 1.5*10^7 groups (the headline
+    cardinality's rows per group): more groups than one level of partitions
+    keeps within shared-memory tables."""
+    init(conn, "16 GB", "16 GB")
+    d = W.groupby(n=60_000_000, groups=15_000_000, dist="uniform", seed_salt=4)
+    conn.create_table("t", {"k": (L.T_BIGINT, d["k"]), "v": (L.T_BIGINT, d["v"]), "f": (L.T_FLOAT, d["f"])})
+    conn.gpu_register_table("t", upload=True)
+    want = orc.groupby_c3(d["k"], d["v"], d["f"], limit=-1)
+    _check_c3_all_groups(conn.gpu_processing(C3_ALL_GROUPS_SQL), want)
+
+
 def _grouped(keys, cols):
     """Per distinct key (ascending): COUNT and, per column, SUM / MIN / MAX / SUM(|x|)."""
     o = np.argsort(keys, kind="stable")

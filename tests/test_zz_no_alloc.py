@@ -4,7 +4,8 @@ given all device memory to its own pool, or may not allow cudaMalloc or
 cudaFree to synchronize the device.
 
 The entry point is checked against the existing path, gpu_processing with
-ORDER BY ... LIMIT, on two calls in a row. The two calls share the fixed
+ORDER BY ... LIMIT, and against numpy's stable argsort, on two calls in a
+row. The two calls share the fixed
 scratch array, so the second call also shows that what the first one left
 there does no harm. This file sorts last, so a run that stops at the first
 failure has already run every other test."""
@@ -55,6 +56,29 @@ def test_topk_noalloc_matches_gpu_processing_twice(conn):
         assert len(got_rows) == k
         np.testing.assert_array_equal(got_rows, want_rows)
         np.testing.assert_array_equal(v[got_rows], want_v)
+        # and a CPU reference that shares no code with either GPU path
+        np.testing.assert_array_equal(got_rows, np.argsort(-v if desc else v, kind="stable")[:k])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n,k", [(20_000_000, 32), (7_000_001, 25)])
+def test_topk_noalloc_large_n_matches_numpy(built_lib, n, k):
+    """Sizes whose full-occupancy grid would need more candidate lists than
+    the fixed array holds: the grid is capped and every row still counts.
+    Checked against numpy's stable argsort (ties: the lower row first),
+    descending then ascending, two calls in a row on the same array."""
+    import torch
+
+    lib = L.load()
+    r = np.random.default_rng(n)
+    v = r.integers(-(2**40), 2**40, n, dtype=np.int64)
+    v[r.integers(0, n, 64)] = 2**40 + 7  # repeated maxima: ties decided by row number
+    v[r.integers(0, n, 64)] = -(2**40) - 7
+    v_dev = torch.from_numpy(v).cuda()
+    for desc in (True, False):
+        want = np.argsort(-v if desc else v, kind="stable")[:k]
+        got = _noalloc(lib, torch, v_dev, n, desc, k)
+        np.testing.assert_array_equal(got, want)
 
 
 @pytest.mark.gpu
