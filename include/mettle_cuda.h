@@ -240,6 +240,19 @@ int mtl_scalar_compare(mtl_ctx *ctx, int32_t op, int32_t type, const void *in, u
 int mtl_topk_noalloc(int32_t type, const void *values, uint64_t n, int32_t k, int32_t descending,
                      uint32_t *out_rows, uint64_t *out_count, void *stream);
 
+/* -------------------------------------------------------------- autotuner */
+/* No counterpart in the reference, which fixes its launch shapes (one thread
+ * per row, a constant threadgroup size: src/metal/shaders/compiler.rs:69-91)
+ * and its hash capacity (src/plan/executor/join_plan.rs:300-303). Runs the
+ * query's program once per candidate and keeps, per device, the fastest
+ * CTAs per SM and tile size (rows a warp takes per step) of each pipeline,
+ * and the hash-table load factor of its join and aggregate tables, keyed by
+ * the kind of step and the size class of its input. The table is saved to
+ * $METTLE_TUNE_FILE (default ~/.cache/mettle_b200/autotune_<device>.txt) and
+ * applied to every query compiled afterwards on that device. `reps` timed
+ * runs per candidate; a text report of the choices goes to `report`. */
+int mtl_autotune(mtl_ctx *ctx, const char *sql, int32_t reps, char *report, size_t report_cap);
+
 /* ------------------------------------------------- failure injection */
 /* Test hook for the failure paths, with no counterpart in the reference
  * (its waits are host-side only). Nothing it does faults, traps or hangs the

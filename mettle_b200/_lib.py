@@ -121,6 +121,7 @@ SIGNATURES = [
     ("mtl_serve_stats_get", C.c_int, [C.c_void_p, C.POINTER(ServeStats)]),
     ("mtl_serve_set_slots", C.c_int, [C.c_void_p, C.c_int32]),
     ("mtl_debug_inject", C.c_int, [C.c_void_p, C.c_int32, C.c_uint32]),
+    ("mtl_autotune", C.c_int, [C.c_void_p, C.c_char_p, C.c_int32, C.c_char_p, C.c_size_t]),
     ("mtl_topk_noalloc", C.c_int, [C.c_int32, C.c_void_p, C.c_uint64, C.c_int32, C.c_int32, C.c_void_p,
                                    C.c_void_p, C.c_void_p]),
 ]

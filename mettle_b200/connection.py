@@ -576,6 +576,14 @@ class Connection:
     def set_serve_slots(self, n: int):
         self._check(self.lib.mtl_serve_set_slots(self.ctx, n))
 
+    def autotune(self, sql: str, reps: int = 3) -> str:
+        """Measures launch shapes and hash load factors for the query's steps
+        and keeps the fastest per device (mtl_autotune); returns the report."""
+        self._require_ctx()
+        buf = C.create_string_buffer(16384)
+        self._check(self.lib.mtl_autotune(self.ctx, sql.encode(), reps, buf, len(buf)))
+        return buf.value.decode()
+
 
 class Statement:
     """A prepared statement: launch() enqueues with no host sync."""

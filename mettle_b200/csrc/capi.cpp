@@ -838,6 +838,33 @@ int mtl_serve_set_slots(mtl_ctx* ctx, int32_t slots) {
   return serve_set_slots(ctx->c, slots);
 }
 
+int mtl_autotune(mtl_ctx* ctx, const char* sql, int32_t reps, char* report, size_t report_cap) {
+  if (!ctx) {
+    set_last_error("call gpu_buffer_init before gpu_processing");
+    return MTL_NOT_INITIALIZED;
+  }
+  return guarded([&] {
+    cudaSetDevice(ctx->c.device);
+    std::string s = sql ? sql : "";
+    if (s.find_first_not_of(" \t\r\n;") == std::string::npos)
+      fail(MTL_INVALID, "gpu_processing requires a non-empty SQL string");
+    SelectStmt ast;
+    try {
+      ast = parse_sql(s);
+    } catch (const SqlError& e) {
+      fail(MTL_UNSUPPORTED, std::string("SQL outside the offloaded subset: ") + e.what());
+    }
+    BoundPlan plan = bind_select(ctx->c, ast);
+    if (plan.constant_only) fail(MTL_INVALID, "a constant query has nothing to tune");
+    const std::string r = autotune(ctx->c, plan, reps);
+    if (report && report_cap) {
+      const size_t n = std::min(report_cap - 1, r.size());
+      memcpy(report, r.data(), n);
+      report[n] = 0;
+    }
+  });
+}
+
 int mtl_debug_inject(mtl_ctx* ctx, int32_t what, uint32_t arg) {
   if (!ctx) return MTL_NOT_INITIALIZED;
   if (what != MTL_INJECT_NONE && what != MTL_INJECT_LOOKBACK_STALL && what != MTL_INJECT_HOLD_QUEUE) {

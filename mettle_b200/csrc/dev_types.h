@@ -127,8 +127,9 @@ struct DBuild {
   int64_t* hash_keys;       // hash: keys
   uint32_t* hash_slot;      // hash: slot + 1 per table entry
   uint32_t* hash_special;   // hash: slot + 1 of the key equal to kEmptyKey
-  uint32_t* payload[kMaxSrc];  // payload[s][slot] = row id of source s
-  uint32_t* n_slots;        // number of slots assigned (device counter)
+  // payload[s][slot] = row id of source s; a build's slot is its own row
+  // number, so the build's own source has no array (null)
+  uint32_t* payload[kMaxSrc];
   int32_t unique_keys;      // the key column holds no duplicates (no check needed)
   int32_t pad;
 };
@@ -271,6 +272,13 @@ struct PipeDesc {
   uint32_t* part_start;             // first record of each partition (P + 1 entries)
   uint32_t* part_chunk_start;       // first chunk of each partition (P + 1 entries)
   uint64_t* part_records;
+
+  // launch shape (0: defaults), picked per pipeline by the autotuner:
+  // resident CTAs per SM of the grid, and consecutive warp-tiles a warp
+  // takes per step of its grid stride (a warp's step covers tile_group x
+  // 256 rows)
+  int32_t grid_per_sm;
+  int32_t tile_group;
 
   uint32_t* status;                 // DevStatus bits
 };

@@ -256,6 +256,8 @@ struct Program {
   std::vector<cudaEvent_t> prof_ev;
   // the whole program captured once as a CUDA graph and replayed
   cudaGraphExec_t graph = nullptr;
+  // autotuner keys of the capacities (hash load factors) this compile chose
+  std::vector<std::pair<std::string, uint64_t>> load_keys;
   ~Program();
 };
 
@@ -337,6 +339,10 @@ struct Ctx {
   // failure injection (mtl_debug_inject): MTL_INJECT_* and its argument
   std::atomic<int> inject_kind{0};
   std::atomic<uint32_t> inject_arg{0};
+  // autotuner table (tune.cpp): key -> (choice a, choice b), read from and
+  // written to a file per device
+  std::map<std::string, std::pair<double, double>> tune;
+  bool tune_loaded = false;
   ~Ctx();
 };
 
@@ -354,6 +360,14 @@ std::shared_ptr<Result> fetch_program(Ctx& ctx, Program& p, cudaStream_t s);
 void free_program(Ctx& ctx, Program& p);
 std::shared_ptr<Result> constant_result(const BoundPlan& plan);
 std::shared_ptr<Result> processing(Ctx& ctx, const std::string& sql);
+
+// autotuner (tune.cpp)
+std::string tune_key_pipeline(const Step& s);
+std::string tune_key_load(const char* what, uint64_t rows);
+void tune_apply(Ctx& ctx, Program& p);
+double tune_load_factor(Ctx& ctx, const char* what, uint64_t rows);
+std::string tune_file_path(const Ctx& ctx);
+std::string autotune(Ctx& ctx, const BoundPlan& plan, int reps);
 
 // serving (serve.cpp)
 struct Request;

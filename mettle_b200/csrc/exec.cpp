@@ -695,8 +695,6 @@ struct Compiler {
     const uint64_t rows = t.rows;
     b.key_ptype = storage_ptype(k.type);
     b.unique_keys = (k.has_unique && k.unique) ? 1 : 0;
-    b.n_slots = (uint32_t*)scratch(8);
-    memset_step(b.n_slots, 0, 8);
     bool dense = false;
     uint64_t span = 0;
     if (k.has_minmax) {
@@ -722,7 +720,9 @@ struct Compiler {
       memset_step(b.dense_bits, 0, ((span + 31) / 32) * 4);
     } else {
       b.kind = B_HASH;
-      b.capacity = std::max<uint64_t>(64, 2 * rows);
+      const double lf = tune_load_factor(ctx, "hash_build", rows);
+      P.load_keys.push_back({tune_key_load("hash_build", rows), rows});
+      b.capacity = std::max<uint64_t>(64, (uint64_t)std::ceil(lf * (double)rows));
       b.hash_keys = (int64_t*)scratch(b.capacity * 8);
       b.hash_slot = (uint32_t*)scratch(b.capacity * 4);
       b.hash_special = (uint32_t*)scratch(8);
@@ -1267,7 +1267,9 @@ struct Compiler {
       else if (rep_src >= 0) groups = std::max<uint64_t>(1, plan.sources[rep_src].table->rows);
       else {
         est_groups = estimate_groups();
-        groups = std::max<uint64_t>(64, est_groups * 2);
+        const double lf = tune_load_factor(ctx, "agg_table", est_groups);
+        P.load_keys.push_back({tune_key_load("agg_table", est_groups), est_groups});
+        groups = std::max<uint64_t>(64, (uint64_t)std::ceil(lf * (double)est_groups));
       }
       // a one-key hash table keeps one more group: the key equal to the
       // empty-slot sentinel
@@ -1300,13 +1302,14 @@ struct Compiler {
       pb.d.build_key_col = add_col(pb, s, up_col[s]);
       pb.d.build_payload_mask = pay;
       for (int q = 0; q < kMaxSrc; ++q)
-        if ((pay >> q) & 1u) {
+        if (q != s && ((pay >> q) & 1u)) {  // the build's own row is its slot
           builds[s].payload[q] = (uint32_t*)scratch(std::max<uint64_t>(1, plan.sources[s].table->rows) * 4);
           pb.d.builds[pb.d.sink_build].payload[q] = builds[s].payload[q];
         }
       if (s == rep_src) {
         fill_aggs(pb, false);
         slot_hit = (uint8_t*)scratch(std::max<uint64_t>(1, plan.sources[s].table->rows));
+        memset_step(slot_hit, 0, std::max<uint64_t>(1, plan.sources[s].table->rows));
         pb.d.slot_hit = slot_hit;
       }
       pb.d.status = P.status;
@@ -1408,7 +1411,7 @@ struct Compiler {
       fill_aggs(pb, true);
       push_pipeline(pb, root_rows);
       const uint64_t cap = std::max<uint64_t>(1, plan.sources[rep_src].table->rows);
-      const uint64_t* n_dev = (const uint64_t*)builds[rep_src].n_slots;
+      const uint64_t* n_dev = nullptr;  // slots are the build table's rows
       std::vector<FinalOut> fo;
       for (size_t i = 0; i < plan.outputs.size(); ++i) {
         const BOut& o = plan.outputs[i];
@@ -1424,7 +1427,7 @@ struct Compiler {
           Column* c = rep_column(*plan.group_keys[o.group_idx]);
           f.col = column_device(ctx, *c);
           pinned_cols.insert(c);
-          f.rid = builds[rep_src].payload[rep_src];
+          f.rid = nullptr;  // the group's slot is its row in the representative table
           fo.push_back(f);
         }
       }
@@ -1696,6 +1699,7 @@ std::unique_ptr<Program> compile(Ctx& ctx, const BoundPlan& plan) {
   try {
     c.compile();
     c.emit_fills();
+    tune_apply(ctx, *P);
   } catch (...) {
     for (void* b : P->blocks) ctx.arena.free(b);
     P->blocks.clear();

@@ -99,7 +99,7 @@ __device__ __forceinline__ void final_value(const FinalOut& f, uint64_t g, uint6
           __ddiv_rn(__longlong_as_double((long long)f.a[g]), __ull2double_rn(f.cnt[g])));
       break;
     case F_GATHER_COL: {
-      const uint32_t r = f.rid[g];
+      const uint32_t r = f.rid ? f.rid[g] : (uint32_t)g;  // null: g is the row itself
       lo = f.width == 4 ? (uint64_t)((const uint32_t*)f.col)[r] : ((const uint64_t*)f.col)[r];
       break;
     }

@@ -969,7 +969,12 @@ __global__ void __launch_bounds__(kThreads, (SINK == SK_AGG_SCALAR || SINK == SK
   const uint64_t n_warps = (uint64_t)gridDim.x * kWarps;
   uint64_t chunk_next = 0, chunk_end = 0;
   auto fetch = [&](uint64_t prev, bool first) -> uint64_t {
-    if (!dynamic_tiles) return first ? (uint64_t)blockIdx.x * kWarps + warp : prev + n_warps;
+    if (!dynamic_tiles) {
+      // groups of G consecutive tiles per warp, groups strided over the warps
+      const uint64_t G = d.tile_group > 1 ? (uint64_t)d.tile_group : 1;
+      if (first) return ((uint64_t)blockIdx.x * kWarps + warp) * G;
+      return (prev + 1) % G ? prev + 1 : prev + 1 + (n_warps - 1) * G;
+    }
     if (chunk_next < chunk_end) return chunk_next++;
     uint32_t t = 0;
     if (lane == 0) t = atomicAdd(d.tile_counter, (uint32_t)kTileFetch);
@@ -1229,7 +1234,8 @@ __global__ void __launch_bounds__(kThreads, (SINK == SK_AGG_SCALAR || SINK == SK
               if (fill)
                 for (int s = 0; s < kMaxSrc; ++s)
                   if ((fill >> s) & 1u)
-                    s_srid[(size_t)((slot_of_src >> (4 * s)) & 0xFu) * TILE + r[j]] = bd.payload[s][slot[j]];
+                    s_srid[(size_t)((slot_of_src >> (4 * s)) & 0xFu) * TILE + r[j]] =
+                        bd.payload[s] ? bd.payload[s][slot[j]] : slot[j];  // no array: the build's own row
             }
             const uint32_t m = __ballot_sync(0xFFFFFFFFu, keep[j]);
             if (keep[j]) sel_out[kept + __popc(m & lt)] = (uint16_t)r[j];
@@ -1358,22 +1364,19 @@ __global__ void __launch_bounds__(kThreads, (SINK == SK_AGG_SCALAR || SINK == SK
       }
     } else if (SINK == SK_BUILD) {
       const DBuild& bd = d.builds[d.sink_build];
-      // One slot reservation per warp-tile: its surviving rows take
-      // consecutive slots.
-      uint32_t sbase = 0;
-      if (lane == 0 && n_sel) sbase = atomicAdd(bd.n_slots, n_sel);
-      sbase = __shfl_sync(0xFFFFFFFFu, sbase, 0);
+      // A build row's slot is its row number in the build table: no shared
+      // counter to contend on, and the build's own row ids need no payload
+      // array (payload[drive_src] stays null).
       for (uint32_t i = lane; i < n_sel; i += 32) {
         const uint32_t r = ident ? i : (uint32_t)sel_in[i];
-        const uint32_t slot = sbase + i;
+        const uint32_t slot = (uint32_t)(tile_base + r);
         const int64_t key = tc_get(tc, d.build_key_col, r);
         for (int s = 0; s < kMaxSrc; ++s)
-          if ((d.build_payload_mask >> s) & 1u) bd.payload[s][slot] = tc_rid(tc, s, r);
+          if (s != d.drive_src && ((d.build_payload_mask >> s) & 1u)) bd.payload[s][slot] = tc_rid(tc, s, r);
         // A representative-row aggregate downstream keeps its states by
         // this slot: initialize them here, so the (build-table sized)
         // state arrays need no clearing per query.
         for (int a = 0; a < d.n_aggs; ++a) agg_init_global(d.aggs[a], slot);
-        if (d.slot_hit) d.slot_hit[slot] = 0;
         build_insert(bd, key, slot, st);
       }
     } else if ((SINK == SK_AGG_HASH || SINK == SK_AGG_SMEM) && d.table.cas) {
@@ -2012,8 +2015,12 @@ static cudaError_t launch_sink(const PipeDesc& d, uint64_t n_hint, cudaStream_t 
       g_occ[{SINK, smem}] = blocks_per_sm;
     }
   }
-  // Grid = resident CTAs per SM x SM count (a persistent grid-stride grid).
-  uint64_t tiles = (n_hint + (uint64_t)kTile * kWarps - 1) / ((uint64_t)kTile * kWarps);
+  // Grid = resident CTAs per SM x SM count (a persistent grid-stride
+  // grid); the autotuner may ask for fewer CTAs per SM and for groups of
+  // consecutive tiles per warp.
+  const uint64_t G = d.tile_group > 1 ? (uint64_t)d.tile_group : 1;
+  uint64_t tiles = (n_hint + (uint64_t)kTile * kWarps * G - 1) / ((uint64_t)kTile * kWarps * G);
+  if (d.grid_per_sm > 0 && d.grid_per_sm < blocks_per_sm) blocks_per_sm = d.grid_per_sm;
   uint64_t max_grid = (uint64_t)sm_count() * (uint64_t)blocks_per_sm;
   uint64_t grid = tiles < max_grid ? tiles : max_grid;
   if (grid == 0) grid = 1;

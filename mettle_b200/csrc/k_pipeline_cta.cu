@@ -949,7 +949,8 @@ __global__ void __launch_bounds__(kThreads) k_pipeline(const __grid_constant__ P
               if (fill)
                 for (int s = 0; s < kMaxSrc; ++s)
                   if ((fill >> s) & 1u)
-                    s_srid[(size_t)((slot_of_src >> (4 * s)) & 0xFu) * TILE + r[j]] = bd.payload[s][slot[j]];
+                    s_srid[(size_t)((slot_of_src >> (4 * s)) & 0xFu) * TILE + r[j]] =
+                        bd.payload[s] ? bd.payload[s][slot[j]] : slot[j];  // no array: the build's own row
             }
             m[j] = __ballot_sync(0xFFFFFFFFu, keep[j]);
             tot += __popc(m[j]);
@@ -1039,22 +1040,14 @@ __global__ void __launch_bounds__(kThreads) k_pipeline(const __grid_constant__ P
           for (uint32_t p = tid; p < lim; p += THREADS) d.out_rids[s][base + p] = tc_rid(tc, s, s_list[p]);
     } else if (SINK == SK_BUILD) {
       const DBuild& bd = d.builds[d.sink_build];
-      // One slot reservation per tile: the tile's surviving rows take
-      // consecutive slots.
-      if (tid == 0) s_base = n_sel ? (uint64_t)atomicAdd(bd.n_slots, n_sel) : 0;
-      __syncthreads();
-      const uint32_t sbase = (uint32_t)s_base;
+      // A build row's slot is its row number in the build table.
       for (uint32_t i = tid; i < n_sel; i += THREADS) {
         const uint32_t r = ident ? i : (uint32_t)sel_in[i];
-        const uint32_t slot = sbase + i;
+        const uint32_t slot = (uint32_t)(tc.base + r);
         const int64_t key = tc_get(tc, d.build_key_col, r);
         for (int s = 0; s < kMaxSrc; ++s)
-          if ((d.build_payload_mask >> s) & 1u) bd.payload[s][slot] = tc_rid(tc, s, r);
-        // A representative-row aggregate downstream keeps its states by
-        // this slot: initialize them here, so the (build-table sized)
-        // state arrays need no clearing per query.
+          if (s != d.drive_src && ((d.build_payload_mask >> s) & 1u)) bd.payload[s][slot] = tc_rid(tc, s, r);
         for (int a = 0; a < d.n_aggs; ++a) agg_init_global(d.aggs[a], slot);
-        if (d.slot_hit) d.slot_hit[slot] = 0;
         build_insert(bd, key, slot, st);
       }
     } else if ((SINK == SK_AGG_HASH || SINK == SK_AGG_SMEM) && d.table.cas) {
