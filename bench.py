@@ -682,10 +682,10 @@ def run_served(args):
                                       np.array_equal(res.columns[2], want["cnt"]))
             else:
                 parity_oracle &= bool(np.array_equal(res.columns[0], want))
-    # closed-loop plain capacity on a prefix of the stream sets the swept rates
-    pre = stream[: min(len(stream), 200)]
-    _, mk, _ = _run_stream(conn, pre, [0.0] * len(pre), served=False)
-    plain_cap = len(pre) / mk
+    # the closed-loop plain capacity on the whole stream (its full mix of
+    # templates and table sizes) sets the swept rates
+    _, mk, _ = _run_stream(conn, stream, [0.0] * len(stream), served=False)
+    plain_cap = len(stream) / mk
     rng = np.random.default_rng(11)
     sweep = []
     for factor in args.c5_rates:
@@ -751,7 +751,7 @@ def main():
     ap.add_argument("--impl", default="mettle", choices=["mettle", "reference"])
     ap.add_argument("--config", default="c4", choices=["c1", "c2", "c3", "c4", "c5"])
     ap.add_argument("--c5-queries", type=int, default=2000)
-    ap.add_argument("--c5-rates", type=float, nargs="+", default=[0.5, 1.0, 2.0])
+    ap.add_argument("--c5-rates", type=float, nargs="+", default=[0.25, 0.5, 0.75, 0.9])
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--scale", type=float, default=1.0, help="table size factor (profiling runs use a small case)")
     ap.add_argument("--keys", default="dense", choices=["dense", "sparse32", "sparse64"],

@@ -275,7 +275,10 @@ int mtl_debug_inject(mtl_ctx *ctx, int32_t what, uint32_t arg);
 typedef struct mtl_serve_stats {
   int64_t submitted, completed, rejected, in_flight, queued;
   int64_t admitted_bytes; /* processing-region bytes held by running requests */
-  int64_t batched_launches; /* graph replays that carried several small queries */
+  int64_t batched_launches; /* batches that carried several small queries */
+  int64_t program_reuses;   /* requests that reused a resident compiled program */
+  int64_t cached_programs;  /* compiled programs resident now */
+  int64_t graph_updates;    /* parameter updates of resident programs' CUDA graphs */
 } mtl_serve_stats;
 int mtl_serve_stats_get(mtl_ctx *ctx, mtl_serve_stats *out);
 /* Streams (slots) the serving loop may run concurrently (default 4). */

@@ -70,7 +70,8 @@ class CacheStats(C.Structure):
 
 class ServeStats(C.Structure):
     _fields_ = [(n, C.c_int64) for n in (
-        "submitted", "completed", "rejected", "in_flight", "queued", "admitted_bytes", "batched_launches")]
+        "submitted", "completed", "rejected", "in_flight", "queued", "admitted_bytes", "batched_launches",
+        "program_reuses", "cached_programs", "graph_updates")]
 
 
 # (name, restype, argtypes) of every exported entry point

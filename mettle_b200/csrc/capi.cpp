@@ -33,6 +33,7 @@ void serve_free(Request* r);
 void serve_stats(Ctx& ctx, mtl_serve_stats* out);
 int serve_set_slots(Ctx& ctx, int slots);
 void serve_wake(Ctx& ctx);
+void serve_drop_programs(Ctx& ctx);
 }  // namespace mtl
 
 using namespace mtl;
@@ -623,6 +624,7 @@ int mtl_cache_reset(mtl_ctx* ctx) {
   if (!ctx) return MTL_NOT_INITIALIZED;
   return guarded([&] {
     Ctx& c = ctx->c;
+    serve_drop_programs(c);  // resident compiled programs release their columns
     std::lock_guard<std::recursive_mutex> g(c.mu);
     c.qcache.clear();
     c.grouped_topk_entries = 0;

@@ -279,6 +279,9 @@ struct PipeDesc {
   // 256 rows)
   int32_t grid_per_sm;
   int32_t tile_group;
+  // SK_MATERIALIZE: 0 = 1024-row CTA tiles (k_pipeline_cta.cu), 1 = 256-row
+  // warp tiles, each warp with its own look-back (k_pipeline.cu)
+  int32_t mat_warp_tiles;
 
   uint32_t* status;                 // DevStatus bits
 };

@@ -197,6 +197,7 @@ struct Step {
   // PIPELINE
   PipeDesc pipe;
   uint64_t n_hint = 0;
+  std::vector<int> pred_filter;  // BoundPlan filter behind each of pipe.preds
   // COMPACT_*
   const void* flag = nullptr;
   uint64_t n = 0;
@@ -258,6 +259,8 @@ struct Program {
   cudaGraphExec_t graph = nullptr;
   // autotuner keys of the capacities (hash load factors) this compile chose
   std::vector<std::pair<std::string, uint64_t>> load_keys;
+  int64_t graph_updates = 0;  // parameter updates of the instantiated graph
+  std::string agg_strategy_key;  // autotuner key of a one-key aggregate's strategy ("" none)
   ~Program();
 };
 
@@ -355,7 +358,12 @@ void column_distinct(Ctx& ctx, Table& t, Column& c);
 // planning / execution (exec.cpp)
 std::unique_ptr<Program> compile(Ctx& ctx, const BoundPlan& plan);
 void run_program(Ctx& ctx, Program& p, cudaStream_t s);
-void run_program_graph(Ctx& ctx, Program& p, cudaStream_t s);
+void run_program_graph(Ctx& ctx, Program& p, cudaStream_t s, bool refresh = false);
+// Program reuse across queries of one shape (serving): the plan's shape
+// (all but its filter literals) and the literals written into a program
+// compiled for that shape.
+std::string plan_shape(const BoundPlan& p);
+void patch_literals(Program& p, const BoundPlan& plan);
 std::shared_ptr<Result> fetch_program(Ctx& ctx, Program& p, cudaStream_t s);
 void free_program(Ctx& ctx, Program& p);
 std::shared_ptr<Result> constant_result(const BoundPlan& plan);
@@ -366,6 +374,10 @@ std::string tune_key_pipeline(const Step& s);
 std::string tune_key_load(const char* what, uint64_t rows);
 void tune_apply(Ctx& ctx, Program& p);
 double tune_load_factor(Ctx& ctx, const char* what, uint64_t rows);
+// One-key aggregate over few groups: 0 planner default, 1 one pass into
+// shared-memory tables, 2 partitioned passes.
+std::string tune_key_agg(uint64_t groups, uint64_t rows);
+int tune_agg_strategy(Ctx& ctx, uint64_t groups, uint64_t rows);
 std::string tune_file_path(const Ctx& ctx);
 std::string autotune(Ctx& ctx, const BoundPlan& plan, int reps);
 

@@ -525,6 +525,7 @@ struct Compiler {
     PipeDesc d;
     std::map<std::pair<int, const Column*>, int> colmap;
     std::vector<double> op_sel;  // estimated pass fraction of each op
+    std::vector<int> pred_filter;  // plan filter of each predicate
     PipeBuilder() {
       memset(&d, 0, sizeof(d));
       d.first_col = -1;
@@ -740,7 +741,8 @@ struct Compiler {
   int state_stride = 1;    // words between groups in the aggregate states
 
   void add_filters(PipeBuilder& pb, int s) {
-    for (const BFilter& f : plan.filters) {
+    for (size_t fi = 0; fi < plan.filters.size(); ++fi) {
+      const BFilter& f = plan.filters[fi];
       if (f.src != s) continue;
       if (pb.d.n_preds >= kMaxPreds) fail(MTL_UNSUPPORTED, "too many predicates on one table");
       int pi = pb.d.n_preds++;
@@ -753,6 +755,7 @@ struct Compiler {
       pb.d.ops[pb.d.n_ops].idx = pi;
       pb.d.n_ops++;
       pb.op_sel.push_back(estimate_selectivity(f));
+      pb.pred_filter.push_back((int)fi);
     }
   }
 
@@ -871,6 +874,7 @@ struct Compiler {
     s.k = Step::PIPELINE;
     s.pipe = pb.d;
     s.n_hint = n_hint;
+    s.pred_filter = pb.pred_filter;
     s.name = std::string("pipeline:") + sinks[pb.d.sink] + ":" + plan.sources[pb.d.drive_src].name;
     P.steps.push_back(s);
     P.kernels += 1;
@@ -887,8 +891,8 @@ struct Compiler {
   // qualify: few groups, a 128-bit input, more distinct inputs than a record
   // holds, more partitions than the count pass supports, or records that do
   // not fit the scratch region. On success pb.d.sink is SK_PART_COUNT.
-  bool push_partitioned(PipeBuilder& pb, uint64_t est, uint64_t rows) {
-    if (est <= 8 || rows == 0 || rows >= (1ull << 31)) return false;
+  bool push_partitioned(PipeBuilder& pb, uint64_t est, uint64_t rows, bool forced = false) {
+    if ((est <= 8 && !forced) || rows == 0 || rows >= (1ull << 31)) return false;
     PipeDesc d = pb.d;
     int nv = 0;
     int slot_prog[kMaxAggs];
@@ -1351,7 +1355,9 @@ struct Compiler {
       pb.d.mat_src_mask = m;
       pb.d.out_count = (uint64_t*)scratch(8);
       pb.d.out_capacity = n_max;
-      const uint64_t tiles = (n_max + pipeline_tile_rows() - 1) / pipeline_tile_rows();
+      // look-back words for the smaller (warp) tiles, so that either kernel
+      // can run the step
+      const uint64_t tiles = (n_max + pipeline_warp_tile_rows() - 1) / pipeline_warp_tile_rows();
       pb.d.tile_status = (uint64_t*)scratch(std::max<uint64_t>(tiles, 1) * 8);
       pb.d.tile_counter = (uint32_t*)scratch(8);
       pb.d.epoch = 1;
@@ -1485,7 +1491,11 @@ struct Compiler {
     // CTA's most frequent keys (the first to arrive), so a skewed key's rows
     // meet in shared memory instead of contending on one global entry.
     pb.d.sink = SK_AGG_HASH;
-    if (cas_table && push_partitioned(pb, est_groups, root_rows)) {
+    // one-key aggregates whose groups all fit a CTA's shared-memory table
+    // may run either way; the autotuner's measured choice decides
+    const int strategy = cas_table && est_groups <= 1536 ? tune_agg_strategy(ctx, est_groups, root_rows) : 0;
+    P.agg_strategy_key = cas_table && est_groups <= 1536 ? tune_key_agg(est_groups, root_rows) : "";
+    if (cas_table && strategy != 1 && push_partitioned(pb, est_groups, root_rows, strategy == 2)) {
       // count, scan, scatter and per-partition aggregation are queued
     } else if (cas_table) {
       pb.d.sink = SK_AGG_SMEM;
@@ -1731,14 +1741,17 @@ Program::~Program() {
 
 // Replays the program as one CUDA graph (captured on first use). Falls back
 // to direct launches when the stream cannot be captured (the legacy default
-// stream) or when per-step profiling is on.
-void run_program_graph(Ctx& ctx, Program& p, cudaStream_t s) {
+// stream) or when per-step profiling is on. With `refresh`, the program's
+// steps changed since the graph was made (new filter literals): they are
+// captured again and the instantiated graph takes their parameters in place
+// (cudaGraphExecUpdate), which costs far less than a new instantiation.
+void run_program_graph(Ctx& ctx, Program& p, cudaStream_t s, bool refresh) {
   static const bool disabled = std::getenv("METTLE_NO_GRAPH") != nullptr;
   if (p.profile || disabled || s == nullptr || s == cudaStreamLegacy || s == cudaStreamPerThread) {
     run_program(ctx, p, s);
     return;
   }
-  if (!p.graph) {
+  if (!p.graph || refresh) {
     cudaGraph_t g = nullptr;
     if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
       cudaGetLastError();
@@ -1754,7 +1767,19 @@ void run_program_graph(Ctx& ctx, Program& p, cudaStream_t s) {
       throw;
     }
     CK(cudaStreamEndCapture(s, &g));
-    cudaError_t e = cudaGraphInstantiate(&p.graph, g, 0);
+    bool updated = false;
+    if (p.graph) {
+      cudaGraphExecUpdateResultInfo info;
+      if (cudaGraphExecUpdate(p.graph, g, &info) == cudaSuccess) {
+        updated = true;
+        p.graph_updates++;
+      } else {
+        cudaGetLastError();
+        cudaGraphExecDestroy(p.graph);
+        p.graph = nullptr;
+      }
+    }
+    cudaError_t e = updated ? cudaSuccess : cudaGraphInstantiate(&p.graph, g, 0);
     cudaGraphDestroy(g);
     if (e != cudaSuccess) {
       cudaGetLastError();
@@ -1764,6 +1789,42 @@ void run_program_graph(Ctx& ctx, Program& p, cudaStream_t s) {
     }
   }
   CK(cudaGraphLaunch(p.graph, s));
+}
+
+// Shape of a bound plan: everything that decides the compiled program
+// except the filter literals, which patch_literals writes into a compiled
+// program of the same shape.
+std::string plan_shape(const BoundPlan& p) {
+  std::string o;
+  auto add = [&](const std::string& x) {
+    o += x;
+    o += '\x1f';
+  };
+  for (auto& s : p.sources)
+    add("S" + s.name + "@" + std::to_string((uintptr_t)s.table.get()) + "v" + std::to_string(s.table->version));
+  for (auto& f : p.filters) add("F" + std::to_string(f.src) + "." + f.col->name + "#" + std::to_string(f.op));
+  for (auto& j : p.joins)
+    add("J" + std::to_string(j.ls) + "." + j.lc->name + "=" + std::to_string(j.rs) + "." + j.rc->name);
+  add(p.is_agg ? "agg" : "rows");
+  for (auto& k : p.group_keys) add("G" + k->text);
+  for (auto& a : p.aggs) add("A" + std::to_string(a.fn) + "(" + (a.arg ? a.arg->text : "*") + ")");
+  for (auto& x : p.outputs)
+    add("O" + x.name + ":" + type_name(x.type) + ":" + (x.expr ? x.expr->text : "") + ":" +
+        std::to_string(x.group_idx) + "/" + std::to_string(x.agg_idx) + (x.hidden ? "h" : ""));
+  for (auto& r : p.order) add("R" + std::to_string(r.out) + (r.desc ? "d" : "a"));
+  add("L" + std::to_string(p.limit) + (p.constant_only ? "c" : ""));
+  return o;
+}
+
+void patch_literals(Program& P, const BoundPlan& plan) {
+  for (Step& s : P.steps) {
+    if (s.k != Step::PIPELINE) continue;
+    for (size_t j = 0; j < s.pred_filter.size() && j < (size_t)kMaxPreds; ++j) {
+      const BFilter& f = plan.filters[s.pred_filter[j]];
+      s.pipe.preds[j].ilit = f.ilit;
+      s.pipe.preds[j].flit = f.flit;
+    }
+  }
 }
 
 static const char* step_kind_name(Step::Kind k) {

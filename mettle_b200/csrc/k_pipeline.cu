@@ -2031,6 +2031,7 @@ static cudaError_t launch_sink(const PipeDesc& d, uint64_t n_hint, cudaStream_t 
 }
 
 int part_max_bits() { return kMaxPartBits; }
+size_t pipeline_warp_tile_rows() { return kTile; }
 int part_max_values() { return kPartMaxVals; }
 
 // Both partition passes run this many CTAs (they must cover the same tiles):
@@ -2070,7 +2071,8 @@ cudaError_t launch_pipeline(const PipeDesc& d, uint64_t n_hint, cudaStream_t s) 
   if (d.tuple_input) return cudaErrorInvalidValue;  // every pipeline scans a base table
   switch (d.sink) {
     case SK_BUILD: return launch_sink<SK_BUILD>(d, n_hint, s);
-    case SK_MATERIALIZE: return launch_pipeline_materialize(d, n_hint, s);
+    case SK_MATERIALIZE:
+      return d.mat_warp_tiles ? launch_sink<SK_MATERIALIZE>(d, n_hint, s) : launch_pipeline_materialize(d, n_hint, s);
     case SK_AGG_HASH: return launch_sink<SK_AGG_HASH>(d, n_hint, s);
     case SK_AGG_SMEM: return launch_sink<SK_AGG_SMEM>(d, n_hint, s);
     case SK_AGG_SLOT: return launch_sink<SK_AGG_SLOT>(d, n_hint, s);

@@ -1341,7 +1341,9 @@ static cudaError_t launch_sink(const PipeDesc& d, uint64_t n_hint, cudaStream_t 
       g_occ[{SINK, smem}] = blocks_per_sm;
     }
   }
-  // Grid = resident CTAs per SM x SM count (a persistent grid-stride grid).
+  // Grid = resident CTAs per SM x SM count (a persistent grid-stride grid);
+  // the autotuner may ask for fewer CTAs per SM.
+  if (d.grid_per_sm > 0 && d.grid_per_sm < blocks_per_sm) blocks_per_sm = d.grid_per_sm;
   uint64_t tiles = (n_hint + kTile - 1) / kTile;
   uint64_t max_grid = (uint64_t)sm_count() * (uint64_t)blocks_per_sm;
   uint64_t grid = tiles < max_grid ? tiles : max_grid;

@@ -11,6 +11,7 @@ namespace mtl {
 
 // ---- pipeline (k_pipeline.cu)
 size_t pipeline_tile_rows();
+size_t pipeline_warp_tile_rows();  // rows of a warp-tile (k_pipeline.cu)
 size_t pipeline_smem_bytes(const PipeDesc& d);
 // n_hint bounds the tuples (grid sizing when the count lives on the device).
 cudaError_t launch_pipeline(const PipeDesc& d, uint64_t n_hint, cudaStream_t s);

@@ -8,9 +8,19 @@
 // the requests already running (its compile step allocates from the region
 // arena; on a shortfall it waits for running requests to release memory, and
 // is rejected only if it cannot fit even alone). Small requests (root table
-// at most kSmallRows rows) that are queued together are compiled together
-// and launched as one captured CUDA graph, which removes the per-kernel
-// launch cost that dominates small queries.
+// at most kSmallRows rows) that are queued together are taken as one batch
+// by one worker and launched back to back on its stream.
+//
+// Compiled programs stay resident between requests: a finished request's
+// program (its device scratch, its descriptors and its instantiated CUDA
+// graph) is kept, keyed by the shape of its plan (everything but the filter
+// literals). A later request of the same shape takes the idle program,
+// gets its literals patched into the pipeline descriptors, and replays the
+// graph after a parameter update (cudaGraphExecUpdate): no parse-to-launch
+// compilation, no descriptor uploads, no graph instantiation. Idle programs
+// are evicted (least recently used first) when a new compile needs their
+// memory, and the cache holds at most kMaxPrograms programs and half the
+// processing region.
 #include <chrono>
 #include <cstring>
 
@@ -20,6 +30,18 @@ namespace mtl {
 
 constexpr uint64_t kSmallRows = 1ull << 20;
 constexpr int kBatchMax = 16;
+constexpr size_t kMaxPrograms = 48;
+
+// A compiled program kept for reuse by later requests of the same shape.
+struct CachedProgram {
+  std::string shape;
+  std::unique_ptr<Program> prog;
+  // the tables the program reads: kept alive while it is cached (their
+  // device columns stay pinned); a table replaced since makes it stale
+  std::vector<std::shared_ptr<Table>> tables;
+  bool busy = false;
+  uint64_t last_use = 0;
+};
 
 struct Request {
   std::string sql;
@@ -33,7 +55,10 @@ struct Request {
   bool small = false;
   // compiled state while running
   BoundPlan plan;
-  std::unique_ptr<Program> prog;
+  std::unique_ptr<Program> prog;    // compiled for this request
+  CachedProgram* cached = nullptr;  // or borrowed from the program cache
+  std::string shape;
+  Program* program() { return cached ? cached->prog.get() : prog.get(); }
 };
 
 struct ServeState {
@@ -45,7 +70,43 @@ struct ServeState {
   bool stop = false;
   int slots = 4;
   std::atomic<int64_t> submitted{0}, completed{0}, rejected{0}, in_flight{0}, admitted_bytes{0}, batched{0};
+  std::atomic<int64_t> reuses{0};
+  // program cache (guarded by mu)
+  std::list<CachedProgram> programs;
+  uint64_t program_bytes = 0;
+  uint64_t tick = 0;
 };
+
+static void drop_locked(Ctx& ctx, ServeState& S, std::list<CachedProgram>::iterator it) {
+  S.program_bytes -= it->prog->scratch_bytes;
+  free_program(ctx, *it->prog);
+  S.programs.erase(it);
+}
+
+// Frees idle cached programs that read a table replaced or dropped since.
+static void evict_stale_locked(Ctx& ctx, ServeState& S) {
+  std::lock_guard<std::recursive_mutex> g(ctx.mu);
+  for (auto it = S.programs.begin(); it != S.programs.end();) {
+    bool stale = false;
+    for (auto& t : it->tables) {
+      auto cur = ctx.tables.find(t->name);
+      stale |= cur == ctx.tables.end() || cur->second != t;
+    }
+    auto nx = std::next(it);
+    if (stale && !it->busy) drop_locked(ctx, S, it);
+    it = nx;
+  }
+}
+
+// Frees the least recently used idle cached program; false when none is idle.
+static bool evict_one_locked(Ctx& ctx, ServeState& S) {
+  auto victim = S.programs.end();
+  for (auto it = S.programs.begin(); it != S.programs.end(); ++it)
+    if (!it->busy && (victim == S.programs.end() || it->last_use < victim->last_use)) victim = it;
+  if (victim == S.programs.end()) return false;
+  drop_locked(ctx, S, victim);
+  return true;
+}
 
 static void finish(ServeState& S, Request* r, int status, const std::string& err) {
   {
@@ -76,6 +137,24 @@ static bool prepare(Ctx& ctx, ServeState& S, Request* r) {
       finish(S, r, MTL_OK, "");
       return false;
     }
+    r->shape = plan_shape(r->plan);
+    {
+      std::lock_guard<std::mutex> lk(S.mu);
+      evict_stale_locked(ctx, S);
+      for (CachedProgram& c : S.programs)
+        if (!c.busy && c.shape == r->shape) {
+          c.busy = true;
+          c.last_use = ++S.tick;
+          r->cached = &c;
+          break;
+        }
+    }
+    if (r->cached) {
+      patch_literals(*r->cached->prog, r->plan);
+      S.reuses++;
+      S.admitted_bytes += (int64_t)r->cached->prog->scratch_bytes;
+      return true;
+    }
     for (;;) {
       try {
         r->prog = compile(ctx, r->plan);
@@ -84,9 +163,12 @@ static bool prepare(Ctx& ctx, ServeState& S, Request* r) {
       } catch (const EngineError& e) {
         if (e.code != MTL_BUDGET_EXCEEDED) throw;
         std::unique_lock<std::mutex> lk(S.mu);
+        // idle cached programs give their memory back first
+        if (evict_one_locked(ctx, S)) continue;
         // Only this request holds no memory: it can never fit.
         if (S.admitted_bytes.load() == 0) throw;
-        S.cv.wait_for(lk, std::chrono::milliseconds(20));
+        // woken when a running request releases its memory
+        S.cv.wait_for(lk, std::chrono::milliseconds(500));
         if (S.stop) throw;
       }
     }
@@ -98,15 +180,42 @@ static bool prepare(Ctx& ctx, ServeState& S, Request* r) {
   return false;
 }
 
-static void release(Ctx& ctx, ServeState& S, Request* r) {
-  if (r->prog) {
-    S.admitted_bytes -= (int64_t)r->prog->scratch_bytes;
-    free_program(ctx, *r->prog);
-    r->prog.reset();
+// Returns a request's program: a borrowed one goes back to the cache idle; a
+// fresh one joins the cache when there is room, else it is freed.
+static void release(Ctx& ctx, ServeState& S, Request* r, bool ok) {
+  std::unique_lock<std::mutex> lk(S.mu);
+  if (r->cached) {
+    S.admitted_bytes -= (int64_t)r->cached->prog->scratch_bytes;
+    r->cached->busy = false;
+    r->cached->last_use = ++S.tick;
+    r->cached = nullptr;
+  } else if (r->prog) {
+    const uint64_t b = r->prog->scratch_bytes;
+    S.admitted_bytes -= (int64_t)b;
+    const uint64_t cap = ctx.budgets.processing_region_bytes / 2;
+    while (ok && (S.programs.size() >= kMaxPrograms || S.program_bytes + b > cap) && evict_one_locked(ctx, S)) {
+    }
+    if (ok && S.programs.size() < kMaxPrograms && S.program_bytes + b <= cap) {
+      S.programs.emplace_back();
+      CachedProgram& c = S.programs.back();
+      c.shape = r->shape;
+      c.prog = std::move(r->prog);
+      for (const Source& src : r->plan.sources) c.tables.push_back(src.table);
+      c.last_use = ++S.tick;
+      S.program_bytes += b;
+    } else {
+      free_program(ctx, *r->prog);
+      r->prog.reset();
+    }
   }
+  lk.unlock();
   S.cv.notify_all();
 }
 
+// Runs a batch on the worker's stream: every request's program is enqueued
+// back to back (a reused program replays its graph after a parameter
+// update; a fresh one is launched directly and captured when it is reused),
+// then the results are fetched in order.
 static void run_batch(Ctx& ctx, ServeState& S, std::vector<Request*>& batch, cudaStream_t s) {
   std::vector<Request*> ready;
   for (Request* r : batch)
@@ -115,45 +224,18 @@ static void run_batch(Ctx& ctx, ServeState& S, std::vector<Request*>& batch, cud
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
-  bool graphed = false;
   try {
-    if (ready.size() > 1) {
-      // One captured graph for the whole batch.
-      cudaGraph_t graph = nullptr;
-      cudaGraphExec_t exec = nullptr;
-      if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
-        bool ok = true;
-        try {
-          for (Request* r : ready) run_program(ctx, *r->prog, s);
-        } catch (...) {
-          ok = false;
-        }
-        if (cudaStreamEndCapture(s, &graph) != cudaSuccess) ok = false;
-        if (ok && cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess) {
-          cudaEventRecord(e0, s);
-          if (cudaGraphLaunch(exec, s) == cudaSuccess) graphed = true;
-          cudaEventRecord(e1, s);
-        }
-        cudaGetLastError();
-        if (graph) cudaGraphDestroy(graph);
-        if (exec) {
-          cudaStreamSynchronize(s);
-          cudaGraphExecDestroy(exec);
-        }
-      } else {
-        cudaGetLastError();
-      }
-      if (graphed) S.batched++;
+    cudaEventRecord(e0, s);
+    for (Request* r : ready) {
+      if (r->cached) run_program_graph(ctx, *r->program(), s, /*refresh=*/true);
+      else run_program(ctx, *r->program(), s);
     }
-    if (!graphed) {
-      cudaEventRecord(e0, s);
-      for (Request* r : ready) run_program(ctx, *r->prog, s);
-      cudaEventRecord(e1, s);
-    }
+    cudaEventRecord(e1, s);
+    if (ready.size() > 1) S.batched++;
   } catch (const EngineError& e) {
     cudaStreamSynchronize(s);
     for (Request* r : ready) {
-      release(ctx, S, r);
+      release(ctx, S, r, false);
       finish(S, r, e.code, e.what());
     }
     cudaEventDestroy(e0);
@@ -163,15 +245,13 @@ static void run_batch(Ctx& ctx, ServeState& S, std::vector<Request*>& batch, cud
   float ms = 0;
   for (Request* r : ready) {
     try {
-      r->result = fetch_program(ctx, *r->prog, s);
-      if (ms == 0) {
-        cudaEventElapsedTime(&ms, e0, e1);
-      }
+      r->result = fetch_program(ctx, *r->program(), s);
+      if (ms == 0) cudaEventElapsedTime(&ms, e0, e1);
       r->result->device_ms = ms / (float)ready.size();
-      release(ctx, S, r);
+      release(ctx, S, r, true);
       finish(S, r, MTL_OK, "");
     } catch (const EngineError& e) {
-      release(ctx, S, r);
+      release(ctx, S, r, false);
       finish(S, r, e.code, e.what());
     }
   }
@@ -226,6 +306,11 @@ void serve_shutdown(Ctx& ctx) {
   }
   S.cv.notify_all();
   for (auto& t : S.workers) t.join();
+  for (cudaStream_t s : S.streams) cudaStreamSynchronize(s);
+  {
+    std::lock_guard<std::mutex> g(S.mu);
+    while (!S.programs.empty()) drop_locked(ctx, S, S.programs.begin());
+  }
   for (cudaStream_t s : S.streams) cudaStreamDestroy(s);
   delete ctx.serve;
   ctx.serve = nullptr;
@@ -309,14 +394,39 @@ void serve_stats(Ctx& ctx, mtl_serve_stats* out) {
   }
   out->admitted_bytes = S.admitted_bytes;
   out->batched_launches = S.batched;
+  out->program_reuses = S.reuses;
+  {
+    std::lock_guard<std::mutex> g(S.mu);
+    out->cached_programs = (int64_t)S.programs.size();
+    for (auto& c : S.programs) out->graph_updates += c.prog->graph_updates;
+  }
 }
 
-// Wakes the workers (after a change of the queue-holding injection).
+// Wakes the workers (after a change of the queue-holding injection). The
+// serving state's lock is taken without the context's (the workers take
+// them in the other order).
 void serve_wake(Ctx& ctx) {
-  std::lock_guard<std::recursive_mutex> g(ctx.mu);
-  if (!ctx.serve) return;
-  { std::lock_guard<std::mutex> q(ctx.serve->mu); }
-  ctx.serve->cv.notify_all();
+  ServeState* S;
+  {
+    std::lock_guard<std::recursive_mutex> g(ctx.mu);
+    S = ctx.serve;
+  }
+  if (!S) return;
+  { std::lock_guard<std::mutex> q(S->mu); }
+  S->cv.notify_all();
+}
+
+// Frees every idle resident program (gpu_cache_reset).
+void serve_drop_programs(Ctx& ctx) {
+  ServeState* S;
+  {
+    std::lock_guard<std::recursive_mutex> g(ctx.mu);
+    S = ctx.serve;
+  }
+  if (!S) return;
+  std::lock_guard<std::mutex> q(S->mu);
+  while (evict_one_locked(ctx, *S)) {
+  }
 }
 
 int serve_set_slots(Ctx& ctx, int slots) {

@@ -113,6 +113,24 @@ static void tune_store(Ctx& ctx, const std::string& key, double a, double b) {
   ctx.tune[key] = {a, b};
 }
 
+// A pipeline step's launch shape: CTAs per SM (0: as many as fit) and the
+// rows a warp takes per step. Order-preserving compaction runs 1024-row CTA
+// tiles or 256-row warp tiles; the other sinks take groups of 256-row tiles.
+static void set_shape(Step& s, int grid_per_sm, int tile_rows) {
+  s.pipe.grid_per_sm = grid_per_sm;
+  if (s.pipe.sink == SK_MATERIALIZE) {
+    s.pipe.mat_warp_tiles = tile_rows == 256 ? 1 : 0;
+  } else {
+    const int g = tile_rows / 256;
+    s.pipe.tile_group = g == 2 || g == 4 ? g : 1;
+  }
+}
+
+static std::vector<int> tile_candidates(const Step& s) {
+  if (s.pipe.sink == SK_MATERIALIZE) return {1024, 256};
+  return {256, 512, 1024};
+}
+
 // Applies the table's launch shapes to a compiled program's pipelines. The
 // two partition passes must cover the same tiles per CTA, so they keep the
 // default shape.
@@ -121,10 +139,7 @@ void tune_apply(Ctx& ctx, Program& p) {
     if (s.k != Step::PIPELINE) continue;
     if (s.pipe.sink == SK_PART_COUNT || s.pipe.sink == SK_PART_SCATTER) continue;
     double a = 0, b = 0;
-    if (tune_lookup(ctx, tune_key_pipeline(s), &a, &b)) {
-      s.pipe.grid_per_sm = (int32_t)a;
-      s.pipe.tile_group = (int32_t)b;
-    }
+    if (tune_lookup(ctx, tune_key_pipeline(s), &a, &b)) set_shape(s, (int)a, (int)b);
   }
 }
 
@@ -136,6 +151,20 @@ double tune_load_factor(Ctx& ctx, const char* what, uint64_t rows) {
   double a = 0, b = 0;
   if (tune_lookup(ctx, tune_key_load(what, rows), &a, &b) && a >= 1.25 && a <= 8) return a;
   return 2.0;
+}
+
+std::string tune_key_agg(uint64_t groups, uint64_t rows) {
+  return "agg_one_key/g" + std::to_string(log2_class(groups)) + "/n" + std::to_string(log2_class(rows));
+}
+
+// A strategy forced by the tuning run of this thread (0: none).
+static thread_local int t_force_agg_strategy = 0;
+
+int tune_agg_strategy(Ctx& ctx, uint64_t groups, uint64_t rows) {
+  if (t_force_agg_strategy) return t_force_agg_strategy;
+  double a = 0, b = 0;
+  if (tune_lookup(ctx, tune_key_agg(groups, rows), &a, &b) && (a == 1 || a == 2)) return (int)a;
+  return 0;
 }
 
 // ------------------------------------------------------------ tuning runs
@@ -214,6 +243,44 @@ std::string autotune(Ctx& ctx, const BoundPlan& plan, int reps) {
     for (auto& k : load_keys) tune_store(ctx, k.first, best_lf, 0);
     rep << "chose load factor " << best_lf << "\n";
   }
+  // one-key aggregate over few groups: one pass into shared-memory tables
+  // against the partitioned passes
+  std::string agg_key;
+  {
+    auto probe = compile(ctx, plan);
+    agg_key = probe->agg_strategy_key;
+    free_program(ctx, *probe);
+  }
+  if (!agg_key.empty()) {
+    double best_t = 1e30;
+    int best = 2;
+    for (int strat : {1, 2}) {
+      t_force_agg_strategy = strat;
+      std::unique_ptr<Program> p;
+      try {
+        p = compile(ctx, plan);
+      } catch (...) {
+        t_force_agg_strategy = 0;
+        throw;
+      }
+      t_force_agg_strategy = 0;
+      double t = 1e30;
+      try {
+        t = total(run_steps(ctx, *p, s, reps));
+      } catch (...) {
+        free_program(ctx, *p);
+        throw;
+      }
+      free_program(ctx, *p);
+      rep << "one-key aggregate " << (strat == 1 ? "in shared memory (one pass)" : "partitioned") << ": " << t
+          << " ms\n";
+      if (t < best_t) {
+        best_t = t;
+        best = strat;
+      }
+    }
+    tune_store(ctx, agg_key, best, 0);
+  }
   // launch shapes, one pipeline step at a time
   auto p = compile(ctx, plan);
   try {
@@ -222,24 +289,22 @@ std::string autotune(Ctx& ctx, const BoundPlan& plan, int reps) {
       Step& st = p->steps[i];
       if (st.k != Step::PIPELINE || st.pipe.sink == SK_PART_COUNT || st.pipe.sink == SK_PART_SCATTER) continue;
       double best_t = 1e30;
-      int best_g = 0, best_tg = 1;
+      int best_g = 0, best_rows = tile_candidates(st)[0];
       for (int g : {0, 1, 2, 3, 4}) {  // 0: as many as fit
-        for (int tg : {1, 2, 4}) {
-          st.pipe.grid_per_sm = g;
-          st.pipe.tile_group = tg;
+        for (int rows : tile_candidates(st)) {
+          set_shape(st, g, rows);
           const double t = run_steps(ctx, *p, s, reps)[i];
-          if (t < best_t * 0.995) {  // ties keep the simpler (earlier) shape
+          if (t < best_t * 0.995) {  // ties keep the earlier (default) shape
             best_t = t;
             best_g = g;
-            best_tg = tg;
+            best_rows = rows;
           }
         }
       }
-      st.pipe.grid_per_sm = best_g;
-      st.pipe.tile_group = best_tg;
-      tune_store(ctx, tune_key_pipeline(st), best_g, best_tg);
+      set_shape(st, best_g, best_rows);
+      tune_store(ctx, tune_key_pipeline(st), best_g, best_rows);
       rep << st.name << " [" << tune_key_pipeline(st) << "]: ctas_per_sm " << (best_g ? std::to_string(best_g) : "max")
-          << ", tile " << 256 * best_tg << " rows per warp step, " << best_t << " ms\n";
+          << ", tile " << best_rows << " rows, " << best_t << " ms\n";
     }
   } catch (...) {
     free_program(ctx, *p);

@@ -44,7 +44,7 @@ def test_autotune_writes_a_table_that_later_queries_use(tmp_path, monkeypatch, b
     for line in lines:
         key, a, b = line.split()
         if key.startswith("pipeline:"):
-            forced.append(f"{key} 1 4")
+            forced.append(f"{key} 1 1024")  # one CTA per SM, 1024 rows per warp step
         else:
             forced.append(f"{key} 1.5 0")
     path.write_text("\n".join(forced) + "\n")
@@ -71,9 +71,9 @@ def test_autotuned_shapes_keep_group_by_and_scan_exact(tmp_path, monkeypatch, bu
         conn.gpu_register_table("t")
         report = conn.autotune(W.C3_SQL, reps=1)
         assert re.search(r"pipeline:agg_\w+", report)
-    for tg in (2, 4):
+    for rows in (512, 1024):
         text = path.read_text()
-        path.write_text(re.sub(r"^(pipeline:\S+) \S+ \S+$", rf"\1 1 {tg}", text, flags=re.M))
+        path.write_text(re.sub(r"^(pipeline:\S+) \S+ \S+$", rf"\1 1 {rows}", text, flags=re.M))
         with Connection() as conn:
             conn.execute("CALL gpu_buffer_init('2 GB', '2 GB')")
             conn.create_table("t", {"k": (L.T_BIGINT, d["k"]), "v": (L.T_BIGINT, d["v"]),
@@ -82,3 +82,38 @@ def test_autotuned_shapes_keep_group_by_and_scan_exact(tmp_path, monkeypatch, bu
             r = conn.gpu_processing(W.C3_SQL)
             want = orc.groupby_c3(d["k"], d["v"], d["f"], limit=100)
             assert np.array_equal(r.columns[0], want["k"]) and np.array_equal(r.columns[2], want["cnt"])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("warp_tiles", [False, True])
+def test_materialize_tile_shapes_keep_row_order(tmp_path, monkeypatch, built_lib, warp_tiles):
+    """Order-preserving compaction with 1024-row CTA tiles or 256-row warp
+    tiles (each warp with its own look-back): the same rows in the same
+    order, bit-exact against the oracle."""
+    import numpy as np
+    from mettle_b200 import _lib as L
+    path = tmp_path / "tune.txt"
+    monkeypatch.setenv("METTLE_TUNE_FILE", str(path))
+    d = W.scan(3_000_000, seed_salt=4)
+    sql = W.scan_sql("a", "<", 0.5)
+    with Connection() as conn:
+        conn.execute("CALL gpu_buffer_init('2 GB', '2 GB')")
+        conn.create_table("t", {"a": (L.T_INTEGER, d["a"]), "b": (L.T_BIGINT, d["b"]), "c": (L.T_FLOAT, d["c"]),
+                                "d": (L.T_DATE, d["d"]), "e": (L.T_TIMESTAMP, d["e"])})
+        conn.gpu_register_table("t")
+        conn.autotune(sql, reps=1)
+    text = path.read_text()
+    assert "pipeline:materialize" in text
+    path.write_text(re.sub(r"^(pipeline:materialize\S*) \S+ \S+$", rf"\1 2 {256 if warp_tiles else 1024}",
+                           text, flags=re.M))
+    with Connection() as conn:
+        conn.execute("CALL gpu_buffer_init('2 GB', '2 GB')")
+        conn.create_table("t", {"a": (L.T_INTEGER, d["a"]), "b": (L.T_BIGINT, d["b"]), "c": (L.T_FLOAT, d["c"]),
+                                "d": (L.T_DATE, d["d"]), "e": (L.T_TIMESTAMP, d["e"])})
+        conn.gpu_register_table("t")
+        r = conn.gpu_processing(sql)
+        rows = orc.filter_rows([(d["a"], "<", int(0.5 * 2**31))])
+        assert np.array_equal(r.columns[0], orc.gather(d["a"], rows))
+        assert np.array_equal(r.columns[1], orc.gather(d["b"], rows, "+", 5))
+        assert np.array_equal(r.columns[2], orc.gather(d["c"], rows, "*", np.float32(10)))
+        assert np.array_equal(r.columns[4], orc.gather(d["e"], rows))

@@ -106,3 +106,37 @@ def test_small_queries_are_graph_batched(conn):
     for q, r in zip(qs, res):
         assert r == conn.gpu_processing(q).fetchall()
     assert conn.serve_stats()["batched_launches"] >= 1
+
+
+@pytest.mark.gpu
+def test_resident_programs_are_reused_with_new_literals(conn):
+    """Requests of one shape reuse a resident compiled program: its filter
+    literals are patched and its CUDA graph replayed after a parameter
+    update. Every result must match the oracle, and a table registered again
+    retires the programs that read its old version."""
+    import oracle as orc
+    conn.execute("CALL gpu_buffer_init('2 GB', '2 GB')")
+    d = W.scan(500_000, seed_salt=9)
+    cols = {"a": (L.T_INTEGER, d["a"]), "b": (L.T_BIGINT, d["b"]), "c": (L.T_FLOAT, d["c"]),
+            "d": (L.T_DATE, d["d"]), "e": (L.T_TIMESTAMP, d["e"])}
+    conn.create_table("t", cols)
+    conn.gpu_register_table("t", upload=True)
+    conn.set_serve_slots(1)  # one worker: requests run one after another
+    cuts = [0.01, 0.3, 0.5, 0.07, 0.9, 0.2]
+    for sel in cuts:
+        q = f"SELECT a, b + 5 AS b5 FROM t WHERE a < {int(sel * 2**31)} AND d >= DATE '1993-01-01'"
+        got = conn.submit(q).wait(timeout_s=60)
+        rows = orc.filter_rows([(d["a"], "<", int(sel * 2**31)), (d["d"], ">=", W.DAY0 + 366)])
+        assert np.array_equal(got.columns[0], orc.gather(d["a"], rows))
+        assert np.array_equal(got.columns[1], orc.gather(d["b"], rows, "+", 5))
+    st = conn.serve_stats()
+    assert st["program_reuses"] >= len(cuts) - 1
+    assert st["graph_updates"] >= 1
+    # a new version of the table: the resident programs of the old one retire
+    d2 = W.scan(200_000, seed_salt=10)
+    conn.create_table("t", {k: (v[0], d2[k]) for k, v in cols.items()})
+    conn.gpu_register_table("t", upload=True)
+    q = f"SELECT a, b + 5 AS b5 FROM t WHERE a < {2**30} AND d >= DATE '1993-01-01'"
+    got = conn.submit(q).wait(timeout_s=60)
+    rows = orc.filter_rows([(d2["a"], "<", 2**30), (d2["d"], ">=", W.DAY0 + 366)])
+    assert np.array_equal(got.columns[0], orc.gather(d2["a"], rows))
