@@ -177,6 +177,7 @@ enum SinkKind : int32_t {
   SK_AGG_SCALAR = 6,   // one group (no GROUP BY)
   SK_PART_COUNT = 7,   // count the surviving rows per key partition, per CTA
   SK_PART_SCATTER = 8, // write (key, values) records into their partitions
+  SK_AGG_FEW = 9,      // one pass into per-CTA tables of every group (k_agg_few, not a pipeline)
 };
 
 // Hash aggregate table (SoA). State word: 0 empty, 1 claimed, 2 ready.

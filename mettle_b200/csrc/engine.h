@@ -186,7 +186,8 @@ class Arena {
 struct Step {
   enum Kind {
     MEMSET, FILL, PIPELINE, COMPACT_FLAGS, COMPACT_READY, FINALIZE, ENCODE, RADIX, TOPK, TOPK_FINAL, GATHER,
-    PART_SCAN, PART_AGG  // partitioned aggregation (descriptor in `pipe`)
+    PART_SCAN, PART_AGG,  // partitioned aggregation (descriptor in `pipe`)
+    AGG_FEW               // one-pass few-group aggregation (descriptor in `pipe`)
   } k;
   std::string name;  // for per-step profiles, e.g. "pipeline:agg_slot:lineitem"
   // MEMSET / FILL (u64 words)

@@ -969,6 +969,42 @@ struct Compiler {
     return true;
   }
 
+  // One pass over one table's columns into per-CTA shared-memory tables that
+  // hold every group (k_agg_few): for a one-key aggregate over few groups of
+  // one table with no filters, whose key and inputs are plain columns.
+  // Returns false (nothing queued) when the query does not have that shape.
+  bool push_few(PipeBuilder& pb, uint64_t est, uint64_t rows) {
+    const PipeDesc& d = pb.d;
+    if (plan.sources.size() != 1 || d.n_ops != 0 || rows == 0 || est > 1536) return false;
+    auto plain = [&](int pi) {
+      const VmProg& p = d.progs[pi];
+      return p.fast.shape == 1 && p.fast.leaf[0].op == VM_COL && !p.fast.leaf_cast[0].on;
+    };
+    if (!plain(d.key_prog[0])) return false;
+    std::set<int> cols;
+    int n128 = 0;
+    for (int a = 0; a < d.n_aggs; ++a) {
+      n128 += d.aggs[a].fn == A_SUM_I128;
+      if (d.aggs[a].prog < 0) continue;
+      if (!plain(d.aggs[a].prog)) return false;
+      cols.insert(d.progs[d.aggs[a].prog].fast.leaf[0].arg);
+    }
+    if ((int)cols.size() > agg_few_max_cols()) return false;
+    uint64_t cap = 64;
+    while (cap < est * 4 / 3 + 16) cap <<= 1;
+    if (cap * (1 + (uint64_t)d.n_aggs + (uint64_t)n128) * 8 > 200 * 1024) return false;
+    pb.d.smem_capacity = (int32_t)cap;
+    pb.d.sink = SK_AGG_FEW;
+    Step s;
+    s.k = Step::AGG_FEW;
+    s.pipe = pb.d;
+    s.n_hint = rows;
+    s.name = "agg_few:" + plan.sources[0].name;
+    P.steps.push_back(s);
+    P.kernels += 1;
+    return true;
+  }
+
   // Aggregate state descriptors for the sink (shared with the rep build).
   struct AggState {
     int fn_dev = 0;   // AggFn
@@ -1495,7 +1531,9 @@ struct Compiler {
     // may run either way; the autotuner's measured choice decides
     const int strategy = cas_table && est_groups <= 1536 ? tune_agg_strategy(ctx, est_groups, root_rows) : 0;
     P.agg_strategy_key = cas_table && est_groups <= 1536 ? tune_key_agg(est_groups, root_rows) : "";
-    if (cas_table && strategy != 1 && push_partitioned(pb, est_groups, root_rows, strategy == 2)) {
+    if (cas_table && strategy != 2 && push_few(pb, est_groups, root_rows)) {
+      // one pass over the columns into per-CTA tables
+    } else if (cas_table && strategy != 1 && push_partitioned(pb, est_groups, root_rows, strategy == 2)) {
       // count, scan, scatter and per-partition aggregation are queued
     } else if (cas_table) {
       pb.d.sink = SK_AGG_SMEM;
@@ -1514,7 +1552,7 @@ struct Compiler {
         pb.d.smem_capacity = 0;
       }
     }
-    if (pb.d.sink != SK_PART_COUNT) push_pipeline(pb, root_rows);
+    if (pb.d.sink != SK_PART_COUNT && pb.d.sink != SK_AGG_FEW) push_pipeline(pb, root_rows);
     std::vector<FinalOut> fo;
     for (size_t i = 0; i < plan.outputs.size(); ++i) {
       const BOut& o = plan.outputs[i];
@@ -1842,6 +1880,7 @@ static const char* step_kind_name(Step::Kind k) {
     case Step::GATHER: return "gather";
     case Step::PART_SCAN: return "part_scan";
     case Step::PART_AGG: return "part_agg";
+    case Step::AGG_FEW: return "agg_few";
   }
   return "step";
 }
@@ -1885,6 +1924,7 @@ void run_program(Ctx& ctx, Program& p, cudaStream_t s) {
       case Step::GATHER: CK(launch_gather_width(st.gin, st.width, st.idx, st.count, st.n_max, st.gout, s)); break;
       case Step::PART_SCAN: CK(launch_part_scan(st.pipe, s)); break;
       case Step::PART_AGG: CK(launch_part_agg(st.pipe, st.n_hint, s)); break;
+      case Step::AGG_FEW: CK(launch_agg_few(st.pipe, st.n_hint, s)); break;
     }
     if (p.profile) CK(cudaEventRecord(p.prof_ev[2 * i + 1], s));
   }

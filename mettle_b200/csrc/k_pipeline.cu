@@ -2067,6 +2067,208 @@ cudaError_t launch_part_agg(const PipeDesc& d, uint64_t n_hint, cudaStream_t s) 
   return cudaGetLastError();
 }
 
+// ------------------------------------------------- one-pass few-group aggregation
+// A one-key aggregate over few groups (all of them fit one CTA's
+// shared-memory table) read straight from its columns in a single pass, with
+// no intermediate records: a grouped aggregate over one table without
+// filters or joins whose key and inputs are plain columns. Each thread reads
+// kFewRows rows per step, one row per CTA-wide stripe so that every warp
+// load is 32 consecutive rows, with all of a step's loads issued before any
+// is used. A row finds its group in the CTA table (keys claimed by CAS;
+// states in one array per aggregate, indexed like the keys); a warp's rows of
+// one group are combined in registers first (match.any, log-step shuffles),
+// so a group takes one shared-memory update per warp and step. The CTA's
+// table is merged into the global table at the end.
+constexpr int kFewThreads = 512;
+constexpr int kFewRows = 4;
+constexpr int kFewCols = 4;  // distinct input columns
+
+__host__ __device__ inline uint32_t few_words(const PipeDesc& d) {
+  uint32_t w = 1u + (uint32_t)d.n_aggs;
+  for (int a = 0; a < d.n_aggs; ++a) w += d.aggs[a].fn == A_SUM_I128;
+  return w;
+}
+
+__device__ __forceinline__ int few_find(uint64_t* keys, uint32_t cap, uint64_t key) {
+  if ((int64_t)key == kEmptyKey) return -1;
+  uint32_t idx = (uint32_t)hash_slot(key_hash1(key), (uint64_t)cap);
+  for (uint32_t probe = 0; probe < cap; ++probe) {
+    const uint64_t k = *(volatile uint64_t*)(keys + idx);
+    if (k == key) return (int)idx;
+    if ((int64_t)k == kEmptyKey) {
+      const unsigned long long prev =
+          atomicCAS((unsigned long long*)(keys + idx), (unsigned long long)kEmptyKey, (unsigned long long)key);
+      if (prev == (unsigned long long)kEmptyKey || prev == key) return (int)idx;
+    }
+    if (++idx == cap) idx = 0;
+  }
+  return -1;
+}
+
+__global__ void __launch_bounds__(kFewThreads, 2) k_agg_few(const __grid_constant__ PipeDesc d) {
+  extern __shared__ __align__(16) uint64_t fsm[];
+  const uint32_t cap = (uint32_t)d.smem_capacity;
+  const int na = d.n_aggs;
+  uint64_t* const skey = fsm;
+  uint64_t* const sst = fsm + cap;               // [aggregate][cap]
+  uint64_t* const shi = sst + (size_t)na * cap;  // [128-bit sum][cap] high words
+  // per aggregate: the row of its high words and its input column (-1: none)
+  __shared__ int hidx[kMaxAggs], acol[kMaxAggs], vcol[kFewCols];
+  __shared__ int s_ncol;
+  int n128 = 0;
+  for (int a = 0; a < na; ++a) n128 += d.aggs[a].fn == A_SUM_I128;
+  if (threadIdx.x == 0) {
+    int h = 0, nc = 0;
+    for (int a = 0; a < kMaxAggs; ++a) {
+      hidx[a] = (a < na && d.aggs[a].fn == A_SUM_I128) ? h++ : -1;
+      acol[a] = -1;
+      if (a >= na || d.aggs[a].prog < 0) continue;
+      const int c = d.progs[d.aggs[a].prog].fast.leaf[0].arg;
+      int f = -1;
+      for (int j = 0; j < nc; ++j)
+        if (vcol[j] == c) f = j;
+      if (f < 0 && nc < kFewCols) {
+        f = nc;
+        vcol[nc++] = c;
+      }
+      acol[a] = f;
+    }
+    for (int j = nc; j < kFewCols; ++j) vcol[j] = 0;
+    s_ncol = nc;
+  }
+  for (uint32_t i = threadIdx.x; i < cap; i += kFewThreads) {
+    skey[i] = (uint64_t)kEmptyKey;
+    for (int a = 0; a < na; ++a) {
+      uint64_t v = 0;
+      switch (d.aggs[a].fn) {
+        case A_MIN_I: v = 0x7FFFFFFFFFFFFFFFULL; break;
+        case A_MAX_I: v = 0x8000000000000000ULL; break;
+        case A_MIN_F: v = ~0ULL; break;
+        default: v = 0; break;
+      }
+      sst[(size_t)a * cap + i] = v;
+    }
+    for (int h = 0; h < n128; ++h) shi[(size_t)h * cap + i] = 0;
+  }
+  __syncthreads();
+  const int ncol = s_ncol;
+  const DCol kc = d.cols[d.progs[d.key_prog[0]].fast.leaf[0].arg];
+  const uint64_t n = d.n;
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t lt = (1u << lane) - 1u;
+  const DAggTable& tb = d.table;
+  const uint64_t gstride = tb.stride > 1 ? (uint64_t)tb.stride : 1;
+  uint32_t st = 0;
+  const bool combinable = n128 == 0;
+  const uint64_t step = (uint64_t)kFewThreads * kFewRows;
+  for (uint64_t base = (uint64_t)blockIdx.x * step; base < n; base += (uint64_t)gridDim.x * step) {
+    uint64_t key[kFewRows];
+    int64_t val[kFewCols][kFewRows];
+    bool act[kFewRows];
+#pragma unroll
+    for (int r = 0; r < kFewRows; ++r) {
+      const uint64_t row = base + (uint64_t)r * kFewThreads + threadIdx.x;
+      act[r] = row < n;
+      const uint64_t rr = act[r] ? row : 0;
+      key[r] = (uint64_t)load_bits(kc.ptr, kc.ptype, rr);
+#pragma unroll
+      for (int c = 0; c < kFewCols; ++c)
+        val[c][r] = c < ncol ? load_bits(d.cols[vcol[c]].ptr, d.cols[vcol[c]].ptype, rr) : 0;
+    }
+#pragma unroll
+    for (int r = 0; r < kFewRows; ++r) {
+      const int slot = act[r] ? few_find(skey, cap, key[r]) : -1;
+      // rows whose key has no CTA entry (the empty-slot sentinel key, or a
+      // table fuller than planned) update the global table directly
+      uint64_t g = kNoGroup;
+      if (act[r] && slot < 0) g = agg_find_cas(tb, key[r], hash_slot(key_hash1(key[r]), tb.capacity), st);
+      const uint32_t code = slot >= 0 ? (uint32_t)slot : 0xFFFFFFFFu;
+      const unsigned peers = __match_any_sync(0xFFFFFFFFu, code);
+      const bool comb = combinable && __any_sync(0xFFFFFFFFu, slot >= 0 && __popc(peers) >= 3);
+      const bool lead = (peers & lt) == 0;
+      for (int a = 0; a < na; ++a) {
+        const DAgg& ag = d.aggs[a];
+        const int c = acol[a];
+        const int32_t vt = c >= 0 ? d.cols[vcol[c]].ptype : P_I64;
+        Val v;
+        v.lo = c == 0 ? val[0][r] : c == 1 ? val[1][r] : c == 2 ? val[2][r] : c == 3 ? val[3][r] : 0;
+        v.hi = v.lo >> 63;
+        const uint32_t sa = smem_u32(sst + (size_t)a * cap + (slot >= 0 ? slot : 0));
+        const uint32_t sh = hidx[a] >= 0 ? smem_u32(shi + (size_t)hidx[a] * cap + (slot >= 0 ? slot : 0)) : 0;
+        auto apply = [&](auto fnc) {
+          constexpr int FN = decltype(fnc)::value;
+          if (comb) {  // warp-uniform; every state is one word
+            if (FN != A_SUM_I128) {
+              const uint64_t x = peer_combine(FN, slot >= 0 ? peers : 0u, lane_state_value(FN, v, vt), lane);
+              if (slot >= 0 && lead) smem_merge(FN, sa, x);
+            }
+          } else if (slot >= 0) {
+            smem_apply(FN, sa, sh, v, vt);
+          }
+          if (slot < 0 && g != kNoGroup) {
+            const uint64_t o = g * gstride;
+            agg_apply_g(FN, (unsigned long long*)ag.lo + o, ag.hi ? (long long*)ag.hi + o : nullptr, v, vt);
+          }
+        };
+        dispatch_fn(ag.fn, apply);
+      }
+    }
+  }
+  __syncthreads();
+  for (uint32_t i = threadIdx.x; i < cap; i += kFewThreads) {
+    const uint64_t key = skey[i];
+    if ((int64_t)key == kEmptyKey) continue;
+    const uint64_t g = agg_find_cas(tb, key, hash_slot(key_hash1(key), tb.capacity), st);
+    if (g == kNoGroup) continue;
+    const uint64_t o = g * gstride;
+    for (int a = 0; a < na; ++a) {
+      const DAgg& ag = d.aggs[a];
+      const int64_t hv = hidx[a] >= 0 ? (int64_t)shi[(size_t)hidx[a] * cap + i] : 0;
+      agg_merge(ag.fn, (unsigned long long*)(ag.lo + o), (long long*)(ag.hi ? ag.hi + o : nullptr),
+                sst[(size_t)a * cap + i], hv);
+    }
+  }
+  if (st) atomicOr(d.status, st);
+}
+
+size_t agg_few_smem_bytes(const PipeDesc& d) { return (size_t)d.smem_capacity * few_words(d) * 8; }
+
+int agg_few_max_cols() { return kFewCols; }
+
+cudaError_t launch_agg_few(const PipeDesc& d, uint64_t n_hint, cudaStream_t s) {
+  if (d.smem_capacity <= 0) return cudaErrorInvalidValue;
+  static std::mutex mu;
+  static size_t smem_set = 0;
+  static std::map<size_t, int> occ;
+  const size_t smem = agg_few_smem_bytes(d);
+  int per_sm = 1;
+  {
+    std::lock_guard<std::mutex> g(mu);
+    if (smem > smem_set) {
+      cudaError_t e = cudaFuncSetAttribute(k_agg_few, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      if (e != cudaSuccess) return e;
+      smem_set = smem;
+    }
+    auto it = occ.find(smem);
+    if (it != occ.end()) {
+      per_sm = it->second;
+    } else {
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_agg_few, kFewThreads, smem) != cudaSuccess ||
+          per_sm < 1) {
+        cudaGetLastError();
+        per_sm = 1;
+      }
+      occ[smem] = per_sm;
+    }
+  }
+  if (d.grid_per_sm > 0 && d.grid_per_sm < per_sm) per_sm = d.grid_per_sm;
+  const uint64_t steps = (n_hint + (uint64_t)kFewThreads * kFewRows - 1) / ((uint64_t)kFewThreads * kFewRows);
+  uint64_t grid = (uint64_t)sm_count() * (uint64_t)per_sm;
+  if (steps < grid) grid = steps ? steps : 1;
+  k_agg_few<<<(unsigned)grid, kFewThreads, smem, s>>>(d);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_pipeline(const PipeDesc& d, uint64_t n_hint, cudaStream_t s) {
   if (d.tuple_input) return cudaErrorInvalidValue;  // every pipeline scans a base table
   switch (d.sink) {

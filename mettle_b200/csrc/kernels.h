@@ -31,6 +31,14 @@ int pipeline_part_ctas();
 size_t part_agg_smem_bytes(const PipeDesc& d);
 cudaError_t launch_part_scan(const PipeDesc& d, cudaStream_t s);
 cudaError_t launch_part_agg(const PipeDesc& d, uint64_t n_hint, cudaStream_t s);
+// One-pass few-group aggregation (k_pipeline.cu): d describes one table
+// (no filters, probes or tuple input), a one-key CAS table in d.table, a
+// plain-column key (d.key_prog[0]) and aggregates whose inputs are plain
+// columns (at most agg_few_max_cols() distinct) or none; d.smem_capacity is
+// the CTA table's entries (a power of two above the group count).
+size_t agg_few_smem_bytes(const PipeDesc& d);
+int agg_few_max_cols();
+cudaError_t launch_agg_few(const PipeDesc& d, uint64_t n_hint, cudaStream_t s);
 
 // ---- aggregate finalize (k_misc.cu)
 // Order-preserving list of READY slots of a hash aggregate table.

@@ -189,6 +189,51 @@ C3_ALL_GROUPS_SQL = ("SELECT k, SUM(v), COUNT(*), MIN(v), MAX(v), AVG(v), SUM(f)
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("groups,dist", [(10, "uniform"), (100, "zipf"), (1000, "uniform"), (1000, "zipf")])
+def test_c3_few_groups_one_pass_all_groups(conn, groups, dist):
+    """Few groups: one pass over the columns into per-CTA shared-memory tables
+    (the plan's agg_few step), with a warp's rows of one group combined before
+    they update; every group on all ten aggregates against the oracle."""
+    init(conn)
+    d = W.groupby(n=6_000_000, groups=groups, dist=dist, seed_salt=groups + 5)
+    conn.create_table("t", {"k": (L.T_BIGINT, d["k"]), "v": (L.T_BIGINT, d["v"]), "f": (L.T_FLOAT, d["f"])})
+    conn.gpu_register_table("t", upload=True)
+    assert any(s.startswith("agg_few") for s in _step_names(conn, C3_ALL_GROUPS_SQL))
+    want = orc.groupby_c3(d["k"], d["v"], d["f"], limit=-1)
+    _check_c3_all_groups(conn.gpu_processing(C3_ALL_GROUPS_SQL), want)
+    r = conn.gpu_processing(W.C3_SQL)
+    top = orc.groupby_c3(d["k"], d["v"], d["f"], limit=100)
+    assert np.array_equal(r.columns[0], top["k"]) and np.array_equal(r.columns[5], top["avg_v"])
+
+
+@pytest.mark.gpu
+def test_few_groups_edge_keys_and_wide_sums(conn):
+    """The one-pass path with the empty-slot sentinel key and both int64
+    extremes as keys (the sentinel's rows update the global table directly)
+    and sums that need 128 bits (no combining)."""
+    init(conn)
+    r = np.random.default_rng(77)
+    n = 3_000_000
+    k = r.integers(0, 50, n).astype(np.int64) * 1_000_003
+    k[::7] = -1
+    k[::11] = np.iinfo(np.int64).min
+    k[::13] = np.iinfo(np.int64).max
+    v = r.integers(2**61, 2**62, n).astype(np.int64)  # sums beyond int64
+    conn.create_table("t", {"k": (L.T_BIGINT, k), "v": (L.T_BIGINT, v)})
+    conn.gpu_register_table("t")
+    sql = "SELECT k, COUNT(*), SUM(v), MIN(v), MAX(v) FROM t GROUP BY k ORDER BY k"
+    assert any(s.startswith("agg_few") for s in _step_names(conn, sql))
+    res = conn.gpu_processing(sql)
+    want = _grouped(k, {"v": v.astype(object)})
+    rows = res.fetchall()
+    assert [x[0] for x in rows] == want["k"].tolist()
+    assert [x[1] for x in rows] == want["cnt"].tolist()
+    assert [int(x[2]) for x in rows] == [int(s) for s in want["v_sum"]]
+    assert [x[3] for x in rows] == [int(s) for s in want["v_min"]]
+    assert [x[4] for x in rows] == [int(s) for s in want["v_max"]]
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("n,groups,dist", [(20_000_000, 4_000_000, "uniform"), (40_000_000, 8_000_000, "zipf")])
 def test_c3_many_partitions_all_groups(conn, n, groups, dist):
     """Millions of groups: the partitioned aggregation at thousands of
