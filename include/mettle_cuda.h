@@ -279,6 +279,7 @@ typedef struct mtl_serve_stats {
   int64_t program_reuses;   /* requests that reused a resident compiled program */
   int64_t cached_programs;  /* compiled programs resident now */
   int64_t graph_updates;    /* parameter updates of resident programs' CUDA graphs */
+  int64_t builds_kept;      /* join builds a resident program kept from its previous run */
 } mtl_serve_stats;
 int mtl_serve_stats_get(mtl_ctx *ctx, mtl_serve_stats *out);
 /* Streams (slots) the serving loop may run concurrently (default 4). */

@@ -71,7 +71,7 @@ class CacheStats(C.Structure):
 class ServeStats(C.Structure):
     _fields_ = [(n, C.c_int64) for n in (
         "submitted", "completed", "rejected", "in_flight", "queued", "admitted_bytes", "batched_launches",
-        "program_reuses", "cached_programs", "graph_updates")]
+        "program_reuses", "cached_programs", "graph_updates", "builds_kept")]
 
 
 # (name, restype, argtypes) of every exported entry point

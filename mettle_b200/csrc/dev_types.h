@@ -132,6 +132,10 @@ struct DBuild {
   uint32_t* payload[kMaxSrc];
   int32_t unique_keys;      // the key column holds no duplicates (no check needed)
   int32_t pad;
+  // hash: optional blocked Bloom filter of the inserted keys (null: none);
+  // bloom_words is a power of two
+  uint32_t* bloom;
+  uint64_t bloom_words;
 };
 
 struct DProbe {

@@ -199,6 +199,12 @@ struct Step {
   PipeDesc pipe;
   uint64_t n_hint = 0;
   std::vector<int> pred_filter;  // BoundPlan filter behind each of pipe.preds
+  // build pipelines: the source built, the sources of its subtree, whether
+  // its result can be kept across runs, and its row count
+  int build_src = -1;
+  uint32_t build_src_mask = 0;
+  bool build_keepable = false;
+  uint64_t orig_n = 0;
   // COMPACT_*
   const void* flag = nullptr;
   uint64_t n = 0;
@@ -261,6 +267,14 @@ struct Program {
   // autotuner keys of the capacities (hash load factors) this compile chose
   std::vector<std::pair<std::string, uint64_t>> load_keys;
   int64_t graph_updates = 0;  // parameter updates of the instantiated graph
+  // scratch initialization (host copy), the build each segment belongs to
+  // (-1: the query's own state), and its device copy read by the fill step
+  std::vector<FillSeg> fills_host, fills_sent;
+  std::vector<int> fill_owner;
+  FillSeg* fills_dev = nullptr;
+  // the filter literals of the last run that completed, for resident builds
+  std::vector<std::pair<int64_t, double>> last_lits;
+  bool last_ok = false;
   std::string agg_strategy_key;  // autotuner key of a one-key aggregate's strategy ("" none)
   ~Program();
 };
@@ -365,6 +379,8 @@ void run_program_graph(Ctx& ctx, Program& p, cudaStream_t s, bool refresh = fals
 // compiled for that shape.
 std::string plan_shape(const BoundPlan& p);
 void patch_literals(Program& p, const BoundPlan& plan);
+int keep_builds(Program& p, const BoundPlan& plan, cudaStream_t s);
+void mark_completed(Program& p, const BoundPlan& plan, bool ok);
 std::shared_ptr<Result> fetch_program(Ctx& ctx, Program& p, cudaStream_t s);
 void free_program(Ctx& ctx, Program& p);
 std::shared_ptr<Result> constant_result(const BoundPlan& plan);

@@ -388,6 +388,8 @@ struct Compiler {
   // the start of the program (arena blocks are 256-byte aligned and sized in
   // 256-byte units, so rounding a segment up to 16 bytes stays in its block).
   std::vector<FillSeg> fills;
+  std::vector<int> fill_owner;  // per segment: the source whose build it belongs to (-1: the query's)
+  int cur_owner = -1;
   void memset_step(void* p, int byte, uint64_t bytes) {
     FillSeg f;
     f.ptr = p;
@@ -395,6 +397,7 @@ struct Compiler {
     f.pattern = 0x0101010101010101ULL * (uint64_t)(byte & 0xFF);
     f.stride = 0;
     fills.push_back(f);
+    fill_owner.push_back(cur_owner);
   }
   void fill_step(void* p, uint64_t words, uint64_t v) {
     FillSeg f;
@@ -403,6 +406,7 @@ struct Compiler {
     f.pattern = v;
     f.stride = 0;
     fills.push_back(f);
+    fill_owner.push_back(cur_owner);
   }
   // one 8-byte word every stride_words words, n times
   void fill_strided(void* p, uint64_t n, uint64_t stride_words, uint64_t v) {
@@ -412,6 +416,7 @@ struct Compiler {
     f.pattern = v;
     f.stride = stride_words * 8;
     fills.push_back(f);
+    fill_owner.push_back(cur_owner);
   }
   void emit_fills() {
     if (fills.empty()) return;
@@ -427,6 +432,9 @@ struct Compiler {
     s.name = "init_scratch";
     P.steps.insert(P.steps.begin(), s);
     P.kernels += 1;
+    P.fills_host = fills;
+    P.fill_owner = fill_owner;
+    P.fills_dev = dev;
   }
 
   // ---- join tree
@@ -688,6 +696,11 @@ struct Compiler {
   std::vector<int> build_probe_index;  // per source: probe index in its parent's pipeline
 
   DBuild make_build(int s) {
+    cur_owner = s;  // the build's own scratch initialization
+    struct Reset {
+      int& o;
+      ~Reset() { o = -1; }
+    } reset{cur_owner};
     DBuild b;
     memset(&b, 0, sizeof(b));
     Table& t = *plan.sources[s].table;
@@ -729,8 +742,31 @@ struct Compiler {
       b.hash_special = (uint32_t*)scratch(8);
       memset_step(b.hash_keys, 0xFF, b.capacity * 8);
       memset_step(b.hash_special, 0, 8);
+      // A build that filters its rows (a predicate, or a probe of its own
+      // builds) holds a fraction of its table's keys, so most probes miss:
+      // a Bloom filter of about 8 bits per table row (small enough to stay
+      // in L2) answers those misses without reading the table in HBM. The
+      // reference builds a membership bitmap for the same purpose
+      // (build_membership_filter_v / membership_filter_mask_v,
+      // src/metal/shaders/kernels.metal:917-956, src/plan/executor/join_plan.rs:312).
+      if (build_filters(s)) {
+        uint64_t words = 64;
+        while (words < rows / 4) words <<= 1;
+        b.bloom_words = words;
+        b.bloom = (uint32_t*)scratch(words * 4);
+        memset_step(b.bloom, 0, words * 4);
+      }
     }
     return b;
+  }
+
+  // Whether source s's build pipeline drops rows: a predicate on s, or a
+  // probe of a child build (an inner join).
+  bool build_filters(int s) const {
+    if (!children[s].empty()) return true;
+    for (const BFilter& f : plan.filters)
+      if (f.src == s && f.op != C_TRUE) return true;
+    return false;
   }
 
   // Sources whose row ids the root pipeline's sink needs.
@@ -1354,6 +1390,12 @@ struct Compiler {
       }
       pb.d.status = P.status;
       push_pipeline(pb, pb.d.n);
+      // a build that initializes no aggregate states can stay resident
+      // across runs of this program whose literals leave its subtree unchanged
+      P.steps.back().build_src = s;
+      P.steps.back().build_src_mask = subtree[s];
+      P.steps.back().build_keepable = s != rep_src;
+      P.steps.back().orig_n = pb.d.n;
     }
 
     // root pipeline
@@ -1852,6 +1894,52 @@ std::string plan_shape(const BoundPlan& p) {
   for (auto& r : p.order) add("R" + std::to_string(r.out) + (r.desc ? "d" : "a"));
   add("L" + std::to_string(p.limit) + (p.constant_only ? "c" : ""));
   return o;
+}
+
+// Builds kept from the program's previous run: a build pipeline whose
+// subtree's filter literals equal those of the last run that completed, and
+// that initializes no aggregate states, is left out (its scan covers no
+// rows and its scratch is not cleared), so its hash table or direct-mapped
+// map, presence bits and payload stay as that run left them. Enqueues on
+// `s` the fill descriptors that leave kept builds' scratch alone. Returns
+// the number of builds kept.
+int keep_builds(Program& P, const BoundPlan& plan, cudaStream_t s) {
+  const bool known = P.last_ok && P.last_lits.size() == plan.filters.size();
+  uint32_t kept_src = 0;
+  int kept = 0;
+  for (Step& st : P.steps) {
+    if (st.k != Step::PIPELINE || st.build_src < 0) continue;
+    bool keep = known && st.build_keepable;
+    for (size_t f = 0; keep && f < plan.filters.size(); ++f)
+      if ((st.build_src_mask >> plan.filters[f].src) & 1u)
+        keep = P.last_lits[f].first == plan.filters[f].ilit && P.last_lits[f].second == plan.filters[f].flit;
+    st.pipe.n = keep ? 0 : st.orig_n;
+    if (keep) {
+      kept_src |= 1u << st.build_src;
+      ++kept;
+    }
+  }
+  if (P.fills_dev && !P.fills_host.empty()) {
+    std::vector<FillSeg> send = P.fills_host;
+    for (size_t i = 0; i < send.size(); ++i)
+      if (P.fill_owner[i] >= 0 && ((kept_src >> P.fill_owner[i]) & 1u)) send[i].bytes = 0;
+    const bool same = send.size() == P.fills_sent.size() &&
+                      memcmp(send.data(), P.fills_sent.data(), send.size() * sizeof(FillSeg)) == 0;
+    if (!same && (!P.fills_sent.empty() || kept)) {
+      P.fills_sent = std::move(send);
+      CK(cudaMemcpyAsync(P.fills_dev, P.fills_sent.data(), P.fills_sent.size() * sizeof(FillSeg),
+                         cudaMemcpyHostToDevice, s));
+    }
+  }
+  return kept;
+}
+
+// Records the literals of a run that completed (kept builds match them next time).
+void mark_completed(Program& P, const BoundPlan& plan, bool ok) {
+  P.last_ok = ok;
+  P.last_lits.clear();
+  if (!ok) return;
+  for (const BFilter& f : plan.filters) P.last_lits.push_back({f.ilit, f.flit});
 }
 
 void patch_literals(Program& P, const BoundPlan& plan) {

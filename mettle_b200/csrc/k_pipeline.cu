@@ -72,6 +72,10 @@ __device__ __forceinline__ void build_insert(const DBuild& b, int64_t key, uint3
     else if (atomicOr(b.dense_bits + (k >> 5), bit) & bit) st |= ST_DUP_BUILD_KEY;
     return;
   }
+  if (b.bloom) {
+    const uint64_t hh = hash64((uint64_t)key);
+    atomicOr(b.bloom + bloom_word(hh, b.bloom_words), bloom_mask(hh));  // no reply needed
+  }
   if (key == kEmptyKey) {
     if (atomicCAS(b.hash_special, 0u, slot + 1) != 0u) st |= ST_DUP_BUILD_KEY;
     return;
@@ -1209,16 +1213,24 @@ __global__ void __launch_bounds__(kThreads, (SINK == SK_AGG_SCALAR || SINK == SK
           } else {
             uint64_t h[kProbeBatch];
             int64_t k0[kProbeBatch];
+            bool maybe[kProbeBatch];
+            // the build's Bloom filter (L2-resident) first: keys it rules
+            // out never touch the table in HBM
 #pragma unroll
             for (int j = 0; j < kProbeBatch; ++j) {
-              h[j] = hash_slot(hash64((uint64_t)key[j]), bd.capacity);
-              k0[j] = (act[j] && key[j] != kEmptyKey) ? bd.hash_keys[h[j]] : kEmptyKey;
+              h[j] = hash64((uint64_t)key[j]);
+              maybe[j] = act[j] && bloom_maybe(bd, h[j]);
+            }
+#pragma unroll
+            for (int j = 0; j < kProbeBatch; ++j) {
+              h[j] = hash_slot(h[j], bd.capacity);
+              k0[j] = (maybe[j] && key[j] != kEmptyKey) ? bd.hash_keys[h[j]] : kEmptyKey;
             }
 #pragma unroll
             for (int j = 0; j < kProbeBatch; ++j) {
               keep[j] = false;
               slot[j] = 0;
-              if (!act[j]) continue;
+              if (!maybe[j]) continue;
               if (k0[j] == key[j] && key[j] != kEmptyKey) {
                 keep[j] = true;
                 slot[j] = bd.hash_slot[h[j]] - 1u;

@@ -518,4 +518,18 @@ __device__ __forceinline__ uint64_t hash64(uint64_t x) {
 // Maps a hash onto [0, cap) without a power-of-two capacity.
 __device__ __forceinline__ uint64_t hash_slot(uint64_t h, uint64_t cap) { return __umul64hi(h, cap); }
 
+// Blocked Bloom filter of a hash-join build (one 32-bit word per key, two
+// bits in it), from the key's 64-bit hash h: the word from the low bits (the
+// table slot uses the high ones), the bits from the middle.
+__device__ __forceinline__ uint32_t bloom_word(uint64_t h, uint64_t words) { return (uint32_t)(h & (words - 1)); }
+__device__ __forceinline__ uint32_t bloom_mask(uint64_t h) {
+  return (1u << ((h >> 32) & 31)) | (1u << ((h >> 37) & 31));
+}
+// false: the key is certainly not in the build (true also when there is no filter)
+__device__ __forceinline__ bool bloom_maybe(const DBuild& b, uint64_t h) {
+  if (!b.bloom) return true;
+  const uint32_t m = bloom_mask(h);
+  return (__ldg(b.bloom + bloom_word(h, b.bloom_words)) & m) == m;
+}
+
 }  // namespace mtl

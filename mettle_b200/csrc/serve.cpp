@@ -20,7 +20,9 @@
 // compilation, no descriptor uploads, no graph instantiation. Idle programs
 // are evicted (least recently used first) when a new compile needs their
 // memory, and the cache holds at most kMaxPrograms programs and half the
-// processing region.
+// processing region. Join builds stay resident with their program: a build
+// whose subtree's literals are those of the program's last completed run
+// (and that initializes no aggregate states) is not rebuilt (keep_builds).
 #include <chrono>
 #include <cstring>
 
@@ -70,7 +72,7 @@ struct ServeState {
   bool stop = false;
   int slots = 4;
   std::atomic<int64_t> submitted{0}, completed{0}, rejected{0}, in_flight{0}, admitted_bytes{0}, batched{0};
-  std::atomic<int64_t> reuses{0};
+  std::atomic<int64_t> reuses{0}, builds_kept{0};
   // program cache (guarded by mu)
   std::list<CachedProgram> programs;
   uint64_t program_bytes = 0;
@@ -227,14 +229,19 @@ static void run_batch(Ctx& ctx, ServeState& S, std::vector<Request*>& batch, cud
   try {
     cudaEventRecord(e0, s);
     for (Request* r : ready) {
-      if (r->cached) run_program_graph(ctx, *r->program(), s, /*refresh=*/true);
-      else run_program(ctx, *r->program(), s);
+      if (r->cached) {
+        S.builds_kept += keep_builds(*r->program(), r->plan, s);
+        run_program_graph(ctx, *r->program(), s, /*refresh=*/true);
+      } else {
+        run_program(ctx, *r->program(), s);
+      }
     }
     cudaEventRecord(e1, s);
     if (ready.size() > 1) S.batched++;
   } catch (const EngineError& e) {
     cudaStreamSynchronize(s);
     for (Request* r : ready) {
+      if (r->program()) mark_completed(*r->program(), r->plan, false);
       release(ctx, S, r, false);
       finish(S, r, e.code, e.what());
     }
@@ -248,9 +255,11 @@ static void run_batch(Ctx& ctx, ServeState& S, std::vector<Request*>& batch, cud
       r->result = fetch_program(ctx, *r->program(), s);
       if (ms == 0) cudaEventElapsedTime(&ms, e0, e1);
       r->result->device_ms = ms / (float)ready.size();
+      mark_completed(*r->program(), r->plan, true);
       release(ctx, S, r, true);
       finish(S, r, MTL_OK, "");
     } catch (const EngineError& e) {
+      mark_completed(*r->program(), r->plan, false);
       release(ctx, S, r, false);
       finish(S, r, e.code, e.what());
     }
@@ -395,6 +404,7 @@ void serve_stats(Ctx& ctx, mtl_serve_stats* out) {
   out->admitted_bytes = S.admitted_bytes;
   out->batched_launches = S.batched;
   out->program_reuses = S.reuses;
+  out->builds_kept = S.builds_kept;
   {
     std::lock_guard<std::mutex> g(S.mu);
     out->cached_programs = (int64_t)S.programs.size();
