@@ -217,7 +217,8 @@ class Workload:
             # those per-kernel figures are reported as diagnostics, while the
             # roofline fraction is the query's 20 B per row over the whole
             # query's time.
-            self.dom_candidates = [("pipeline:agg_", self.bytes), ("pipeline:part_count", 8 * self.rows),
+            self.dom_candidates = [("pipeline:agg_", self.bytes), ("agg_few", self.bytes),
+                                   ("pipeline:part_count", 8 * self.rows),
                                    ("pipeline:part_scatter", 52 * self.rows), ("part_agg", 32 * self.rows)]
             self.query_frac_is_roofline = True
             self.desc = f"c3 group-by {self.rows} rows, G={g} {dist}: SUM/COUNT/MIN/MAX/AVG x2, top-100"
@@ -364,7 +365,9 @@ def run_reference(args):
 
 
 def _budget_sql(wl) -> str:
-    gb = max(8, int(wl.bytes * 3 / 2**30) + 8)
+    # scratch for the largest plans: partition records (32 B per row) and a
+    # one-key table of twice the groups at 64 B per entry
+    gb = max(16, int(wl.bytes * 8 / 2**30) + 8)
     return f"CALL gpu_buffer_init('{gb} GB', '{gb} GB', pinned_memory_size = '{2 * gb} GB')"
 
 
@@ -380,6 +383,13 @@ def measure(wl, args, dist, local: int, with_e2e: bool, cpu_seconds: float) -> d
     conn = Connection(device=local)
     conn.execute(_budget_sql(wl))
     wl.register(conn, upload=True)
+    tune_report = None
+    if args.autotune:
+        # the autotuner measures this query's launch shapes, hash load factors
+        # and aggregation strategy, and the statement below is compiled with
+        # its choices (untimed)
+        tune_report = conn.autotune(wl.sql, reps=3)
+        print(tune_report, file=sys.stderr, flush=True)
     stmt = conn.prepare(wl.sql)
     # A dedicated (non-default) stream: the library enqueues on it and the
     # CUDA events below are recorded on the same stream.
@@ -433,7 +443,7 @@ def measure(wl, args, dist, local: int, with_e2e: bool, cpu_seconds: float) -> d
             per[p].append(sum(t for n, t in steps if n.startswith(p)))
     stmt.set_profiling(False)
     dom_prefix, dom_bytes = max(cands, key=lambda c: statistics.mean(per[c[0]]))
-    dom_ms = statistics.mean(per[dom_prefix])
+    dom_ms = max(statistics.mean(per[dom_prefix]), 1e-9)
     peak, peak_src = measured_peak()
     achieved = dom_bytes / (dom_ms / 1e3) / 1e9
     traffic = profile_traffic(f"{wl.name}:{dom_prefix}")
@@ -451,7 +461,7 @@ def measure(wl, args, dist, local: int, with_e2e: bool, cpu_seconds: float) -> d
                      "dominant_kernel": {"name": dom_prefix, "ms": dom_ms, "bytes": dom_bytes,
                                          "frac": achieved / peak}})
     out = {"value": value, "ms_per_step": query_ms, "roofline": roof, "gpu_launches": kernels * args.steps,
-           "clocks": clocks, "parity": parity,
+           "clocks": clocks, "parity": parity, "autotuned": tune_report is not None,
            "step_ms": {k: v / prof_runs for k, v in sorted(totals.items(), key=lambda kv: -kv[1])[:8]}}
     stmt.close()
     conn.close()
@@ -759,6 +769,8 @@ def main():
     ap.add_argument("--launches", type=int, default=0,
                     help="profile mode: run the prepared statement this many times and print per-step times")
     ap.add_argument("--no-extra", action="store_true", help="measure the headline configuration only")
+    ap.add_argument("--autotune", action="store_true",
+                    help="run the autotuner on each measured query first (untimed) and measure its choices")
     ap.add_argument("--groups", type=int, default=None, help="config-3 group count (default 10^6)")
     ap.add_argument("--dist", default=None, choices=["uniform", "zipf"], help="config-3 key distribution")
     args = ap.parse_args()
