@@ -500,6 +500,7 @@ def measure(wl, args, dist, local: int, with_e2e: bool, cpu_seconds: float) -> d
 # Extra configurations measured beside the headline in the default run:
 # (key, config, kwargs).
 EXTRA_CONFIGS = [
+    ("c1_plain_small", "c1", {}),
     ("c2_scan_a_lt_2e30", "c2", {}),
     ("c3_groups_1e6_uniform", "c3", {"groups": 1_000_000, "dist": "uniform"}),
     ("c3_groups_5e7_uniform", "c3", {"groups": 50_000_000, "dist": "uniform"}),
@@ -541,7 +542,9 @@ def run_mettle(args):
         for key, cfg, kw in EXTRA_CONFIGS:
             x = Workload(cfg, **kw)
             r = measure(x, args, dist, local, with_e2e=False, cpu_seconds=min(args.cpu_seconds, 5.0))
-            extra[key] = {"workload": x.desc, "metric": "pipeline rows/s", "unit": "rows/s", **r}
+            l2 = ("inputs (4 MB) fit in L2 and stay there between launches: a latency-bound small query"
+                  if cfg == "c1" else "inputs larger than L2 (126 MB); no flush")
+            extra[key] = {"workload": x.desc, "metric": "pipeline rows/s", "unit": "rows/s", "l2": l2, **r}
             del x
     if rank == 0:
         line = {
