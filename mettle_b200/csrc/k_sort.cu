@@ -332,6 +332,23 @@ __global__ void __launch_bounds__(THREADS) k_topk(const SortItem* __restrict__ k
   }
 }
 
+// The leading 64 bits of a key of `bits` significant bits (right aligned in
+// w[0..3], w[0] most significant); shorter keys are returned whole.
+__device__ __forceinline__ uint64_t key_top64(const uint64_t* w, int bits) {
+  if (bits <= 64) return w[3];
+  const int s = bits - 64;  // lowest bit of the leading 64
+  const int wi = 3 - (s >> 6), sh = s & 63;
+  uint64_t x = w[wi] >> sh;
+  if (sh) x |= w[wi - 1] << (64 - sh);
+  return x;
+}
+
+// Bits 0-3: which bytes of w are nonzero.
+__device__ __forceinline__ uint32_t nz_bytes(uint32_t w) {
+  return ((w & 0xFFu) ? 1u : 0u) | ((w & 0xFF00u) ? 2u : 0u) | ((w & 0xFF0000u) ? 4u : 0u) |
+         ((w & 0xFF000000u) ? 8u : 0u);
+}
+
 // ------------------------------------------------------------ warp top-K
 // K <= 32: each warp keeps its best K as a sorted list in registers (lane i
 // holds rank i). A row enters only if it beats the warp's current K-th best
@@ -461,7 +478,7 @@ __global__ void __launch_bounds__(THREADS) k_topk_warp(const SortItem* __restric
                                                        uint64_t n_max, int K, SortItem* __restrict__ out_keys,
                                                        uint32_t* __restrict__ out_idx, uint64_t* out_count,
                                                        int final_pass, const uint32_t* __restrict__ remap = nullptr,
-                                                       uint64_t* reset = nullptr) {
+                                                       uint64_t* reset = nullptr, int cut_bits = 0) {
   constexpr int WARPS = THREADS / 32;
   __shared__ Cand s_l[WARPS][32];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -470,6 +487,9 @@ __global__ void __launch_bounds__(THREADS) k_topk_warp(const SortItem* __restric
   const uint64_t per = (n + gridDim.x - 1) / gridDim.x;
   const uint64_t lo = (uint64_t)blockIdx.x * per;
   const uint64_t hi = lo + per < n ? lo + per : n;
+  // merge of the fused top-K's candidates: the first pass is over, so its
+  // cut is final (the smallest leading bits of any warp's K-th key)
+  const uint64_t cut = (reset && cut_bits > 0) ? ~*(volatile unsigned long long*)reset : ~0ULL;
   Cand L = cand_inf();
   for (uint64_t base = lo + (uint64_t)warp * 32; base < hi; base += (uint64_t)THREADS) {
     const uint64_t g = base + lane;
@@ -480,6 +500,7 @@ __global__ void __launch_bounds__(THREADS) k_topk_warp(const SortItem* __restric
       c.w[0] = k.w[0]; c.w[1] = k.w[1]; c.w[2] = k.w[2]; c.w[3] = k.w[3];
       c.ix = idx ? idx[g] : (uint32_t)g;
       valid = c.ix != 0xFFFFFFFFu;  // padding of a previous pass
+      if (cut_bits > 0 && key_top64(c.w, cut_bits) > cut) valid = false;
     }
     warp_offer_batch(L, c, valid, K, lane);
   }
@@ -527,17 +548,6 @@ __device__ __forceinline__ bool u256_gt(const U256& a, const Cand& b) {
   return false;
 }
 
-// The leading 64 bits of a key of `bits` significant bits (right aligned in
-// w[0..3], w[0] most significant); shorter keys are returned whole.
-__device__ __forceinline__ uint64_t key_top64(const uint64_t* w, int bits) {
-  if (bits <= 64) return w[3];
-  const int s = bits - 64;  // lowest bit of the leading 64
-  const int wi = 3 - (s >> 6), sh = s & 63;
-  uint64_t x = w[wi] >> sh;
-  if (sh) x |= w[wi - 1] << (64 - sh);
-  return x;
-}
-
 // Cross-CTA state of one fused top-K launch, at the start of its temp area;
 // it must be zero when the launch starts (the merge pass clears it again).
 struct TopkFinalState {
@@ -545,19 +555,20 @@ struct TopkFinalState {
   unsigned long long n_cand;   // candidates appended
 };
 
-template <int THREADS, int R>
+template <int THREADS>
 __global__ void __launch_bounds__(THREADS) k_topk_final(const __grid_constant__ TopkFinalSpec spec, int K,
                                                         TopkFinalState* __restrict__ gst,
                                                         SortItem* __restrict__ out_keys,
                                                         uint32_t* __restrict__ out_idx) {
   constexpr int WARPS = THREADS / 32;
   __shared__ Cand s_l[WARPS][32];
-  __shared__ uint32_t s_live[WARPS][32 * R + 32];
+  __shared__ uint32_t s_live[WARPS][64];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const uint32_t lt = (1u << lane) - 1u;
   const uint64_t n = spec.n_dev ? (*spec.n_dev < spec.n_max ? *spec.n_dev : spec.n_max) : spec.n_max;
-  const uint64_t per = (n + gridDim.x - 1) / gridDim.x;
-  const uint64_t lo = (uint64_t)blockIdx.x * per;
+  // CTA ranges start on multiples of 512 groups (16-byte aligned flag loads)
+  const uint64_t per = ((n + gridDim.x - 1) / gridDim.x + 511) & ~511ULL;
+  const uint64_t lo = (uint64_t)blockIdx.x * per < n ? (uint64_t)blockIdx.x * per : n;
   const uint64_t hi = lo + per < n ? lo + per : n;
   const int tb = spec.total_bits;
   uint32_t* const wb = s_live[warp];
@@ -606,44 +617,62 @@ __global__ void __launch_bounds__(THREADS) k_topk_final(const __grid_constant__ 
       }
     }
   };
-  // Each warp walks its part of the range R groups per lane at a time,
-  // gathers the live ones in wb (ballots, no divergence later) and offers
-  // them 32 at a time.
+  // Each lane takes 16 consecutive groups per step (one 16-byte load of
+  // their flags, or four of their states), so a warp covers 512 groups per
+  // step; the live ones are gathered in wb with one ballot per position and
+  // offered 32 at a time.
+  const bool vec_flag = spec.flag && (((uintptr_t)spec.flag & 15) == 0);
+  const bool vec_state = spec.state && (((uintptr_t)spec.state & 15) == 0);
   uint32_t cnt = 0;
-  for (uint64_t base = lo + (uint64_t)warp * 32 * R; base < hi; base += (uint64_t)THREADS * R) {
-    bool live[R];
+  for (uint64_t base = lo + (uint64_t)warp * 512; base < hi; base += (uint64_t)THREADS * 16) {
+    const uint64_t g0 = base + (uint64_t)lane * 16;
+    uint32_t m16 = 0;  // bit j: group g0 + j is live
+    if (g0 < hi) {
+      const uint32_t nin = hi - g0 >= 16 ? 16u : (uint32_t)(hi - g0);
+      m16 = nin == 16 ? 0xFFFFu : ((1u << nin) - 1u);
+      if (spec.flag) {
+        uint32_t f = 0;
+        if (vec_flag && nin == 16) {
+          const uint4 v = *(const uint4*)(spec.flag + g0);
+          f = nz_bytes(v.x) | (nz_bytes(v.y) << 4) | (nz_bytes(v.z) << 8) | (nz_bytes(v.w) << 12);
+        } else {
+          for (uint32_t j = 0; j < nin; ++j) f |= (spec.flag[g0 + j] != 0 ? 1u : 0u) << j;
+        }
+        m16 &= f;
+      }
+      if (spec.state) {
+        uint32_t f = 0;
+        if (vec_state && nin == 16) {
 #pragma unroll
-    for (int r = 0; r < R; ++r) {
-      const uint64_t g = base + (uint64_t)r * 32 + lane;
-      live[r] = g < hi;
+          for (int q = 0; q < 4; ++q) {
+            const uint4 v = *(const uint4*)(spec.state + g0 + 4 * q);
+            f |= ((v.x == 2u ? 1u : 0u) | (v.y == 2u ? 2u : 0u) | (v.z == 2u ? 4u : 0u) | (v.w == 2u ? 8u : 0u))
+                 << (4 * q);
+          }
+        } else {
+          for (uint32_t j = 0; j < nin; ++j) f |= (spec.state[g0 + j] == 2u ? 1u : 0u) << j;
+        }
+        m16 &= f;
+      }
     }
-    if (spec.flag) {
-#pragma unroll
-      for (int r = 0; r < R; ++r) live[r] = live[r] && spec.flag[base + (uint64_t)r * 32 + lane] != 0;
-    }
-    if (spec.state) {
-#pragma unroll
-      for (int r = 0; r < R; ++r) live[r] = live[r] && spec.state[base + (uint64_t)r * 32 + lane] == 2u;
-    }
-#pragma unroll
-    for (int r = 0; r < R; ++r) {
-      const uint32_t m = __ballot_sync(0xFFFFFFFFu, live[r]);
-      if (live[r]) wb[cnt + __popc(m & lt)] = (uint32_t)(base + (uint64_t)r * 32 + lane);
+    if (!__any_sync(0xFFFFFFFFu, m16 != 0)) continue;
+#pragma unroll 1
+    for (int j = 0; j < 16; ++j) {
+      const bool lv = (m16 >> j) & 1u;
+      const uint32_t m = __ballot_sync(0xFFFFFFFFu, lv);
+      if (!m) continue;  // warp-uniform
+      if (lv) wb[cnt + __popc(m & lt)] = (uint32_t)(g0 + (uint64_t)j);
       cnt += __popc(m);
-    }
-    __syncwarp();
-    while (cnt >= 32) {
-      process(32);
-      __syncwarp();
-      const uint32_t rest = cnt - 32;
-      uint32_t x[R + 1];
-#pragma unroll
-      for (int q = 0; q <= R; ++q) x[q] = (uint32_t)(q * 32 + lane) < rest ? wb[32 + q * 32 + lane] : 0u;
-      __syncwarp();
-#pragma unroll
-      for (int q = 0; q <= R; ++q)
-        if ((uint32_t)(q * 32 + lane) < rest) wb[q * 32 + lane] = x[q];
-      cnt = rest;
+      if (cnt >= 32) {  // warp-uniform: offer 32, keep the rest (< 32)
+        __syncwarp();
+        process(32);
+        __syncwarp();
+        const uint32_t rest = cnt - 32;
+        const uint32_t x = (uint32_t)lane < rest ? wb[32 + lane] : 0u;
+        __syncwarp();
+        if ((uint32_t)lane < rest) wb[lane] = x;
+        cnt = rest;
+      }
       __syncwarp();
     }
   }
@@ -670,11 +699,11 @@ __global__ void __launch_bounds__(THREADS) k_topk_final(const __grid_constant__ 
 }
 
 constexpr int kTfThreads = 256;  // first pass
-constexpr int kTfItems = 4;      // groups per lane per step
+constexpr int kTfItems = 16;     // groups per lane per step
 static unsigned topk_final_ctas(uint64_t n_max, unsigned max_ctas) {
   static int per_sm = 0;
   if (!per_sm) {
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_topk_final<kTfThreads, kTfItems>, kTfThreads, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_topk_final<kTfThreads>, kTfThreads, 0);
     if (per_sm <= 0) per_sm = 1;
   }
   uint64_t ctas = (uint64_t)sms() * (uint64_t)per_sm;
@@ -704,9 +733,9 @@ cudaError_t launch_topk_final(const TopkFinalSpec& spec, int k, uint32_t* out_g,
   TopkFinalState* gst = (TopkFinalState*)temp;
   SortItem* pk = (SortItem*)((uint8_t*)temp + 256);
   uint32_t* pi = (uint32_t*)(pk + (uint64_t)ctas * k);
-  k_topk_final<kTfThreads, kTfItems><<<ctas, kTfThreads, 0, s>>>(spec, k, gst, pk, pi);
+  k_topk_final<kTfThreads><<<ctas, kTfThreads, 0, s>>>(spec, k, gst, pk, pi);
   k_topk_warp<1024><<<1, 1024, 0, s>>>(pk, pi, (const uint64_t*)&gst->n_cand, (uint64_t)ctas * k, k, nullptr, out_g,
-                                       out_count, 1, nullptr, (uint64_t*)gst);
+                                       out_count, 1, nullptr, (uint64_t*)gst, spec.total_bits);
   return cudaGetLastError();
 }
 
