@@ -16,6 +16,7 @@
 namespace mtl {
 
 // ------------------------------------------------------------ limits
+constexpr int kMatScanTiles = 4096;  // tiles per chunk of the two-pass compaction's scan
 constexpr int kMaxSrc = 6;       // tables in one query
 constexpr int kMaxPreds = 12;    // filter predicates in one pipeline
 constexpr int kMaxProbes = 5;    // join probes in one pipeline
@@ -182,6 +183,8 @@ enum SinkKind : int32_t {
   SK_PART_COUNT = 7,   // count the surviving rows per key partition, per CTA
   SK_PART_SCATTER = 8, // write (key, values) records into their partitions
   SK_AGG_FEW = 9,      // one pass into per-CTA tables of every group (k_agg_few, not a pipeline)
+  SK_MAT_COUNT = 10,   // two-pass order-preserving compaction: survivors per tile
+  SK_MAT_WRITE = 11,   // two-pass order-preserving compaction: outputs at scanned offsets
 };
 
 // Hash aggregate table (SoA). State word: 0 empty, 1 claimed, 2 ready.
@@ -248,6 +251,11 @@ struct PipeDesc {
   uint32_t* tile_counter;           // dynamic tile ids + finished CTAs
   uint32_t epoch;                   // look-back epoch (no memset per launch)
   uint32_t lb_spin_limit;           // polls before a look-back wait gives up (0: kSpinLimit)
+  // two-pass compaction (SK_MAT_COUNT, then SK_MAT_WRITE): per 256-row tile
+  // its survivors, then (after the scan) its offset within its chunk of
+  // kMatScanTiles tiles; chunk_pos[c] = rows before chunk c
+  uint32_t* tile_pos;
+  uint64_t* chunk_pos;
   int32_t lb_stall_first;           // failure injection: tile 0 never publishes its prefix
   // aggregates
   int32_t n_aggs;

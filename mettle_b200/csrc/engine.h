@@ -187,7 +187,8 @@ struct Step {
   enum Kind {
     MEMSET, FILL, PIPELINE, COMPACT_FLAGS, COMPACT_READY, FINALIZE, ENCODE, RADIX, TOPK, TOPK_FINAL, GATHER,
     PART_SCAN, PART_AGG,  // partitioned aggregation (descriptor in `pipe`)
-    AGG_FEW               // one-pass few-group aggregation (descriptor in `pipe`)
+    AGG_FEW,              // one-pass few-group aggregation (descriptor in `pipe`)
+    MAT_SCAN              // scan between the two passes of the compaction (descriptor in `pipe`)
   } k;
   std::string name;  // for per-step profiles, e.g. "pipeline:agg_slot:lineitem"
   // MEMSET / FILL (u64 words)
@@ -276,6 +277,7 @@ struct Program {
   std::vector<std::pair<int64_t, double>> last_lits;
   bool last_ok = false;
   std::string agg_strategy_key;  // autotuner key of a one-key aggregate's strategy ("" none)
+  std::string mat_strategy_key;  // autotuner key of the compaction's strategy ("" none)
   ~Program();
 };
 
@@ -395,6 +397,10 @@ double tune_load_factor(Ctx& ctx, const char* what, uint64_t rows);
 // shared-memory tables, 2 partitioned passes.
 std::string tune_key_agg(uint64_t groups, uint64_t rows);
 int tune_agg_strategy(Ctx& ctx, uint64_t groups, uint64_t rows);
+// Order-preserving compaction: 0 default (two passes), 1 one pass with a
+// decoupled look-back, 2 two passes.
+std::string tune_key_mat(uint64_t rows);
+int tune_mat_strategy(Ctx& ctx, uint64_t rows);
 std::string tune_file_path(const Ctx& ctx);
 std::string autotune(Ctx& ctx, const BoundPlan& plan, int reps);
 

@@ -835,7 +835,7 @@ struct Compiler {
         d.sink == SK_PART_SCATTER)
       for (int a = 0; a < d.n_aggs; ++a)
         if (d.aggs[a].prog >= 0) prog_cols(d.progs[d.aggs[a].prog], sink);
-    if (d.sink == SK_MATERIALIZE)
+    if (d.sink == SK_MATERIALIZE || d.sink == SK_MAT_WRITE)
       for (int q = 0; q < d.n_out; ++q) prog_cols(d.progs[d.out_prog[q]], sink);
     d.n_sink_cols = (int)std::min<size_t>(sink.size(), 6);
     for (int i = 0; i < d.n_sink_cols; ++i) d.sink_cols[i] = sink[i];
@@ -904,7 +904,8 @@ struct Compiler {
 
   void push_pipeline(PipeBuilder& pb, uint64_t n_hint) {
     static const char* sinks[] = {"none",       "build",      "materialize", "agg_hash",    "agg_smem",
-                                  "agg_slot",   "agg_scalar", "part_count",  "part_scatter"};
+                                  "agg_slot",   "agg_scalar", "part_count",  "part_scatter",
+                                  "agg_few",    "mat_count",  "mat_write"};
     plan_columns(pb);
     Step s;
     s.k = Step::PIPELINE;
@@ -1433,9 +1434,35 @@ struct Compiler {
       pb.d.mat_src_mask = m;
       pb.d.out_count = (uint64_t*)scratch(8);
       pb.d.out_capacity = n_max;
+      const uint64_t tiles = (n_max + pipeline_warp_tile_rows() - 1) / pipeline_warp_tile_rows();
+      // Two passes by default: a count of each tile's survivors, a scan, and
+      // the write at known offsets (no wait on other tiles); the single pass
+      // with a decoupled look-back when the autotuner measured it faster (or
+      // a test injects a look-back stall).
+      const bool injected = ctx.inject_kind.load() == MTL_INJECT_LOOKBACK_STALL;
+      const int mstrat = injected ? 1 : tune_mat_strategy(ctx, root_rows);
+      P.mat_strategy_key = injected ? "" : tune_key_mat(root_rows);
+      if (mstrat != 1 && root_rows < (1ull << 32)) {
+        const uint64_t chunks = (tiles + kMatScanTiles - 1) / kMatScanTiles;
+        pb.d.tile_pos = (uint32_t*)scratch(std::max<uint64_t>(tiles, 1) * 4);
+        pb.d.chunk_pos = (uint64_t*)scratch(std::max<uint64_t>(chunks, 1) * 8);
+        PipeBuilder count = pb;
+        count.d.sink = SK_MAT_COUNT;
+        push_pipeline(count, root_rows);
+        Step sc;
+        sc.k = Step::MAT_SCAN;
+        sc.pipe = pb.d;
+        sc.n_hint = root_rows;
+        sc.name = "mat_scan";
+        P.steps.push_back(sc);
+        P.kernels += 2;
+        pb.d.sink = SK_MAT_WRITE;
+        push_pipeline(pb, root_rows);
+        order_and_limit(pb.d.out_count, n_max, {});
+        return;
+      }
       // look-back words for the smaller (warp) tiles, so that either kernel
       // can run the step
-      const uint64_t tiles = (n_max + pipeline_warp_tile_rows() - 1) / pipeline_warp_tile_rows();
       pb.d.tile_status = (uint64_t*)scratch(std::max<uint64_t>(tiles, 1) * 8);
       pb.d.tile_counter = (uint32_t*)scratch(8);
       pb.d.epoch = 1;
@@ -1573,7 +1600,9 @@ struct Compiler {
     // may run either way; the autotuner's measured choice decides
     const int strategy = cas_table && est_groups <= 1536 ? tune_agg_strategy(ctx, est_groups, root_rows) : 0;
     P.agg_strategy_key = cas_table && est_groups <= 1536 ? tune_key_agg(est_groups, root_rows) : "";
-    if (cas_table && strategy != 2 && push_few(pb, est_groups, root_rows)) {
+    // one pass by default only for the fewest groups (measured faster there;
+    // above them the partitioned passes win unless the autotuner says otherwise)
+    if (cas_table && (strategy == 1 || (strategy == 0 && est_groups <= 16)) && push_few(pb, est_groups, root_rows)) {
       // one pass over the columns into per-CTA tables
     } else if (cas_table && strategy != 1 && push_partitioned(pb, est_groups, root_rows, strategy == 2)) {
       // count, scan, scatter and per-partition aggregation are queued
@@ -1969,6 +1998,7 @@ static const char* step_kind_name(Step::Kind k) {
     case Step::PART_SCAN: return "part_scan";
     case Step::PART_AGG: return "part_agg";
     case Step::AGG_FEW: return "agg_few";
+    case Step::MAT_SCAN: return "mat_scan";
   }
   return "step";
 }
@@ -2013,6 +2043,7 @@ void run_program(Ctx& ctx, Program& p, cudaStream_t s) {
       case Step::PART_SCAN: CK(launch_part_scan(st.pipe, s)); break;
       case Step::PART_AGG: CK(launch_part_agg(st.pipe, st.n_hint, s)); break;
       case Step::AGG_FEW: CK(launch_agg_few(st.pipe, st.n_hint, s)); break;
+      case Step::MAT_SCAN: CK(launch_mat_scan(st.pipe, st.n_hint, s)); break;
     }
     if (p.profile) CK(cudaEventRecord(p.prof_ev[2 * i + 1], s));
   }

@@ -1264,11 +1264,20 @@ __global__ void __launch_bounds__(kThreads, (SINK == SK_AGG_SCALAR || SINK == SK
     }
 
     // ---- sink over the surviving rows (sorted: ballots keep row order)
-    if (SINK == SK_MATERIALIZE) {
+    if (SINK == SK_MAT_COUNT) {
+      // first pass of the two-pass compaction: the tile's survivors
+      if (lane == 0) d.tile_pos[tile] = n_sel;
+    } else if (SINK == SK_MATERIALIZE || SINK == SK_MAT_WRITE) {
       const uint32_t total = n_sel;
-      const uint64_t base = lb_exclusive_warp(d.tile_status, tile, total, d.epoch, d.status,
-                                              d.lb_spin_limit ? d.lb_spin_limit : kSpinLimit, !d.lb_stall_first);
-      if (lane == 0 && tile == n_tiles - 1) *d.out_count = base + total;
+      uint64_t base;
+      if (SINK == SK_MAT_WRITE) {
+        // second pass: the tile's offset from the scan of the first pass's counts
+        base = (uint64_t)d.tile_pos[tile] + d.chunk_pos[tile / kMatScanTiles];
+      } else {
+        base = lb_exclusive_warp(d.tile_status, tile, total, d.epoch, d.status,
+                                 d.lb_spin_limit ? d.lb_spin_limit : kSpinLimit, !d.lb_stall_first);
+        if (lane == 0 && tile == n_tiles - 1) *d.out_count = base + total;
+      }
       // write phase: one output column at a time over the compacted rows
       const uint32_t lim = base >= d.out_capacity ? 0u
                            : (uint32_t)(d.out_capacity - base < (uint64_t)total ? d.out_capacity - base : total);
@@ -1999,7 +2008,7 @@ size_t pipeline_smem_bytes(const PipeDesc& d) {
 // queries cost host time on every launch otherwise.
 static std::mutex g_occ_mu;
 static std::map<std::pair<int, size_t>, int> g_occ;
-static size_t g_smem_set[9];
+static size_t g_smem_set[16];  // indexed by sink
 
 template <int SINK>
 static cudaError_t launch_sink(const PipeDesc& d, uint64_t n_hint, cudaStream_t s) {
@@ -2055,6 +2064,82 @@ cudaError_t launch_part_scan(const PipeDesc& d, cudaStream_t s) {
   if (d.part_chunk == 0) return cudaErrorInvalidValue;
   k_part_scan<<<1, kScanThreads, 0, s>>>(d.part_counts, d.part_offsets, d.part_start, d.part_chunk_start, d.part_ctas,
                                          d.part_bits, d.part_chunk);
+  return cudaGetLastError();
+}
+
+// ------------------------------------------------- two-pass compaction scan
+// Between the two passes of the order-preserving compaction: the tiles'
+// survivor counts (tile_pos) become offsets within their chunk of
+// kMatScanTiles tiles, in place, and chunk_pos the rows before each chunk;
+// out_count gets the total. Two launches, no waits between CTAs.
+constexpr int kMatScanThreads = kMatScanTiles / 4;
+
+__global__ void __launch_bounds__(kMatScanThreads) k_mat_scan_local(uint32_t* __restrict__ pos, uint64_t n_tiles,
+                                                                     uint64_t* __restrict__ chunk_pos) {
+  __shared__ uint32_t s_warp[kMatScanThreads / 32 + 1];
+  const uint64_t base = (uint64_t)blockIdx.x * kMatScanTiles + (uint64_t)threadIdx.x * 4;
+  uint32_t v[4], sum = 0;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    v[i] = base + i < n_tiles ? pos[base + i] : 0u;
+    sum += v[i];
+  }
+  uint32_t total;
+  uint32_t run = block_excl_sum<kMatScanThreads>(sum, s_warp, &total);
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+    if (base + i < n_tiles) {
+      pos[base + i] = run;
+      run += v[i];
+    }
+  if (threadIdx.x == 0) chunk_pos[blockIdx.x] = total;
+}
+
+__global__ void __launch_bounds__(kMatScanThreads) k_mat_scan_chunks(uint64_t* __restrict__ chunk_pos,
+                                                                      uint32_t n_chunks, uint64_t* out_count) {
+  __shared__ uint64_t s_w[kMatScanThreads / 32];
+  const uint32_t b = threadIdx.x * 4;
+  uint64_t v[4], sum = 0;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    v[i] = b + i < n_chunks ? chunk_pos[b + i] : 0ull;
+    sum += v[i];
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint64_t incl = sum;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint64_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+    if (lane >= o) incl += y;
+  }
+  if (lane == 31) s_w[warp] = incl;
+  __syncthreads();
+  if (warp == 0) {
+    uint64_t w = s_w[lane];
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint64_t y = __shfl_up_sync(0xFFFFFFFFu, w, o);
+      if (lane >= o) w += y;
+    }
+    s_w[lane] = w;  // inclusive over warps
+  }
+  __syncthreads();
+  uint64_t run = (warp ? s_w[warp - 1] : 0ull) + incl - sum;
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+    if (b + i < n_chunks) {
+      chunk_pos[b + i] = run;
+      run += v[i];
+    }
+  if (threadIdx.x == 0) *out_count = s_w[kMatScanThreads / 32 - 1];
+}
+
+cudaError_t launch_mat_scan(const PipeDesc& d, uint64_t n_rows, cudaStream_t s) {
+  const uint64_t n_tiles = (n_rows + kTile - 1) / kTile;
+  const uint64_t n_chunks = (n_tiles + kMatScanTiles - 1) / kMatScanTiles;
+  if (n_chunks > (uint64_t)kMatScanTiles) return cudaErrorInvalidValue;  // beyond 2^32 rows
+  if (n_tiles) k_mat_scan_local<<<(unsigned)n_chunks, kMatScanThreads, 0, s>>>(d.tile_pos, n_tiles, d.chunk_pos);
+  k_mat_scan_chunks<<<1, kMatScanThreads, 0, s>>>(d.chunk_pos, (uint32_t)n_chunks, d.out_count);
   return cudaGetLastError();
 }
 
@@ -2287,6 +2372,8 @@ cudaError_t launch_pipeline(const PipeDesc& d, uint64_t n_hint, cudaStream_t s) 
     case SK_BUILD: return launch_sink<SK_BUILD>(d, n_hint, s);
     case SK_MATERIALIZE:
       return d.mat_warp_tiles ? launch_sink<SK_MATERIALIZE>(d, n_hint, s) : launch_pipeline_materialize(d, n_hint, s);
+    case SK_MAT_COUNT: return launch_sink<SK_MAT_COUNT>(d, n_hint, s);
+    case SK_MAT_WRITE: return launch_sink<SK_MAT_WRITE>(d, n_hint, s);
     case SK_AGG_HASH: return launch_sink<SK_AGG_HASH>(d, n_hint, s);
     case SK_AGG_SMEM: return launch_sink<SK_AGG_SMEM>(d, n_hint, s);
     case SK_AGG_SLOT: return launch_sink<SK_AGG_SLOT>(d, n_hint, s);

@@ -12,6 +12,12 @@ namespace mtl {
 // ---- pipeline (k_pipeline.cu)
 size_t pipeline_tile_rows();
 size_t pipeline_warp_tile_rows();  // rows of a warp-tile (k_pipeline.cu)
+// Two-pass order-preserving compaction (k_pipeline.cu): an SK_MAT_COUNT
+// pipeline writes each 256-row tile's survivors into d.tile_pos,
+// launch_mat_scan turns them into offsets (d.tile_pos within chunks of
+// kMatScanTiles tiles, d.chunk_pos per chunk, *d.out_count the total), and an
+// SK_MAT_WRITE pipeline over the same rows and ops writes the outputs there.
+cudaError_t launch_mat_scan(const PipeDesc& d, uint64_t n_rows, cudaStream_t s);
 size_t pipeline_smem_bytes(const PipeDesc& d);
 // n_hint bounds the tuples (grid sizing when the count lives on the device).
 cudaError_t launch_pipeline(const PipeDesc& d, uint64_t n_hint, cudaStream_t s);

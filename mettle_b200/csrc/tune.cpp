@@ -167,6 +167,17 @@ int tune_agg_strategy(Ctx& ctx, uint64_t groups, uint64_t rows) {
   return 0;
 }
 
+std::string tune_key_mat(uint64_t rows) { return "materialize_strategy/n" + std::to_string(log2_class(rows)); }
+
+static thread_local int t_force_mat_strategy = 0;
+
+int tune_mat_strategy(Ctx& ctx, uint64_t rows) {
+  if (t_force_mat_strategy) return t_force_mat_strategy;
+  double a = 0, b = 0;
+  if (tune_lookup(ctx, tune_key_mat(rows), &a, &b) && (a == 1 || a == 2)) return (int)a;
+  return 0;
+}
+
 // ------------------------------------------------------------ tuning runs
 namespace {
 
@@ -244,12 +255,44 @@ std::string autotune(Ctx& ctx, const BoundPlan& plan, int reps) {
     rep << "chose load factor " << best_lf << "\n";
   }
   // one-key aggregate over few groups: one pass into shared-memory tables
-  // against the partitioned passes
-  std::string agg_key;
+  // against the partitioned passes; order-preserving compaction: one pass
+  // with a look-back against two passes
+  std::string agg_key, mat_key;
   {
     auto probe = compile(ctx, plan);
     agg_key = probe->agg_strategy_key;
+    mat_key = probe->mat_strategy_key;
     free_program(ctx, *probe);
+  }
+  if (!mat_key.empty()) {
+    double best_t = 1e30;
+    int best = 2;
+    for (int strat : {2, 1}) {
+      t_force_mat_strategy = strat;
+      std::unique_ptr<Program> p;
+      try {
+        p = compile(ctx, plan);
+      } catch (...) {
+        t_force_mat_strategy = 0;
+        throw;
+      }
+      t_force_mat_strategy = 0;
+      double t = 1e30;
+      try {
+        t = total(run_steps(ctx, *p, s, reps));
+      } catch (...) {
+        free_program(ctx, *p);
+        throw;
+      }
+      free_program(ctx, *p);
+      rep << "compaction " << (strat == 1 ? "in one pass (look-back)" : "in two passes (count, scan, write)") << ": "
+          << t << " ms\n";
+      if (t < best_t * 0.98) {
+        best_t = t;
+        best = strat;
+      }
+    }
+    tune_store(ctx, mat_key, best, 0);
   }
   if (!agg_key.empty()) {
     double best_t = 1e30;

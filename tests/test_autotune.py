@@ -86,15 +86,24 @@ def test_autotuned_shapes_keep_group_by_and_scan_exact(tmp_path, monkeypatch, bu
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("warp_tiles", [False, True])
-def test_materialize_tile_shapes_keep_row_order(tmp_path, monkeypatch, built_lib, warp_tiles):
-    """Order-preserving compaction with 1024-row CTA tiles or 256-row warp
-    tiles (each warp with its own look-back): the same rows in the same
-    order, bit-exact against the oracle."""
+@pytest.mark.parametrize("variant", ["two_pass", "lookback_cta_tiles", "lookback_warp_tiles"])
+def test_materialize_strategies_keep_row_order(tmp_path, monkeypatch, built_lib, variant):
+    """Order-preserving compaction in two passes (count, scan, write: the
+    default), or in one pass with a decoupled look-back over 1024-row CTA
+    tiles or 256-row warp tiles (each warp with its own look-back), chosen
+    through the autotuner's table: the same rows in the same order,
+    bit-exact against the oracle."""
     import numpy as np
     from mettle_b200 import _lib as L
     path = tmp_path / "tune.txt"
     monkeypatch.setenv("METTLE_TUNE_FILE", str(path))
+    lines = []
+    if variant != "two_pass":
+        lines.append("materialize_strategy/n22 1 0")  # 3*10^6 rows: size class 2^22
+    if variant == "lookback_warp_tiles":
+        # the scan streams a, b and c (16 bytes per row)
+        lines.append("pipeline:materialize/n22/s16/p0/a0 2 256")
+    path.write_text("".join(x + "\n" for x in lines))
     d = W.scan(3_000_000, seed_salt=4)
     sql = W.scan_sql("a", "<", 0.5)
     with Connection() as conn:
@@ -102,19 +111,33 @@ def test_materialize_tile_shapes_keep_row_order(tmp_path, monkeypatch, built_lib
         conn.create_table("t", {"a": (L.T_INTEGER, d["a"]), "b": (L.T_BIGINT, d["b"]), "c": (L.T_FLOAT, d["c"]),
                                 "d": (L.T_DATE, d["d"]), "e": (L.T_TIMESTAMP, d["e"])})
         conn.gpu_register_table("t")
-        conn.autotune(sql, reps=1)
-    text = path.read_text()
-    assert "pipeline:materialize" in text
-    path.write_text(re.sub(r"^(pipeline:materialize\S*) \S+ \S+$", rf"\1 2 {256 if warp_tiles else 1024}",
-                           text, flags=re.M))
-    with Connection() as conn:
-        conn.execute("CALL gpu_buffer_init('2 GB', '2 GB')")
-        conn.create_table("t", {"a": (L.T_INTEGER, d["a"]), "b": (L.T_BIGINT, d["b"]), "c": (L.T_FLOAT, d["c"]),
-                                "d": (L.T_DATE, d["d"]), "e": (L.T_TIMESTAMP, d["e"])})
-        conn.gpu_register_table("t")
+        st = conn.prepare(sql)
+        st.set_profiling(True)
+        st.launch()
+        st.fetch()
+        names = [n for n, _ in st.step_times()]
+        st.close()
+        if variant == "two_pass":
+            assert "mat_scan" in names, names
+        else:
+            assert any(n.startswith("pipeline:materialize") for n in names), names
         r = conn.gpu_processing(sql)
         rows = orc.filter_rows([(d["a"], "<", int(0.5 * 2**31))])
         assert np.array_equal(r.columns[0], orc.gather(d["a"], rows))
         assert np.array_equal(r.columns[1], orc.gather(d["b"], rows, "+", 5))
         assert np.array_equal(r.columns[2], orc.gather(d["c"], rows, "*", np.float32(10)))
         assert np.array_equal(r.columns[4], orc.gather(d["e"], rows))
+
+
+@pytest.mark.gpu
+def test_autotune_measures_both_compactions(tmp_path, monkeypatch, built_lib):
+    from mettle_b200 import _lib as L
+    monkeypatch.setenv("METTLE_TUNE_FILE", str(tmp_path / "tune.txt"))
+    d = W.scan(2_000_000, seed_salt=6)
+    with Connection() as conn:
+        conn.execute("CALL gpu_buffer_init('2 GB', '2 GB')")
+        conn.create_table("t", {"a": (L.T_INTEGER, d["a"]), "b": (L.T_BIGINT, d["b"]), "c": (L.T_FLOAT, d["c"]),
+                                "d": (L.T_DATE, d["d"]), "e": (L.T_TIMESTAMP, d["e"])})
+        conn.gpu_register_table("t")
+        report = conn.autotune(W.scan_sql("d", ">=", 0.1), reps=1)
+        assert "compaction in one pass" in report and "compaction in two passes" in report

@@ -190,10 +190,15 @@ C3_ALL_GROUPS_SQL = ("SELECT k, SUM(v), COUNT(*), MIN(v), MAX(v), AVG(v), SUM(f)
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("groups,dist", [(10, "uniform"), (100, "zipf"), (1000, "uniform"), (1000, "zipf")])
-def test_c3_few_groups_one_pass_all_groups(conn, groups, dist):
+def test_c3_few_groups_one_pass_all_groups(conn, tmp_path, monkeypatch, groups, dist):
     """Few groups: one pass over the columns into per-CTA shared-memory tables
-    (the plan's agg_few step), with a warp's rows of one group combined before
-    they update; every group on all ten aggregates against the oracle."""
+    (the plan's agg_few step; chosen through the autotuner's table above 16
+    groups), with a warp's rows of one group combined before they update;
+    every group on all ten aggregates against the oracle."""
+    g = max(1, (groups - 1).bit_length())  # size classes: log2, rounded up
+    path = tmp_path / "tune.txt"
+    path.write_text(f"agg_one_key/g{g}/n23 1 0\n")  # 6*10^6 rows: class 2^23
+    monkeypatch.setenv("METTLE_TUNE_FILE", str(path))
     init(conn)
     d = W.groupby(n=6_000_000, groups=groups, dist=dist, seed_salt=groups + 5)
     conn.create_table("t", {"k": (L.T_BIGINT, d["k"]), "v": (L.T_BIGINT, d["v"]), "f": (L.T_FLOAT, d["f"])})
@@ -207,10 +212,13 @@ def test_c3_few_groups_one_pass_all_groups(conn, groups, dist):
 
 
 @pytest.mark.gpu
-def test_few_groups_edge_keys_and_wide_sums(conn):
+def test_few_groups_edge_keys_and_wide_sums(conn, tmp_path, monkeypatch):
     """The one-pass path with the empty-slot sentinel key and both int64
     extremes as keys (the sentinel's rows update the global table directly)
     and sums that need 128 bits (no combining)."""
+    path = tmp_path / "tune.txt"
+    path.write_text("agg_one_key/g6/n22 1 0\n")  # 53 groups over 3*10^6 rows
+    monkeypatch.setenv("METTLE_TUNE_FILE", str(path))
     init(conn)
     r = np.random.default_rng(77)
     n = 3_000_000
