@@ -1923,7 +1923,10 @@ __global__ void __launch_bounds__(kPartAggThreads, 2) k_part_agg(const __grid_co
       idx[q] = -1;
       g[q] = kNoGroup;
       if (upd[q]) {
-        idx[q] = smem_cas_find(s, key[q], probes, d.part_bits);
+        // the default window as a constant: the loop then compiles as in
+        // the common case it is (a short window only for overfull tables)
+        idx[q] = probes == kPartProbes ? smem_cas_find(s, key[q], kPartProbes, d.part_bits)
+                                       : smem_cas_find(s, key[q], probes, d.part_bits);
         if (idx[q] < 0) g[q] = agg_find_cas(tb, key[q], hash_slot(key_hash1(key[q]), tb.capacity), st);
       }
     }
