@@ -392,6 +392,7 @@ struct Compiler {
   int cur_owner = -1;
   void memset_step(void* p, int byte, uint64_t bytes) {
     FillSeg f;
+    memset(&f, 0, sizeof(f));
     f.ptr = p;
     f.bytes = (bytes + 15) & ~15ULL;
     f.pattern = 0x0101010101010101ULL * (uint64_t)(byte & 0xFF);
@@ -401,6 +402,7 @@ struct Compiler {
   }
   void fill_step(void* p, uint64_t words, uint64_t v) {
     FillSeg f;
+    memset(&f, 0, sizeof(f));
     f.ptr = p;
     f.bytes = (words * 8 + 15) & ~15ULL;
     f.pattern = v;
@@ -408,9 +410,21 @@ struct Compiler {
     fills.push_back(f);
     fill_owner.push_back(cur_owner);
   }
+  // n entries of stride_words words (even), each a copy of entry_dev
+  void fill_entries(void* p, uint64_t n, uint64_t stride_words, const uint64_t* entry_dev) {
+    FillSeg f;
+    memset(&f, 0, sizeof(f));
+    f.ptr = p;
+    f.bytes = n * stride_words * 8;
+    f.entry = entry_dev;
+    f.entry_words = stride_words;
+    fills.push_back(f);
+    fill_owner.push_back(cur_owner);
+  }
   // one 8-byte word every stride_words words, n times
   void fill_strided(void* p, uint64_t n, uint64_t stride_words, uint64_t v) {
     FillSeg f;
+    memset(&f, 0, sizeof(f));
     f.ptr = p;
     f.bytes = n * stride_words * 8;
     f.pattern = v;
@@ -1576,16 +1590,19 @@ struct Compiler {
       state_stride = (int)stride;
       pb.d.table.keys[0] = aos;
       pb.d.table.stride = (int32_t)stride;
-      fill_strided(aos, n_ent, stride, ~0ULL);
+      // every entry starts as: empty key, state identities, zero high
+      // words; written whole, in one pass over the table
+      std::vector<uint64_t> entry(stride, 0);
+      entry[0] = ~0ULL;
       uint64_t hw = 1 + states.size();
       for (size_t s = 0; s < states.size(); ++s) {
         states[s].lo = aos + 1 + s;
-        fill_strided(states[s].lo, n_ent, stride, state_identity(states[s].fn_dev));
-        if (states[s].fn_dev == A_SUM_I128) {
-          states[s].hi = (int64_t*)(aos + hw++);
-          fill_strided(states[s].hi, n_ent, stride, 0);
-        }
+        entry[1 + s] = state_identity(states[s].fn_dev);
+        if (states[s].fn_dev == A_SUM_I128) states[s].hi = (int64_t*)(aos + hw++);
       }
+      uint64_t* entry_dev = (uint64_t*)scratch(stride * 8);
+      upload(entry_dev, entry.data(), stride * 8);
+      fill_entries(aos, n_ent, stride, entry_dev);
     } else {
       pb.d.table.stride = 1;
     }

@@ -327,6 +327,15 @@ __global__ void k_fill_segments(const FillSeg* __restrict__ segs) {
     return;
   }
   const uint64_t n16 = sg.bytes / 16;
+  if (sg.entry) {
+    const uint64_t h = sg.entry_words / 2;  // 16-byte pieces per entry
+    ulonglong2* p = (ulonglong2*)sg.ptr;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n16; i += (uint64_t)gridDim.x * blockDim.x) {
+      const uint64_t w = 2 * (i % h);
+      p[i] = make_ulonglong2(__ldg(sg.entry + w), __ldg(sg.entry + w + 1));
+    }
+    return;
+  }
   const ulonglong2 v = make_ulonglong2(sg.pattern, sg.pattern);
   ulonglong2* p = (ulonglong2*)sg.ptr;
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n16; i += (uint64_t)gridDim.x * blockDim.x)

@@ -179,6 +179,10 @@ struct FillSeg {
   uint64_t bytes;
   uint64_t pattern;
   uint64_t stride;  // 0: fill [ptr, ptr + bytes); else one 8-byte word every `stride` bytes
+  // non-null (with stride 0): whole entries of entry_words words (even), word
+  // w of the segment set to entry[w % entry_words], in 16-byte stores
+  const uint64_t* entry;
+  uint64_t entry_words;
 };
 cudaError_t launch_fill_segments(const FillSeg* segs_dev, int n_segs, uint64_t max_bytes, cudaStream_t s);
 
