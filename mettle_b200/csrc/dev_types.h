@@ -17,6 +17,7 @@ namespace mtl {
 
 // ------------------------------------------------------------ limits
 constexpr int kMatScanTiles = 4096;  // tiles per chunk of the two-pass compaction's scan
+constexpr int kMaxStream = 6;        // columns a warp-tile pipeline stages into shared memory
 constexpr int kMaxSrc = 6;       // tables in one query
 constexpr int kMaxPreds = 12;    // filter predicates in one pipeline
 constexpr int kMaxProbes = 5;    // join probes in one pipeline
@@ -230,7 +231,7 @@ struct PipeDesc {
   // them is staged into shared memory with bulk (TMA) copies, double
   // buffered, so their HBM traffic is in flight independently of registers.
   int32_t n_stream;
-  int32_t stream_cols[4];
+  int32_t stream_cols[kMaxStream];
 
   // sink
   int32_t sink;

@@ -857,6 +857,14 @@ struct Compiler {
     d.n_stream = 0;
     if (d.tuple_input) return;
     uint32_t budget = 16;  // bytes per tuple: 64 KB of double-buffered tiles
+    int max_stream = 4;
+    // the write pass of the two-pass compaction reads every output column
+    // of about every surviving row: all of them are staged (up to 32 bytes
+    // a row), so the write phase reads shared memory only
+    if (d.sink == SK_MAT_WRITE) {
+      budget = 32;
+      max_stream = kMaxStream;
+    }
     // the scatter pass reads every input of the records: 80 KB still lets
     // two of its CTAs share an SM
     if (d.sink == SK_PART_SCATTER) budget = 20;
@@ -868,7 +876,7 @@ struct Compiler {
     }
     uint32_t used = 0;
     auto try_stream = [&](int col) {
-      if (d.cols[col].src != d.drive_src || d.n_stream >= 4) return;
+      if (d.cols[col].src != d.drive_src || d.n_stream >= max_stream) return;
       for (int i = 0; i < d.n_stream; ++i)
         if (d.stream_cols[i] == col) return;
       uint32_t w = (uint32_t)ptype_width(d.cols[col].ptype);
@@ -1688,7 +1696,10 @@ struct Compiler {
     int bits = 0;
     auto part_bits = [](int32_t pt) { return pt == P_I128 ? 128 : (pt == P_I32 || pt == P_F32) ? 32 : 64; };
     auto add_part = [&](int out_i, bool desc) {
-      const int32_t pt = dense[out_i].ptype;
+      // a 128-bit output holding a 64-bit sum orders by its 64-bit image: its
+      // high word is only the sign, and the leading key bits (the pruning
+      // cut) then carry the sum itself
+      const int32_t pt = fo[out_i].kind == F_SUM_I64_AS_I128 ? P_I64 : dense[out_i].ptype;
       if (bits + part_bits(pt) > 256 || ts.n_parts >= kMaxOrder) return false;
       ts.ptype[ts.n_parts] = pt;
       ts.desc[ts.n_parts] = desc ? 1 : 0;

@@ -499,15 +499,15 @@ constexpr int kTile = 256;                // rows per warp-tile
 
 struct StreamLayout {
   int n;
-  int col[4];
-  int width[4];
-  uint32_t off[4];
+  int col[kMaxStream];
+  int width[kMaxStream];
+  uint32_t off[kMaxStream];
   uint32_t bytes;  // per buffer
 };
 
 __host__ __device__ inline uint32_t stream_bytes_per_row(const PipeDesc& d) {
   uint32_t w = 0;
-  for (int i = 0; i < d.n_stream && i < 4; ++i) w += (uint32_t)ptype_width(d.cols[d.stream_cols[i]].ptype);
+  for (int i = 0; i < d.n_stream && i < kMaxStream; ++i) w += (uint32_t)ptype_width(d.cols[d.stream_cols[i]].ptype);
   return w;
 }
 
@@ -532,7 +532,7 @@ __device__ __forceinline__ uint32_t tc_rid(const TileCtx& t, int src, uint32_t r
 __device__ __forceinline__ int stream_index(const StreamLayout& S, int col) {
   int k = -1;
 #pragma unroll
-  for (int i = 0; i < 4; ++i)
+  for (int i = 0; i < kMaxStream; ++i)
     if (i < S.n && S.col[i] == col) k = i;
   return k;
 }
@@ -894,11 +894,11 @@ __global__ void __launch_bounds__(kThreads, (SINK == SK_AGG_SCALAR || SINK == SK
   uint32_t st = 0;
 
   StreamLayout S;
-  S.n = d.n_stream < 4 ? d.n_stream : 4;
+  S.n = d.n_stream < kMaxStream ? d.n_stream : kMaxStream;
   {
     uint32_t off = 0;
 #pragma unroll
-    for (int i = 0; i < 4; ++i) {
+    for (int i = 0; i < kMaxStream; ++i) {
       S.col[i] = i < S.n ? d.stream_cols[i] : -1;
       S.width[i] = i < S.n ? ptype_width(d.cols[S.col[i]].ptype) : 0;
       S.off[i] = off;

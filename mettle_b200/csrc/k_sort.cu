@@ -706,8 +706,9 @@ static unsigned topk_final_ctas(uint64_t n_max, unsigned max_ctas) {
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_topk_final<kTfThreads>, kTfThreads, 0);
     if (per_sm <= 0) per_sm = 1;
   }
+  // one wave of CTAs, each covering at least one step of 16 groups per lane
   uint64_t ctas = (uint64_t)sms() * (uint64_t)per_sm;
-  const uint64_t want = (n_max + kTfThreads * kTfItems * 4 - 1) / (kTfThreads * kTfItems * 4);
+  const uint64_t want = (n_max + kTfThreads * kTfItems - 1) / (kTfThreads * kTfItems);
   if (want < ctas) ctas = want ? want : 1;
   if (max_ctas && ctas > max_ctas) ctas = max_ctas;
   return (unsigned)ctas;

@@ -60,7 +60,7 @@ static int log2_class(uint64_t n) {
 std::string tune_key_pipeline(const Step& s) {
   const PipeDesc& d = s.pipe;
   uint32_t stream = 0;
-  for (int i = 0; i < d.n_stream && i < 4; ++i) stream += (uint32_t)ptype_width(d.cols[d.stream_cols[i]].ptype);
+  for (int i = 0; i < d.n_stream && i < kMaxStream; ++i) stream += (uint32_t)ptype_width(d.cols[d.stream_cols[i]].ptype);
   // the step name without the table: "pipeline:<sink>"
   std::string kind = s.name.substr(0, s.name.rfind(':'));
   std::ostringstream k;
