@@ -234,6 +234,7 @@ struct Step {
   void* gout = nullptr;
   // TOPK_FINAL
   TopkFinalSpec tfs;
+  int topk_phase = 0;  // launch_topk_final's phase
   const uint32_t* remap = nullptr;  // TOPK: write remap[i] for winner i
 };
 

@@ -858,13 +858,8 @@ struct Compiler {
     if (d.tuple_input) return;
     uint32_t budget = 16;  // bytes per tuple: 64 KB of double-buffered tiles
     int max_stream = 4;
-    // the write pass of the two-pass compaction reads every output column
-    // of about every surviving row: all of them are staged (up to 32 bytes
-    // a row), so the write phase reads shared memory only
-    if (d.sink == SK_MAT_WRITE) {
-      budget = 32;
-      max_stream = kMaxStream;
-    }
+    // (staging every output column of the compaction's write pass, up to
+    // 32 bytes a row, halves its resident CTAs and measured no faster)
     // the scatter pass reads every input of the records: 80 KB still lets
     // two of its CTAs share an SM
     if (d.sink == SK_PART_SCATTER) budget = 20;
@@ -1735,6 +1730,10 @@ struct Compiler {
     t.out_count = oc;
     t.temp = scratch(topk_final_temp_bytes(cap, K));
     memset_step(t.temp, 0, 256);  // the launch's cross-CTA state starts at zero
+    t.topk_phase = 1;  // the first pass, then the merge as its own step
+    P.steps.push_back(t);
+    t.topk_phase = 2;
+    t.name = "topk_merge";
     P.steps.push_back(t);
     P.kernels += 2;
     std::vector<FinalOut> vis;
@@ -2066,7 +2065,9 @@ void run_program(Ctx& ctx, Program& p, cudaStream_t s) {
         CK(launch_topk(st.keys, st.kidx, st.count, st.n_max, st.topk, st.out_idx, st.out_count, st.temp, p.status,
                        s, st.remap));
         break;
-      case Step::TOPK_FINAL: CK(launch_topk_final(st.tfs, st.topk, st.out_idx, st.out_count, st.temp, s)); break;
+      case Step::TOPK_FINAL:
+        CK(launch_topk_final(st.tfs, st.topk, st.out_idx, st.out_count, st.temp, s, 0, st.topk_phase));
+        break;
       case Step::GATHER: CK(launch_gather_width(st.gin, st.width, st.idx, st.count, st.n_max, st.gout, s)); break;
       case Step::PART_SCAN: CK(launch_part_scan(st.pipe, s)); break;
       case Step::PART_AGG: CK(launch_part_agg(st.pipe, st.n_hint, s)); break;

@@ -655,25 +655,45 @@ __global__ void __launch_bounds__(THREADS) k_topk_final(const __grid_constant__ 
         m16 &= f;
       }
     }
-    if (!__any_sync(0xFFFFFFFFu, m16 != 0)) continue;
-#pragma unroll 1
-    for (int j = 0; j < 16; ++j) {
-      const bool lv = (m16 >> j) & 1u;
-      const uint32_t m = __ballot_sync(0xFFFFFFFFu, lv);
-      if (!m) continue;  // warp-uniform
-      if (lv) wb[cnt + __popc(m & lt)] = (uint32_t)(g0 + (uint64_t)j);
-      cnt += __popc(m);
-      if (cnt >= 32) {  // warp-uniform: offer 32, keep the rest (< 32)
-        __syncwarp();
-        process(32);
-        __syncwarp();
-        const uint32_t rest = cnt - 32;
-        const uint32_t x = (uint32_t)lane < rest ? wb[32 + lane] : 0u;
-        __syncwarp();
-        if ((uint32_t)lane < rest) wb[lane] = x;
-        cnt = rest;
+    // each lane appends its live groups at its prefix position; live groups
+    // are sparse, so a lane rarely has more than one
+    const uint32_t c = __popc(m16);
+    uint32_t incl = c;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+      if (lane >= o) incl += y;
+    }
+    const uint32_t total = __shfl_sync(0xFFFFFFFFu, incl, 31);
+    if (total == 0) continue;
+    // wb holds logical entries [shift, shift + 64); this step's entries take
+    // logical positions [cnt, cnt + total), this lane's from `pos`; every
+    // full batch of 32 is offered and the rest moves down
+    uint32_t pos = cnt + incl - c;
+    uint32_t bits = m16;
+    const uint32_t fill = cnt + total;
+    uint32_t shift = 0;
+    for (;;) {
+      while (bits && pos < shift + 64) {
+        const int j = __ffs(bits) - 1;
+        bits &= bits - 1;
+        wb[pos - shift] = (uint32_t)(g0 + (uint64_t)j);
+        ++pos;
       }
       __syncwarp();
+      const uint32_t have = (fill < shift + 64 ? fill : shift + 64) - shift;  // warp-uniform
+      if (have < 32) {
+        cnt = have;
+        break;
+      }
+      process(32);
+      __syncwarp();
+      const uint32_t rest = have - 32;
+      const uint32_t x = (uint32_t)lane < rest ? wb[32 + lane] : 0u;
+      __syncwarp();
+      if ((uint32_t)lane < rest) wb[lane] = x;
+      __syncwarp();
+      shift += 32;
     }
   }
   if (cnt) process(cnt);
@@ -725,7 +745,7 @@ unsigned topk_final_max_ctas_for(size_t temp_bytes, int k) {
 }
 
 cudaError_t launch_topk_final(const TopkFinalSpec& spec, int k, uint32_t* out_g, uint64_t* out_count, void* temp,
-                              cudaStream_t s, unsigned max_ctas) {
+                              cudaStream_t s, unsigned max_ctas, int phase) {
   if (k <= 0 || k > 32 || spec.n_parts <= 0 || spec.n_parts > kMaxOrder || spec.total_bits > 256 ||
       spec.bits0 <= 0 || spec.bits0 > spec.total_bits)
     return cudaErrorInvalidValue;
@@ -734,9 +754,10 @@ cudaError_t launch_topk_final(const TopkFinalSpec& spec, int k, uint32_t* out_g,
   TopkFinalState* gst = (TopkFinalState*)temp;
   SortItem* pk = (SortItem*)((uint8_t*)temp + 256);
   uint32_t* pi = (uint32_t*)(pk + (uint64_t)ctas * k);
-  k_topk_final<kTfThreads><<<ctas, kTfThreads, 0, s>>>(spec, k, gst, pk, pi);
-  k_topk_warp<1024><<<1, 1024, 0, s>>>(pk, pi, (const uint64_t*)&gst->n_cand, (uint64_t)ctas * k, k, nullptr, out_g,
-                                       out_count, 1, nullptr, (uint64_t*)gst, spec.total_bits);
+  if (phase != 2) k_topk_final<kTfThreads><<<ctas, kTfThreads, 0, s>>>(spec, k, gst, pk, pi);
+  if (phase != 1)
+    k_topk_warp<1024><<<1, 1024, 0, s>>>(pk, pi, (const uint64_t*)&gst->n_cand, (uint64_t)ctas * k, k, nullptr, out_g,
+                                         out_count, 1, nullptr, (uint64_t*)gst, spec.total_bits);
   return cudaGetLastError();
 }
 

@@ -144,8 +144,10 @@ struct TopkFinalSpec {
 size_t topk_final_temp_bytes(uint64_t n_max, int k, unsigned max_ctas = 0);
 // The largest max_ctas whose temp fits in temp_bytes.
 unsigned topk_final_max_ctas_for(size_t temp_bytes, int k);
+// phase: 0 both kernels, 1 the first pass only, 2 the merge pass only (the
+// two phases as separate steps of a program, each timed on its own).
 cudaError_t launch_topk_final(const TopkFinalSpec& spec, int k, uint32_t* out_g, uint64_t* out_count, void* temp,
-                              cudaStream_t s, unsigned max_ctas = 0);
+                              cudaStream_t s, unsigned max_ctas = 0, int phase = 0);
 
 // ---- gathers for final materialization (k_misc.cu)
 // out[i] = in[idx[i]] for fixed width elements (4, 8 or 16 bytes).
