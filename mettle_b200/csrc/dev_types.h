@@ -277,6 +277,7 @@ struct PipeDesc {
   int32_t part_words;
   int32_t part_nvals;               // inputs per record (value slots in use)
   int32_t part_combine;             // few keys per partition: combine a warp's records of one key
+  int32_t part_split;               // log2 of the CTAs sharing a chunk (each a share of its keys)
   int32_t part_ctas;
   uint32_t part_chunk;              // records per CTA of the per-partition aggregation
   int32_t part_val[kMaxAggs];

@@ -990,12 +990,22 @@ struct Compiler {
     d.part_combine = est / np < 128 ? 1 : 0;
     d.part_ctas = ctas;
     d.smem_capacity = (int32_t)cap;
-    d.smem_probes = overfull ? 8 : 0;  // 0: the kernel's default window
+    // Partitions holding more groups than a table are split: 2^split CTAs
+    // share each chunk (read from L2), each taking the keys of its share,
+    // so that every share fits about 60 % of a table.
+    int split = 0;
+    while (overfull && split < 6 && (uint64_t)((double)cap * 0.6) << (bits + split) < est) ++split;
+    const bool still_overfull = (uint64_t)((double)cap * 0.6) << (bits + split) < est;
+    d.part_split = split;
+    d.smem_probes = still_overfull ? 8 : 0;  // 0: the kernel's default window
     // records per CTA: half a partition's average, but small enough for
     // eight CTAs per SM, and at least 4096
     const uint64_t min_ctas = 4ull * (uint64_t)pipeline_part_ctas();
     d.part_chunk = (uint32_t)std::max<uint64_t>(
         4096, std::min<uint64_t>((rows + 2 * np - 1) / (2 * np), (rows + min_ctas - 1) / min_ctas));
+    // split partitions: about one chunk per partition, so that each group is
+    // merged into the global table once
+    if (split) d.part_chunk = (uint32_t)std::max<uint64_t>(4096, (rows + np - 1) / np * 5 / 4);
     d.part_records = (uint64_t*)scratch(rec_bytes);
     d.part_counts = (uint32_t*)scratch((uint64_t)ctas * np * 4);
     d.part_offsets = (uint32_t*)scratch((uint64_t)ctas * np * 4);

@@ -1834,7 +1834,13 @@ constexpr uint32_t kPartProbes = 64;
 __global__ void __launch_bounds__(kPartAggThreads, 2) k_part_agg(const __grid_constant__ PipeDesc d) {
   extern __shared__ __align__(128) uint8_t smem[];
   const uint32_t np = 1u << d.part_bits;
-  const uint32_t cb = blockIdx.x;
+  // With a split (partitions holding more groups than one table), 2^split
+  // CTAs share a chunk, each taking the records whose next hash bits select
+  // it; they read the chunk from L2 and each holds its share of the groups.
+  const uint32_t split = (uint32_t)d.part_split;
+  const uint32_t sub = blockIdx.x & ((1u << split) - 1u);
+  const uint32_t cb = blockIdx.x >> split;
+  const int sub_shift = 64 - d.part_bits - (int)split;
   if (cb >= d.part_chunk_start[np]) return;  // the whole CTA leaves, before any barrier
   // the chunk's partition: chunk_start[lo] <= cb < chunk_start[hi]
   uint32_t lo = 0, hi = np;
@@ -1879,19 +1885,26 @@ __global__ void __launch_bounds__(kPartAggThreads, 2) k_part_agg(const __grid_co
 #pragma unroll
       for (int v = 0; v < kPartMaxVals; ++v) val[q][v] = 0;
       if (act[q]) {
+        // streamed once (evict first), or kept in L2 for the other CTAs of a split chunk
         if (W == 1) {
-          key[q] = __ldcs(rec);
+          key[q] = split ? __ldcg(rec) : __ldcs(rec);
         } else {
           if (W == 4) {  // one 32-byte load
-            asm volatile("ld.global.cs.v4.u64 {%0, %1, %2, %3}, [%4];"
-                         : "=l"(key[q]), "=l"(val[q][0]), "=l"(val[q][1]), "=l"(val[q][2])
-                         : "l"(rec));
+            if (split)
+              asm volatile("ld.global.cg.v4.u64 {%0, %1, %2, %3}, [%4];"
+                           : "=l"(key[q]), "=l"(val[q][0]), "=l"(val[q][1]), "=l"(val[q][2])
+                           : "l"(rec));
+            else
+              asm volatile("ld.global.cs.v4.u64 {%0, %1, %2, %3}, [%4];"
+                           : "=l"(key[q]), "=l"(val[q][0]), "=l"(val[q][1]), "=l"(val[q][2])
+                           : "l"(rec));
           } else {
-            const ulonglong2 x = __ldcs((const ulonglong2*)rec);
+            const ulonglong2 x = split ? __ldcg((const ulonglong2*)rec) : __ldcs((const ulonglong2*)rec);
             key[q] = x.x;
             val[q][0] = x.y;
           }
         }
+        if (split) act[q] = ((uint32_t)(key_hash1(key[q]) >> sub_shift) & ((1u << split) - 1u)) == sub;
       }
     }
     // Records of one key in the same warp (a skewed key's) are combined in
@@ -1925,8 +1938,8 @@ __global__ void __launch_bounds__(kPartAggThreads, 2) k_part_agg(const __grid_co
       if (upd[q]) {
         // the default window as a constant: the loop then compiles as in
         // the common case it is (a short window only for overfull tables)
-        idx[q] = probes == kPartProbes ? smem_cas_find(s, key[q], kPartProbes, d.part_bits)
-                                       : smem_cas_find(s, key[q], probes, d.part_bits);
+        idx[q] = probes == kPartProbes ? smem_cas_find(s, key[q], kPartProbes, d.part_bits + (int)split)
+                                       : smem_cas_find(s, key[q], probes, d.part_bits + (int)split);
         if (idx[q] < 0) g[q] = agg_find_cas(tb, key[q], hash_slot(key_hash1(key[q]), tb.capacity), st);
       }
     }
@@ -2162,7 +2175,7 @@ cudaError_t launch_part_agg(const PipeDesc& d, uint64_t n_hint, cudaStream_t s) 
     }
   }
   // at most records / chunk + one partial chunk per partition
-  const uint64_t grid = n_hint / d.part_chunk + (1ull << d.part_bits);
+  const uint64_t grid = (n_hint / d.part_chunk + (1ull << d.part_bits)) << d.part_split;
   k_part_agg<<<(unsigned)grid, kPartAggThreads, smem, s>>>(d);
   return cudaGetLastError();
 }
