@@ -718,6 +718,132 @@ __global__ void __launch_bounds__(THREADS) k_topk_final(const __grid_constant__ 
   }
 }
 
+// Merge pass of the fused top-K by selection: one CTA reads the candidates'
+// leading 64 key bits into registers (kMsPer per thread), finds the K-th
+// smallest of them exactly with a radix select over 8-bit digits (a
+// shared-memory histogram per digit), keeps only the candidates at or below
+// it (the K best, plus ties on those bits), and orders those with the warp
+// lists. The candidates' count is not known on the host, so this runs when
+// their bound (CTAs x K of the first pass) fits kMsThreads x kMsPer; 16-bit
+// positions and 16 warps keep its static shared memory under 48 KB.
+constexpr int kMsThreads = 512;
+constexpr int kMsPer = 16;
+constexpr int kMsMax = kMsThreads * kMsPer;
+
+__global__ void __launch_bounds__(kMsThreads) k_topk_merge_select(const SortItem* __restrict__ keys,
+                                                                  const uint32_t* __restrict__ idx,
+                                                                  const uint64_t* count, uint64_t n_max, int K,
+                                                                  int cut_bits, uint32_t* __restrict__ out_idx,
+                                                                  uint64_t* out_count, uint64_t* reset) {
+  constexpr int WARPS = kMsThreads / 32;
+  __shared__ uint32_t s_hist[256];
+  __shared__ uint16_t s_sel[kMsMax];  // positions of the selected candidates
+  __shared__ uint32_t s_nsel;
+  __shared__ uint64_t s_prefix;
+  __shared__ uint32_t s_need;
+  __shared__ Cand s_l[WARPS][32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint64_t n = count ? *count : n_max;
+  if (n > n_max) n = n_max;
+  if (n > (uint64_t)kMsMax) n = kMsMax;  // the host launches this only below the bound
+  uint64_t t[kMsPer];
+  bool v[kMsPer];
+#pragma unroll
+  for (int r = 0; r < kMsPer; ++r) {
+    const uint64_t i = (uint64_t)r * kMsThreads + threadIdx.x;
+    v[r] = i < n && idx[i] != 0xFFFFFFFFu;
+    t[r] = 0;
+    if (v[r]) t[r] = key_top64(keys[i].w, cut_bits);
+  }
+  if (threadIdx.x == 0) {
+    s_prefix = 0;
+    s_need = (uint32_t)K;
+    s_nsel = 0;
+  }
+  // radix select of the K-th smallest leading word, most significant digit first
+  uint64_t mask = 0;
+  for (int shift = 56; shift >= 0; shift -= 8) {
+    for (int b = threadIdx.x; b < 256; b += kMsThreads) s_hist[b] = 0;
+    __syncthreads();
+    const uint64_t prefix = s_prefix;
+#pragma unroll
+    for (int r = 0; r < kMsPer; ++r)
+      if (v[r] && (t[r] & mask) == prefix) atomicAdd(&s_hist[(t[r] >> shift) & 255u], 1u);
+    __syncthreads();
+    if (warp == 0) {
+      // lane l holds bins [8l, 8l + 8): find the bin where the count reaches s_need
+      uint32_t c[8], sum = 0;
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        c[j] = s_hist[lane * 8 + j];
+        sum += c[j];
+      }
+      uint32_t incl = sum;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+        if (lane >= o) incl += y;
+      }
+      const uint32_t need = s_need;
+      const uint32_t total = __shfl_sync(0xFFFFFFFFu, incl, 31);
+      // fewer candidates than needed under this prefix: take them all (the
+      // largest digit keeps every one at or below the threshold)
+      const uint32_t want = need <= total ? need : total;
+      const uint32_t excl = incl - sum;
+      const bool mine = want > 0 && excl < want && want <= incl;
+      const uint32_t ball = __ballot_sync(0xFFFFFFFFu, mine);
+      if (ball == 0 && lane == 0) {  // no candidate under the prefix at all
+        s_prefix = prefix | (255ull << shift);
+      } else if (mine) {
+        uint32_t run = excl, d = 0;
+#pragma unroll
+        for (int j = 0; j < 8; ++j)
+          if (run < want && run + c[j] >= want) {
+            d = (uint32_t)(lane * 8 + j);
+            break;
+          } else {
+            run += c[j];
+          }
+        s_prefix = prefix | ((uint64_t)d << shift);
+        s_need = want - run;
+      }
+    }
+    mask |= 255ull << shift;
+    __syncthreads();
+  }
+  // the K best have leading words at or below the selected one
+  const uint64_t thr = s_prefix;
+#pragma unroll
+  for (int r = 0; r < kMsPer; ++r)
+    if (v[r] && t[r] <= thr) s_sel[atomicAdd(&s_nsel, 1u)] = (uint16_t)(r * kMsThreads + threadIdx.x);
+  __syncthreads();
+  const uint32_t ns = s_nsel;
+  Cand L = cand_inf();
+  for (uint32_t base = (uint32_t)warp * 32; base < ns; base += kMsThreads) {
+    const uint32_t q = base + lane;
+    Cand c = cand_inf();
+    const bool ok = q < ns;
+    if (ok) {
+      const uint32_t i = s_sel[q];
+      const SortItem k = keys[i];
+      c.w[0] = k.w[0]; c.w[1] = k.w[1]; c.w[2] = k.w[2]; c.w[3] = k.w[3];
+      c.ix = idx[i];
+    }
+    warp_offer_batch(L, c, ok, K, lane);
+  }
+  block_merge_lists<WARPS>(L, s_l, warp, lane);
+  if (warp == 0) {
+    const uint32_t valid = __ballot_sync(0xFFFFFFFFu, lane < K && L.ix != 0xFFFFFFFFu);
+    if (lane < K && L.ix != 0xFFFFFFFFu) out_idx[lane] = L.ix;
+    if (lane == 0) *out_count = (uint64_t)__popc(valid);
+  }
+  // every thread read *count and the cut before the barriers above
+  if (reset && threadIdx.x == 0) {
+    reset[0] = 0;
+    reset[1] = 0;
+  }
+}
+
 constexpr int kTfThreads = 256;  // first pass
 constexpr int kTfItems = 16;     // groups per lane per step
 static unsigned topk_final_ctas(uint64_t n_max, unsigned max_ctas) {
@@ -755,9 +881,14 @@ cudaError_t launch_topk_final(const TopkFinalSpec& spec, int k, uint32_t* out_g,
   SortItem* pk = (SortItem*)((uint8_t*)temp + 256);
   uint32_t* pi = (uint32_t*)(pk + (uint64_t)ctas * k);
   if (phase != 2) k_topk_final<kTfThreads><<<ctas, kTfThreads, 0, s>>>(spec, k, gst, pk, pi);
-  if (phase != 1)
-    k_topk_warp<1024><<<1, 1024, 0, s>>>(pk, pi, (const uint64_t*)&gst->n_cand, (uint64_t)ctas * k, k, nullptr, out_g,
-                                         out_count, 1, nullptr, (uint64_t*)gst, spec.total_bits);
+  if (phase != 1) {
+    if ((uint64_t)ctas * k <= (uint64_t)kMsMax)
+      k_topk_merge_select<<<1, kMsThreads, 0, s>>>(pk, pi, (const uint64_t*)&gst->n_cand, (uint64_t)ctas * k, k,
+                                                   spec.total_bits, out_g, out_count, (uint64_t*)gst);
+    else
+      k_topk_warp<1024><<<1, 1024, 0, s>>>(pk, pi, (const uint64_t*)&gst->n_cand, (uint64_t)ctas * k, k, nullptr,
+                                           out_g, out_count, 1, nullptr, (uint64_t*)gst, spec.total_bits);
+  }
   return cudaGetLastError();
 }
 
