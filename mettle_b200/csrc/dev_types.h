@@ -277,7 +277,7 @@ struct PipeDesc {
   int32_t part_words;
   int32_t part_nvals;               // inputs per record (value slots in use)
   int32_t part_combine;             // few keys per partition: combine a warp's records of one key
-  int32_t part_split;               // log2 of the CTAs sharing a chunk (each a share of its keys)
+  int32_t part_split;               // log2 of the sub-partitions a chunk is aggregated in, one at a time
   int32_t part_ctas;
   uint32_t part_chunk;              // records per CTA of the per-partition aggregation
   int32_t part_val[kMaxAggs];
@@ -287,6 +287,7 @@ struct PipeDesc {
   uint32_t* part_start;             // first record of each partition (P + 1 entries)
   uint32_t* part_chunk_start;       // first chunk of each partition (P + 1 entries)
   uint64_t* part_records;
+  uint64_t* part_sub;               // records placed by sub-partition (part_split > 0), same positions
 
   // launch shape (0: defaults), picked per pipeline by the autotuner:
   // resident CTAs per SM of the grid, and consecutive warp-tiles a warp

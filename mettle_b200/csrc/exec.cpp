@@ -983,6 +983,17 @@ struct Compiler {
     const uint64_t words = nv == 0 ? 1 : nv == 1 ? 2 : 4;  // 16-byte aligned records
     const uint64_t rec_bytes = rows * words * 8;
     if (rec_bytes + (64ull << 20) > ctx.arena.largest_free()) return false;
+    // Partitions holding more groups than a table are sub-partitioned: the
+    // CTA of a chunk places its records by the next 2^split hash bits and
+    // aggregates one sub-partition at a time, each about 60 % of a table.
+    // That needs a second record buffer; without room for it, the keys a
+    // full table leaves out update the global table directly.
+    int split = 0;
+    if (overfull) {
+      while (split < part_max_split() && (uint64_t)((double)cap * 0.6) << (bits + split) < est) ++split;
+      if (2 * rec_bytes + (64ull << 20) > ctx.arena.largest_free()) split = 0;
+    }
+    const bool still_overfull = (uint64_t)((double)cap * 0.6) << (bits + split) < est;
     const int ctas = pipeline_part_ctas();
     d.part_bits = bits;
     d.part_words = (int32_t)words;
@@ -990,12 +1001,6 @@ struct Compiler {
     d.part_combine = est / np < 128 ? 1 : 0;
     d.part_ctas = ctas;
     d.smem_capacity = (int32_t)cap;
-    // Partitions holding more groups than a table are split: 2^split CTAs
-    // share each chunk (read from L2), each taking the keys of its share,
-    // so that every share fits about 60 % of a table.
-    int split = 0;
-    while (overfull && split < 6 && (uint64_t)((double)cap * 0.6) << (bits + split) < est) ++split;
-    const bool still_overfull = (uint64_t)((double)cap * 0.6) << (bits + split) < est;
     d.part_split = split;
     d.smem_probes = still_overfull ? 8 : 0;  // 0: the kernel's default window
     // records per CTA: half a partition's average, but small enough for
@@ -1003,10 +1008,11 @@ struct Compiler {
     const uint64_t min_ctas = 4ull * (uint64_t)pipeline_part_ctas();
     d.part_chunk = (uint32_t)std::max<uint64_t>(
         4096, std::min<uint64_t>((rows + 2 * np - 1) / (2 * np), (rows + min_ctas - 1) / min_ctas));
-    // split partitions: about one chunk per partition, so that each group is
-    // merged into the global table once
+    // sub-partitioned chunks: about one chunk per partition, so that each
+    // group is merged into the global table once
     if (split) d.part_chunk = (uint32_t)std::max<uint64_t>(4096, (rows + np - 1) / np * 5 / 4);
     d.part_records = (uint64_t*)scratch(rec_bytes);
+    d.part_sub = split ? (uint64_t*)scratch(rec_bytes) : nullptr;
     d.part_counts = (uint32_t*)scratch((uint64_t)ctas * np * 4);
     d.part_offsets = (uint32_t*)scratch((uint64_t)ctas * np * 4);
     d.part_start = (uint32_t*)scratch((np + 1) * 4);

@@ -579,6 +579,145 @@ __device__ __forceinline__ int64_t tc_get(const TileCtx& t, int col, uint32_t r)
   return acc_get(col_acc(t, col), t, r);
 }
 
+// ---- typed write phase of the order-preserving compaction
+// One output column over the compacted rows with its value source and
+// conversion fixed: TIn is how the column is held (int32_t sign-extends,
+// uint32_t zero-extends, as acc_get does), TOut how the output stores it
+// (the width store_val picks), G whether the column is read from HBM at the
+// driving source's rows rather than from the streamed tile. f maps the
+// loaded value (widened to int64, as the VM holds it) to the stored one.
+// Four rows per lane are loaded before any is stored.
+template <typename TIn, typename TOut, bool G, class F>
+__device__ __forceinline__ void write_rows(const TIn* __restrict__ src, TOut* __restrict__ dst, uint32_t lim,
+                                           bool ident, const uint16_t* sel, int lane, F f) {
+  constexpr int B = 4;
+  auto ld = [&](uint32_t q) -> int64_t {
+    const uint32_t r = ident ? q : (uint32_t)sel[q];
+    if (G) return (int64_t)__ldg(src + r);
+    return (int64_t)src[r];
+  };
+  uint32_t p = (uint32_t)lane;
+  for (; p + 32 * (B - 1) < lim; p += 32 * B) {
+    int64_t v[B];
+#pragma unroll
+    for (int j = 0; j < B; ++j) v[j] = ld(p + 32 * j);
+#pragma unroll
+    for (int j = 0; j < B; ++j) dst[p + 32 * j] = (TOut)f(v[j]);
+  }
+  for (; p < lim; p += 32) dst[p] = (TOut)f(ld(p));
+}
+
+// Column value sources the typed writer covers: the streamed tile, or the
+// driving source's column in HBM.
+struct WriteSrc {
+  const uint8_t* p;  // first row of the tile
+  bool g;
+  int width;
+  int32_t ptype;
+};
+
+__device__ __forceinline__ bool write_src(const TileCtx& t, int col, WriteSrc& w) {
+  const ColAcc a = col_acc(t, col);
+  w.width = a.width;
+  w.ptype = a.ptype;
+  if (a.width != 4 && a.width != 8) return false;
+  if (a.sm) {
+    w.p = a.sm;
+    w.g = false;
+    return true;
+  }
+  if (a.src != t.d->drive_src) return false;
+  w.p = (const uint8_t*)a.g + t.base * (uint64_t)a.width;
+  w.g = true;
+  return true;
+}
+
+// Dispatches one typed loop over the (source kind, held type) of a column
+// for a fixed output type.
+template <typename TOut, class F>
+__device__ __forceinline__ void write_any(const WriteSrc& w, void* out, uint64_t base, uint32_t lim, bool ident,
+                                          const uint16_t* sel, int lane, F f) {
+  TOut* const dst = (TOut*)out + base;
+  if (w.width == 8) {
+    if (w.g) write_rows<int64_t, TOut, true>((const int64_t*)w.p, dst, lim, ident, sel, lane, f);
+    else write_rows<int64_t, TOut, false>((const int64_t*)w.p, dst, lim, ident, sel, lane, f);
+  } else if (w.ptype == P_I32) {
+    if (w.g) write_rows<int32_t, TOut, true>((const int32_t*)w.p, dst, lim, ident, sel, lane, f);
+    else write_rows<int32_t, TOut, false>((const int32_t*)w.p, dst, lim, ident, sel, lane, f);
+  } else {
+    if (w.g) write_rows<uint32_t, TOut, true>((const uint32_t*)w.p, dst, lim, ident, sel, lane, f);
+    else write_rows<uint32_t, TOut, false>((const uint32_t*)w.p, dst, lim, ident, sel, lane, f);
+  }
+}
+
+// Writes output column `pg` over the compacted rows when it is a column of
+// the driving source, plain or combined with a constant by + - * in a
+// non-128-bit type, into a 4- or 8-byte output; returns false for every
+// other program (the caller evaluates those with the VM). The arithmetic
+// is vm_arith's, with the same overflow rules.
+__device__ __forceinline__ bool write_col_typed(const VmProg& pg, const TileCtx& t, void* out, uint64_t base,
+                                                uint32_t lim, bool ident, const uint16_t* sel, int lane,
+                                                uint32_t& st) {
+  const int32_t ot = pg.out_type;
+  if (ot == P_I128) return false;
+  const bool o4 = ot == P_I32 || ot == P_F32;
+  WriteSrc w;
+  if (pg.n == 1 && pg.ins[0].op == VM_COL) {
+    if (!write_src(t, pg.ins[0].arg, w)) return false;
+    auto id = [](int64_t x) { return x; };
+    if (o4) write_any<uint32_t>(w, out, base, lim, ident, sel, lane, id);
+    else write_any<int64_t>(w, out, base, lim, ident, sel, lane, id);
+    return true;
+  }
+  if (!(pg.n == 3 && pg.ins[0].op == VM_COL && pg.ins[1].op == VM_CONST && pg.ins[2].op >= VM_ADD &&
+        pg.ins[2].op <= VM_MUL && pg.ins[2].type != P_I128))
+    return false;
+  if (!write_src(t, pg.ins[0].arg, w)) return false;
+  const int64_t k = pg.ins[1].k;
+  const int16_t op = pg.ins[2].op;
+  uint32_t s2 = 0;
+  switch (pg.ins[2].type) {
+    case P_I32: {
+      auto f = [&](int64_t x) {
+        return fit32(op == VM_ADD ? x + k : op == VM_SUB ? x - k : x * k, s2);
+      };
+      if (o4) write_any<uint32_t>(w, out, base, lim, ident, sel, lane, f);
+      else write_any<int64_t>(w, out, base, lim, ident, sel, lane, f);
+      break;
+    }
+    case P_I64: {
+      auto f = [&](int64_t x) {
+        return op == VM_ADD ? add64(x, k, s2) : op == VM_SUB ? sub64(x, k, s2) : mul64(x, k, s2);
+      };
+      if (o4) write_any<uint32_t>(w, out, base, lim, ident, sel, lane, f);
+      else write_any<int64_t>(w, out, base, lim, ident, sel, lane, f);
+      break;
+    }
+    case P_F32: {
+      const float y = as_f32(k);
+      auto f = [&](int64_t x) {
+        const float a = as_f32(x);
+        return f32_bits(op == VM_ADD ? __fadd_rn(a, y) : op == VM_SUB ? __fsub_rn(a, y) : __fmul_rn(a, y));
+      };
+      if (o4) write_any<uint32_t>(w, out, base, lim, ident, sel, lane, f);
+      else write_any<int64_t>(w, out, base, lim, ident, sel, lane, f);
+      break;
+    }
+    default: {
+      const double y = as_f64(k);
+      auto f = [&](int64_t x) {
+        const double a = as_f64(x);
+        return f64_bits(op == VM_ADD ? __dadd_rn(a, y) : op == VM_SUB ? __dsub_rn(a, y) : __dmul_rn(a, y));
+      };
+      if (o4) write_any<uint32_t>(w, out, base, lim, ident, sel, lane, f);
+      else write_any<int64_t>(w, out, base, lim, ident, sel, lane, f);
+      break;
+    }
+  }
+  st |= s2;
+  return true;
+}
+
 // Stack slots of the expression VM held in registers. Every instruction's
 // stack position depends on the program only, so it is the same in all
 // lanes and the slot selects below are uniform branches.
@@ -1286,7 +1425,9 @@ __global__ void __launch_bounds__(kThreads, (SINK == SK_AGG_SCALAR || SINK == SK
         const VmProg& pg = d.progs[d.out_prog[q]];
         void* out = d.out_ptr[q];
         const int32_t ot = pg.out_type;
-        if (pg.n == 1 && pg.ins[0].op == VM_COL) {
+        if (write_col_typed(pg, tc, out, base, lim, ident, sel_in, lane, st)) {
+          // typed loop over the column
+        } else if (pg.n == 1 && pg.ins[0].op == VM_COL) {
           // plain column: typed copy
           const ColAcc ca = col_acc(tc, pg.ins[0].arg);
 #pragma unroll 4
@@ -1821,26 +1962,27 @@ constexpr int kPartBatch = 2;  // records per thread with loads in flight togeth
 // several CTAs while a CTA sees one partition's keys only. The records go
 // into a shared-memory table (the layout of SmemCas, capacity
 // d.smem_capacity); a record whose key finds no entry within d.smem_probes
-// (at most kPartProbes) slots of its home slot goes to the global table directly (a key is
-// claimed only within that window, so its records always take the same
-// route). Partitions with more groups than the table use a short window:
-// once the table is full, records of the keys left out go straight to the
-// global table, where a partition's groups share one stretch that stays in
-// L2 while its CTAs run.
-// slots goes to the global table directly. Then every entry is merged into
-// the global table.
+// (at most kPartProbes) slots of its home slot goes to the global table
+// directly (a key is claimed only within that window, so its records always
+// take the same route). Then every entry is merged into the global table.
+//
+// Partitions holding more groups than a table (beyond the partition limit)
+// are sub-partitioned by the CTA itself: with d.part_split = s > 0 it counts
+// its chunk's records per sub-partition (the 2^s hash bits below the
+// partition's), places them by sub-partition into d.part_sub (a counting
+// sort, at the chunk's own positions), and then aggregates one
+// sub-partition at a time, merging and clearing the table after each, so
+// that each round's groups fit the table.
 constexpr uint32_t kPartProbes = 64;
+constexpr int kMaxPartSplit = 5;  // sub-partitions per chunk: up to 32, one per lane
 
 __global__ void __launch_bounds__(kPartAggThreads, 2) k_part_agg(const __grid_constant__ PipeDesc d) {
   extern __shared__ __align__(128) uint8_t smem[];
+  __shared__ uint32_t s_sub[1 << kMaxPartSplit];       // records per sub-partition, then write cursors
+  __shared__ uint32_t s_subpos[(1 << kMaxPartSplit) + 1];  // first record of each sub-partition
   const uint32_t np = 1u << d.part_bits;
-  // With a split (partitions holding more groups than one table), 2^split
-  // CTAs share a chunk, each taking the records whose next hash bits select
-  // it; they read the chunk from L2 and each holds its share of the groups.
   const uint32_t split = (uint32_t)d.part_split;
-  const uint32_t sub = blockIdx.x & ((1u << split) - 1u);
-  const uint32_t cb = blockIdx.x >> split;
-  const int sub_shift = 64 - d.part_bits - (int)split;
+  const uint32_t cb = blockIdx.x;
   if (cb >= d.part_chunk_start[np]) return;  // the whole CTA leaves, before any barrier
   // the chunk's partition: chunk_start[lo] <= cb < chunk_start[hi]
   uint32_t lo = 0, hi = np;
@@ -1855,7 +1997,6 @@ __global__ void __launch_bounds__(kPartAggThreads, 2) k_part_agg(const __grid_co
   const uint32_t re = pend - rb < d.part_chunk ? pend : rb + d.part_chunk;
   SmemCas s;
   smem_cas_init(d, s, smem);
-  __syncthreads();
   uint32_t st = 0;
   const int W = d.part_words;
   const int na = d.n_aggs;
@@ -1866,137 +2007,238 @@ __global__ void __launch_bounds__(kPartAggThreads, 2) k_part_agg(const __grid_co
                                                                                      : kPartProbes;
   constexpr int B = kPartBatch;
   const uint32_t lane = threadIdx.x & 31;
+  const uint32_t lt = (1u << lane) - 1u;
   // Records of one key are combined within a warp before updating where a
   // warp often holds several of them: in a partition over twice the average
   // size (a skewed key's), or when partitions have few keys. Every state must
   // be one word.
   bool warp_ok = d.part_combine != 0 || psize > 2 * (d.part_start[np] >> d.part_bits) + 1024;
   for (int a = 0; a < na; ++a) warp_ok &= d.aggs[a].fn != A_SUM_I128;
-  for (uint32_t i0 = rb; i0 < re; i0 += kPartAggThreads * B) {
-    uint64_t key[B];
-    uint64_t val[B][kPartMaxVals];
-    bool act[B];
+  const int hshift = d.part_bits + (int)split;
+
+  // Aggregates the records [b, e) of `recs` into the table (keys it cannot
+  // hold into the global table). Each record is read once (evict first).
+  auto agg_range = [&](const uint64_t* recs, uint32_t b, uint32_t e) {
+    for (uint32_t i0 = b; i0 < e; i0 += kPartAggThreads * B) {
+      uint64_t key[B];
+      uint64_t val[B][kPartMaxVals];
+      bool act[B];
 #pragma unroll
-    for (int q = 0; q < B; ++q) {
-      const uint32_t i = i0 + (uint32_t)q * kPartAggThreads + threadIdx.x;
-      act[q] = i < re;
-      const uint64_t* rec = d.part_records + (uint64_t)(act[q] ? i : rb) * (uint64_t)W;
-      key[q] = 0;
+      for (int q = 0; q < B; ++q) {
+        const uint32_t i = i0 + (uint32_t)q * kPartAggThreads + threadIdx.x;
+        act[q] = i < e;
+        const uint64_t* rec = recs + (uint64_t)(act[q] ? i : b) * (uint64_t)W;
+        key[q] = 0;
 #pragma unroll
-      for (int v = 0; v < kPartMaxVals; ++v) val[q][v] = 0;
-      if (act[q]) {
-        // streamed once (evict first), or kept in L2 for the other CTAs of a split chunk
-        if (W == 1) {
-          key[q] = split ? __ldcg(rec) : __ldcs(rec);
-        } else {
-          if (W == 4) {  // one 32-byte load
-            if (split)
-              asm volatile("ld.global.cg.v4.u64 {%0, %1, %2, %3}, [%4];"
-                           : "=l"(key[q]), "=l"(val[q][0]), "=l"(val[q][1]), "=l"(val[q][2])
-                           : "l"(rec));
-            else
-              asm volatile("ld.global.cs.v4.u64 {%0, %1, %2, %3}, [%4];"
-                           : "=l"(key[q]), "=l"(val[q][0]), "=l"(val[q][1]), "=l"(val[q][2])
-                           : "l"(rec));
+        for (int v = 0; v < kPartMaxVals; ++v) val[q][v] = 0;
+        if (act[q]) {
+          if (W == 1) {
+            key[q] = __ldcs(rec);
+          } else if (W == 4) {  // one 32-byte load
+            asm volatile("ld.global.cs.v4.u64 {%0, %1, %2, %3}, [%4];"
+                         : "=l"(key[q]), "=l"(val[q][0]), "=l"(val[q][1]), "=l"(val[q][2])
+                         : "l"(rec));
           } else {
-            const ulonglong2 x = split ? __ldcg((const ulonglong2*)rec) : __ldcs((const ulonglong2*)rec);
+            const ulonglong2 x = __ldcs((const ulonglong2*)rec);
             key[q] = x.x;
             val[q][0] = x.y;
           }
         }
-        if (split) act[q] = ((uint32_t)(key_hash1(key[q]) >> sub_shift) & ((1u << split) - 1u)) == sub;
       }
-    }
-    // Records of one key in the same warp (a skewed key's) are combined in
-    // registers first: only the lowest lane of each key's group updates.
-    bool upd[B];      // this lane's record updates an entry
-    bool comb[B];     // (warp-uniform) batch q combines records of a key first
-    unsigned peers[B];
-  #pragma unroll
-    for (int q = 0; q < B; ++q) {
-      upd[q] = act[q];
-      comb[q] = false;
-      peers[q] = 0;
-      if (warp_ok) {
-        // every lane takes part in the warp votes (key[q] is 0 where the lane has no record)
-        const unsigned am = __ballot_sync(0xFFFFFFFFu, act[q]);
-        const unsigned same = __match_any_sync(0xFFFFFFFFu, key[q]);
-        peers[q] = act[q] ? (same & am) : 0u;
-        // combining pays for itself once some key holds four lanes
-        comb[q] = __any_sync(0xFFFFFFFFu, __popc(peers[q]) >= 4);
-        // when combining, only the lowest lane of each key's group updates
-        if (comb[q]) upd[q] = act[q] && (peers[q] & ((1u << lane) - 1u)) == 0;
-      }
-    }
-    // the updating records' entries: shared-memory index, else the global group
-    int idx[B];
-    uint64_t g[B];
-#pragma unroll
-    for (int q = 0; q < B; ++q) {
-      idx[q] = -1;
-      g[q] = kNoGroup;
-      if (upd[q]) {
-        // the default window as a constant: the loop then compiles as in
-        // the common case it is (a short window only for overfull tables)
-        idx[q] = probes == kPartProbes ? smem_cas_find(s, key[q], kPartProbes, d.part_bits + (int)split)
-                                       : smem_cas_find(s, key[q], probes, d.part_bits + (int)split);
-        if (idx[q] < 0) g[q] = agg_find_cas(tb, key[q], hash_slot(key_hash1(key[q]), tb.capacity), st);
-      }
-    }
-    // one aggregate at a time over the batch, compiled per function
-    int hw = 0;
-    for (int a = 0; a < na; ++a) {
-      const DAgg& ag = d.aggs[a];
-      const int vs = d.part_val[a];
-      const int32_t vt = vs >= 0 ? d.progs[ag.prog].out_type : P_I64;
-      Val v[B];
+      // Records of one key in the same warp (a skewed key's) are combined in
+      // registers first: only the lowest lane of each key's group updates.
+      bool upd[B];      // this lane's record updates an entry
+      bool comb[B];     // (warp-uniform) batch q combines records of a key first
+      unsigned peers[B];
 #pragma unroll
       for (int q = 0; q < B; ++q) {
-        const uint64_t x = vs == 0 ? val[q][0] : vs == 1 ? val[q][1] : vs == 2 ? val[q][2] : 0;
-        v[q].lo = (int64_t)x;
-        v[q].hi = v[q].lo >> 63;
+        upd[q] = act[q];
+        comb[q] = false;
+        peers[q] = 0;
+        if (warp_ok) {
+          // every lane takes part in the warp votes (key[q] is 0 where the lane has no record)
+          const unsigned am = __ballot_sync(0xFFFFFFFFu, act[q]);
+          const unsigned same = __match_any_sync(0xFFFFFFFFu, key[q]);
+          peers[q] = act[q] ? (same & am) : 0u;
+          // combining pays for itself once some key holds four lanes
+          comb[q] = __any_sync(0xFFFFFFFFu, __popc(peers[q]) >= 4);
+          // when combining, only the lowest lane of each key's group updates
+          if (comb[q]) upd[q] = act[q] && (peers[q] & lt) == 0;
+        }
       }
-      const uint32_t sa = smem_u32(s.e + 1 + a), sh = smem_u32(s.e + 1 + na + hw);
-      unsigned long long* const glo = (unsigned long long*)ag.lo;
-      long long* const ghi = (long long*)ag.hi;
-      auto apply = [&](auto fnc) {
-        constexpr int FN = decltype(fnc)::value;
+      // the updating records' entries: shared-memory index, else the global group
+      int idx[B];
+      uint64_t g[B];
+#pragma unroll
+      for (int q = 0; q < B; ++q) {
+        idx[q] = -1;
+        g[q] = kNoGroup;
+        if (upd[q]) {
+          // the default window as a constant: the loop then compiles as in
+          // the common case it is (a short window only for overfull tables)
+          idx[q] = probes == kPartProbes ? smem_cas_find(s, key[q], kPartProbes, hshift)
+                                         : smem_cas_find(s, key[q], probes, hshift);
+          if (idx[q] < 0) g[q] = agg_find_cas(tb, key[q], hash_slot(key_hash1(key[q]), tb.capacity), st);
+        }
+      }
+      // one aggregate at a time over the batch, compiled per function
+      int hw = 0;
+      for (int a = 0; a < na; ++a) {
+        const DAgg& ag = d.aggs[a];
+        const int vs = d.part_val[a];
+        const int32_t vt = vs >= 0 ? d.progs[ag.prog].out_type : P_I64;
+        Val v[B];
 #pragma unroll
         for (int q = 0; q < B; ++q) {
-          if (comb[q]) {  // warp-uniform; only when every state is one word
-            if (FN != A_SUM_I128) {
-              const uint64_t x = peer_combine(FN, peers[q], lane_state_value(FN, v[q], vt), lane);
-              if (idx[q] >= 0) smem_merge(FN, sa + (uint32_t)idx[q] * estride, x);
-              else if (g[q] != kNoGroup) agg_merge(FN, glo + g[q] * gstride, nullptr, x, 0);
-            }
-            continue;
-          }
-          if (idx[q] >= 0) {
-            const uint32_t eo = (uint32_t)idx[q] * estride;
-            smem_apply(FN, sa + eo, sh + eo, v[q], vt);
-          } else if (g[q] != kNoGroup) {
-            const uint64_t o = g[q] * gstride;
-            agg_apply_g(FN, glo + o, ghi ? ghi + o : nullptr, v[q], vt);
-          }
+          const uint64_t x = vs == 0 ? val[q][0] : vs == 1 ? val[q][1] : vs == 2 ? val[q][2] : 0;
+          v[q].lo = (int64_t)x;
+          v[q].hi = v[q].lo >> 63;
         }
-      };
-      dispatch_fn(ag.fn, apply);
-      hw += ag.fn == A_SUM_I128;
+        const uint32_t sa = smem_u32(s.e + 1 + a), sh = smem_u32(s.e + 1 + na + hw);
+        unsigned long long* const glo = (unsigned long long*)ag.lo;
+        long long* const ghi = (long long*)ag.hi;
+        auto apply = [&](auto fnc) {
+          constexpr int FN = decltype(fnc)::value;
+#pragma unroll
+          for (int q = 0; q < B; ++q) {
+            if (comb[q]) {  // warp-uniform; only when every state is one word
+              if (FN != A_SUM_I128) {
+                const uint64_t x = peer_combine(FN, peers[q], lane_state_value(FN, v[q], vt), lane);
+                if (idx[q] >= 0) smem_merge(FN, sa + (uint32_t)idx[q] * estride, x);
+                else if (g[q] != kNoGroup) agg_merge(FN, glo + g[q] * gstride, nullptr, x, 0);
+              }
+              continue;
+            }
+            if (idx[q] >= 0) {
+              const uint32_t eo = (uint32_t)idx[q] * estride;
+              smem_apply(FN, sa + eo, sh + eo, v[q], vt);
+            } else if (g[q] != kNoGroup) {
+              const uint64_t o = g[q] * gstride;
+              agg_apply_g(FN, glo + o, ghi ? ghi + o : nullptr, v[q], vt);
+            }
+          }
+        };
+        dispatch_fn(ag.fn, apply);
+        hw += ag.fn == A_SUM_I128;
+      }
+    }
+  };
+
+  // Merges every entry of the table into the global table.
+  auto merge_table = [&]() {
+    for (uint32_t i = threadIdx.x; i < s.cap; i += kPartAggThreads) {
+      const uint64_t* ent = s.e + (size_t)i * s.stride;
+      const uint64_t key = ent[0];
+      if ((int64_t)key == kEmptyKey) continue;
+      const uint64_t gg = agg_find_cas(tb, key, hash_slot(key_hash1(key), tb.capacity), st);
+      if (gg == kNoGroup) continue;
+      const uint64_t o = gg * gstride;
+      int hw2 = 0;
+      for (int a = 0; a < na; ++a) {
+        const DAgg& ag = d.aggs[a];
+        const int64_t hv = ag.fn == A_SUM_I128 ? (int64_t)ent[1 + na + hw2++] : 0;
+        agg_merge(ag.fn, (unsigned long long*)(ag.lo + o), (long long*)(ag.hi ? ag.hi + o : nullptr), ent[1 + a],
+                  hv);
+      }
+    }
+  };
+
+  if (split == 0) {
+    __syncthreads();
+    agg_range(d.part_records, rb, re);
+    __syncthreads();
+    merge_table();
+    if (st) atomicOr(d.status, st);
+    return;
+  }
+
+  // ---- sub-partitioned chunk: count, place, then one round per sub-partition
+  const uint32_t S = 1u << split;
+  const int sub_shift = 64 - d.part_bits - (int)split;
+  if (threadIdx.x < S) s_sub[threadIdx.x] = 0;
+  __syncthreads();
+  // This lane's sub-partition (S: no record), the lanes of the warp that share
+  // it, and (in lane j < S) how many lanes hold sub-partition j: S ballots.
+  auto sub_masks = [&](uint32_t sb, unsigned& mine, uint32_t& cnt_j) {
+    mine = 0;
+    cnt_j = 0;
+    for (uint32_t j = 0; j < S; ++j) {
+      const unsigned m = __ballot_sync(0xFFFFFFFFu, sb == j);
+      if (sb == j) mine = m;
+      if (lane == j) cnt_j = (uint32_t)__popc(m);
+    }
+  };
+  // the loops below run whole warps over the chunk, so every lane votes
+  const uint32_t span = (re - rb + 31) & ~31u;
+  for (uint32_t i0 = 0; i0 < span; i0 += kPartAggThreads) {
+    const uint32_t i = rb + i0 + threadIdx.x;
+    if (i0 + (threadIdx.x & ~31u) >= span) break;  // warp-uniform
+    uint32_t sb = S;
+    if (i < re) sb = (uint32_t)(key_hash1(__ldcg(d.part_records + (uint64_t)i * (uint64_t)W)) >> sub_shift) & (S - 1u);
+    unsigned mine;
+    uint32_t cnt_j;
+    sub_masks(sb, mine, cnt_j);
+    if (lane < S && cnt_j) atomicAdd(&s_sub[lane], cnt_j);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t run = 0;
+    for (uint32_t j = 0; j < S; ++j) {
+      s_subpos[j] = run;
+      run += s_sub[j];
+      s_sub[j] = s_subpos[j];  // write cursor
+    }
+    s_subpos[S] = run;
+  }
+  __syncthreads();
+  for (uint32_t i0 = 0; i0 < span; i0 += kPartAggThreads) {
+    const uint32_t i = rb + i0 + threadIdx.x;
+    if (i0 + (threadIdx.x & ~31u) >= span) break;  // warp-uniform
+    const bool act = i < re;
+    const uint64_t* rec = d.part_records + (uint64_t)(act ? i : rb) * (uint64_t)W;
+    uint64_t w[4] = {0, 0, 0, 0};
+    if (act) {
+      if (W == 4)
+        asm volatile("ld.global.cs.v4.u64 {%0, %1, %2, %3}, [%4];"
+                     : "=l"(w[0]), "=l"(w[1]), "=l"(w[2]), "=l"(w[3])
+                     : "l"(rec));
+      else if (W == 2) {
+        const ulonglong2 x = __ldcs((const ulonglong2*)rec);
+        w[0] = x.x;
+        w[1] = x.y;
+      } else {
+        w[0] = __ldcs(rec);
+      }
+    }
+    const uint32_t sb = act ? (uint32_t)(key_hash1(w[0]) >> sub_shift) & (S - 1u) : S;
+    unsigned mine;
+    uint32_t cnt_j;
+    sub_masks(sb, mine, cnt_j);
+    uint32_t base_j = 0;
+    if (lane < S && cnt_j) base_j = atomicAdd(&s_sub[lane], cnt_j);
+    const uint32_t base = __shfl_sync(0xFFFFFFFFu, base_j, sb < S ? sb : 0);
+    if (act) {
+      uint64_t* dst = d.part_sub + ((uint64_t)rb + base + (uint32_t)__popc(mine & lt)) * (uint64_t)W;
+      if (W == 4) {  // one 32-byte store
+        asm volatile("st.global.v4.u64 [%0], {%1, %2, %3, %4};" ::"l"(dst), "l"(w[0]), "l"(w[1]), "l"(w[2]),
+                     "l"(w[3])
+                     : "memory");
+      } else if (W == 2) {
+        *(ulonglong2*)dst = make_ulonglong2(w[0], w[1]);
+      } else {
+        dst[0] = w[0];
+      }
     }
   }
   __syncthreads();
-  for (uint32_t i = threadIdx.x; i < s.cap; i += kPartAggThreads) {
-    const uint64_t* ent = s.e + (size_t)i * s.stride;
-    const uint64_t key = ent[0];
-    if ((int64_t)key == kEmptyKey) continue;
-    const uint64_t gg = agg_find_cas(tb, key, hash_slot(key_hash1(key), tb.capacity), st);
-    if (gg == kNoGroup) continue;
-    const uint64_t o = gg * gstride;
-    int hw2 = 0;
-    for (int a = 0; a < na; ++a) {
-      const DAgg& ag = d.aggs[a];
-      const int64_t hv = ag.fn == A_SUM_I128 ? (int64_t)ent[1 + na + hw2++] : 0;
-      agg_merge(ag.fn, (unsigned long long*)(ag.lo + o), (long long*)(ag.hi ? ag.hi + o : nullptr), ent[1 + a], hv);
+  for (uint32_t j = 0; j < S; ++j) {
+    agg_range(d.part_sub, rb + s_subpos[j], rb + s_subpos[j + 1]);
+    __syncthreads();
+    merge_table();
+    __syncthreads();
+    if (j + 1 < S) {
+      smem_cas_init(d, s, smem);
+      __syncthreads();
     }
   }
   if (st) atomicOr(d.status, st);
@@ -2068,6 +2310,7 @@ static cudaError_t launch_sink(const PipeDesc& d, uint64_t n_hint, cudaStream_t 
 }
 
 int part_max_bits() { return kMaxPartBits; }
+int part_max_split() { return kMaxPartSplit; }
 size_t pipeline_warp_tile_rows() { return kTile; }
 int part_max_values() { return kPartMaxVals; }
 
@@ -2174,8 +2417,10 @@ cudaError_t launch_part_agg(const PipeDesc& d, uint64_t n_hint, cudaStream_t s) 
       smem_set = smem;
     }
   }
+  if (d.part_split < 0 || d.part_split > kMaxPartSplit || (d.part_split > 0 && !d.part_sub))
+    return cudaErrorInvalidValue;
   // at most records / chunk + one partial chunk per partition
-  const uint64_t grid = (n_hint / d.part_chunk + (1ull << d.part_bits)) << d.part_split;
+  const uint64_t grid = n_hint / d.part_chunk + (1ull << d.part_bits);
   k_part_agg<<<(unsigned)grid, kPartAggThreads, smem, s>>>(d);
   return cudaGetLastError();
 }

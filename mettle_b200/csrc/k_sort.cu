@@ -746,23 +746,39 @@ __global__ void __launch_bounds__(kMsThreads) k_topk_merge_select(const SortItem
   uint64_t n = count ? *count : n_max;
   if (n > n_max) n = n_max;
   if (n > (uint64_t)kMsMax) n = kMsMax;  // the host launches this only below the bound
+  // the first pass is over, so its cut is final: a candidate above it is
+  // beaten by K others
+  const uint64_t cut = reset ? ~*(volatile unsigned long long*)reset : ~0ULL;
   uint64_t t[kMsPer];
   bool v[kMsPer];
+  uint32_t mine = 0;
 #pragma unroll
   for (int r = 0; r < kMsPer; ++r) {
     const uint64_t i = (uint64_t)r * kMsThreads + threadIdx.x;
     v[r] = i < n && idx[i] != 0xFFFFFFFFu;
     t[r] = 0;
     if (v[r]) t[r] = key_top64(keys[i].w, cut_bits);
+    v[r] = v[r] && t[r] <= cut;
+    mine += v[r];
   }
   if (threadIdx.x == 0) {
     s_prefix = 0;
     s_need = (uint32_t)K;
     s_nsel = 0;
   }
-  // radix select of the K-th smallest leading word, most significant digit first
+  __syncthreads();
+  if (mine) atomicAdd(&s_nsel, mine);
+  __syncthreads();
+  // Few candidates under the cut (the usual case): the warp lists take them
+  // all. Otherwise a radix select of the K-th smallest leading word, most
+  // significant digit first, keeps the K best and their ties.
+  const bool few = s_nsel <= 2u * kMsThreads;
+  __syncthreads();
+  if (threadIdx.x == 0) s_nsel = 0;
+  if (few && threadIdx.x == 0) s_prefix = ~0ULL;
+  __syncthreads();
   uint64_t mask = 0;
-  for (int shift = 56; shift >= 0; shift -= 8) {
+  for (int shift = 56; shift >= 0 && !few; shift -= 8) {
     for (int b = threadIdx.x; b < 256; b += kMsThreads) s_hist[b] = 0;
     __syncthreads();
     const uint64_t prefix = s_prefix;

@@ -32,6 +32,7 @@ cudaError_t launch_pipeline_materialize(const PipeDesc& d, uint64_t n_hint, cuda
 // chunk of at most d.part_chunk records of one partition, with a
 // shared-memory table of d.smem_capacity entries; n_hint bounds the records.
 int part_max_bits();
+int part_max_split();  // log2 of the most sub-partitions k_part_agg takes a chunk in
 int part_max_values();
 int pipeline_part_ctas();
 size_t part_agg_smem_bytes(const PipeDesc& d);

@@ -117,6 +117,22 @@ def test_c2_multi_predicate_and_empty(scan_conn):
     assert r.rows == 0
 
 
+@pytest.mark.gpu
+def test_c2_full_size(conn):
+    """The measured scan at its full size: 10^8 rows, half of them selected,
+    every output column compared in row order with the oracle's gathers."""
+    init(conn, "8 GB", "8 GB")
+    d = W.scan(100_000_000)
+    conn.create_table("t", {"a": (L.T_INTEGER, d["a"]), "b": (L.T_BIGINT, d["b"]), "c": (L.T_FLOAT, d["c"]),
+                            "d": (L.T_DATE, d["d"]), "e": (L.T_TIMESTAMP, d["e"])})
+    conn.gpu_register_table("t", upload=True)
+    r = conn.gpu_processing(W.scan_sql("a", "<", 0.5))
+    want = scan_expect(d, "a", "<", literal_value("a", 0.5))
+    assert r.rows == len(want["a"]) and abs(r.rows - 50_000_000) < 100_000
+    for i, name in enumerate(["a", "b5", "c10", "d", "e"]):
+        assert np.array_equal(r.columns[i], want[name]), name
+
+
 # ------------------------------------------------------------------ config 3
 @pytest.mark.gpu
 @pytest.mark.parametrize("groups,dist", [(1000, "uniform"), (1000, "zipf"), (100_000, "uniform"),
