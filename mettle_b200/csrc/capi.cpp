@@ -343,7 +343,17 @@ int mtl_table_register(mtl_ctx* ctx, const char* table, uint64_t rows, int32_t n
       auto it = c.tables.find(tname);
       if (it != c.tables.end()) {
         for (auto& oc : it->second->cols) {
-          if (oc->dev) c.dev_cache_bytes -= oc->dev_bytes;
+          if (oc->dev) {
+            c.dev_cache_bytes -= oc->dev_bytes;
+            // freed on the stream that allocates column buffers, so the next
+            // version's uploads reuse the memory in stream order instead of
+            // growing the pool (a statement still using it keeps it)
+            if (oc->pins == 0) {
+              cudaFreeAsync(oc->dev, c.copy_stream);
+              oc->dev = nullptr;
+              oc->dev_bytes = 0;
+            }
+          }
           if (oc->host_owned_pinned) c.pinned_bytes -= oc->rows * oc->width();
         }
         c.tables.erase(it);

@@ -860,9 +860,15 @@ struct Compiler {
     int max_stream = 4;
     // (staging every output column of the compaction's write pass, up to
     // 32 bytes a row, halves its resident CTAs and measured no faster)
-    // the scatter pass reads every input of the records: 80 KB still lets
-    // two of its CTAs share an SM
-    if (d.sink == SK_PART_SCATTER) budget = 20;
+    // The scatter pass reads every input of the records (up to 20 bytes a
+    // row staged), within about 110 KB with its partition cursors so that
+    // two of its CTAs (its fixed grid) share an SM: with the most partitions
+    // fewer bytes are staged and the rest read directly.
+    if (d.sink == SK_PART_SCATTER) {
+      const uint32_t cursors = (4u << d.part_bits);
+      budget = 20;
+      while (budget > 4 && cursors + 8 * (2 * 256 * budget + 2048) > 110 * 1024) budget -= 4;
+    }
     if (d.sink == SK_AGG_SMEM) {
       // keep the CTA within about 110 KB so two fit on an SM: stream
       // buffers take 2 x 2048 bytes per streamed byte of a row

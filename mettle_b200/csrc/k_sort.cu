@@ -10,6 +10,7 @@
 #include "final_common.cuh"
 #include "kern_common.cuh"
 #include "kernels.h"
+#include <mutex>
 
 namespace mtl {
 
@@ -552,7 +553,7 @@ __device__ __forceinline__ bool u256_gt(const U256& a, const Cand& b) {
 // it must be zero when the launch starts (the merge pass clears it again).
 struct TopkFinalState {
   unsigned long long cut_inv;  // ~(smallest published cut); 0: none yet
-  unsigned long long n_cand;   // candidates appended
+  unsigned long long unused;   // (cleared with the cut)
 };
 
 template <int THREADS>
@@ -564,7 +565,6 @@ __global__ void __launch_bounds__(THREADS) k_topk_final(const __grid_constant__ 
   __shared__ Cand s_l[WARPS][32];
   __shared__ uint32_t s_live[WARPS][64];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const uint32_t lt = (1u << lane) - 1u;
   const uint64_t n = spec.n_dev ? (*spec.n_dev < spec.n_max ? *spec.n_dev : spec.n_max) : spec.n_max;
   // CTA ranges start on multiples of 512 groups (16-byte aligned flag loads)
   const uint64_t per = ((n + gridDim.x - 1) / gridDim.x + 511) & ~511ULL;
@@ -698,163 +698,118 @@ __global__ void __launch_bounds__(THREADS) k_topk_final(const __grid_constant__ 
   }
   if (cnt) process(cnt);
   block_merge_lists<WARPS>(L, s_l, warp, lane);
-  if (warp == 0) {
-    // append the CTA's candidates that can still win
-    uint64_t gc = 0;
-    if (lane == 0) gc = ~*(volatile unsigned long long*)&gst->cut_inv;
-    gc = __shfl_sync(0xFFFFFFFFu, gc, 0);
-    const bool keep = lane < K && L.ix != 0xFFFFFFFFu && key_top64(L.w, tb) <= gc;
-    const uint32_t m = __ballot_sync(0xFFFFFFFFu, keep);
-    unsigned long long base = 0;
-    if (lane == 0 && m) base = atomicAdd(&gst->n_cand, (unsigned long long)__popc(m));
-    base = __shfl_sync(0xFFFFFFFFu, base, 0);
-    if (keep) {
-      const uint64_t at = base + (uint64_t)__popc(m & lt);
-      SortItem it;
-      it.w[0] = L.w[0]; it.w[1] = L.w[1]; it.w[2] = L.w[2]; it.w[3] = L.w[3];
-      out_keys[at] = it;
-      out_idx[at] = L.ix;
-    }
+  if (warp == 0 && lane < K) {
+    // the CTA's list in its own K slots, best first: the candidates that can
+    // still win (a prefix: the leading bits grow along the list), then
+    // padding
+    const uint64_t gc = ~*(volatile unsigned long long*)&gst->cut_inv;
+    const bool keep = L.ix != 0xFFFFFFFFu && key_top64(L.w, tb) <= gc;
+    const uint64_t at = (uint64_t)blockIdx.x * (uint64_t)K + (uint64_t)lane;
+    SortItem it;
+    it.w[0] = L.w[0]; it.w[1] = L.w[1]; it.w[2] = L.w[2]; it.w[3] = L.w[3];
+    out_keys[at] = it;
+    out_idx[at] = keep ? L.ix : 0xFFFFFFFFu;
   }
 }
 
-// Merge pass of the fused top-K by selection: one CTA reads the candidates'
-// leading 64 key bits into registers (kMsPer per thread), finds the K-th
-// smallest of them exactly with a radix select over 8-bit digits (a
-// shared-memory histogram per digit), keeps only the candidates at or below
-// it (the K best, plus ties on those bits), and orders those with the warp
-// lists. The candidates' count is not known on the host, so this runs when
-// their bound (CTAs x K of the first pass) fits kMsThreads x kMsPer; 16-bit
-// positions and 16 warps keep its static shared memory under 48 KB.
-constexpr int kMsThreads = 512;
-constexpr int kMsPer = 16;
-constexpr int kMsMax = kMsThreads * kMsPer;
+// Merge pass of the fused top-K. The first pass leaves each CTA's K best in
+// the CTA's own K slots (padding, index 0xFFFFFFFF, after the last that can
+// still win). One CTA sorts the candidates' leading 64 key bits, with their
+// positions, by a bitonic sort in shared memory (every compare-exchange of a
+// pass in parallel, log^2 passes); the K-th leading word T then bounds the
+// winners: every candidate below T wins, and those equal to T are ordered
+// by their full keys. The m <= 32 candidates at or below T are sorted by
+// their full keys with one warp sort and the first K are the result (more
+// than 32 ties at T go through warp lists). A block-wide sort instead of a
+// serial merge: its depth is the passes, not the candidates or the rounds.
+constexpr int kMsThreads = 1024;
+constexpr uint32_t kMsMaxN = 8192;  // candidates (power of two) the shared arrays hold
 
-__global__ void __launch_bounds__(kMsThreads) k_topk_merge_select(const SortItem* __restrict__ keys,
-                                                                  const uint32_t* __restrict__ idx,
-                                                                  const uint64_t* count, uint64_t n_max, int K,
-                                                                  int cut_bits, uint32_t* __restrict__ out_idx,
-                                                                  uint64_t* out_count, uint64_t* reset) {
-  constexpr int WARPS = kMsThreads / 32;
-  __shared__ uint32_t s_hist[256];
-  __shared__ uint16_t s_sel[kMsMax];  // positions of the selected candidates
-  __shared__ uint32_t s_nsel;
-  __shared__ uint64_t s_prefix;
-  __shared__ uint32_t s_need;
-  __shared__ Cand s_l[WARPS][32];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  uint64_t n = count ? *count : n_max;
-  if (n > n_max) n = n_max;
-  if (n > (uint64_t)kMsMax) n = kMsMax;  // the host launches this only below the bound
-  // the first pass is over, so its cut is final: a candidate above it is
-  // beaten by K others
-  const uint64_t cut = reset ? ~*(volatile unsigned long long*)reset : ~0ULL;
-  uint64_t t[kMsPer];
-  bool v[kMsPer];
-  uint32_t mine = 0;
-#pragma unroll
-  for (int r = 0; r < kMsPer; ++r) {
-    const uint64_t i = (uint64_t)r * kMsThreads + threadIdx.x;
-    v[r] = i < n && idx[i] != 0xFFFFFFFFu;
-    t[r] = 0;
-    if (v[r]) t[r] = key_top64(keys[i].w, cut_bits);
-    v[r] = v[r] && t[r] <= cut;
-    mine += v[r];
-  }
-  if (threadIdx.x == 0) {
-    s_prefix = 0;
-    s_need = (uint32_t)K;
-    s_nsel = 0;
+__device__ __forceinline__ bool ms_greater(uint64_t ta, uint32_t pa, uint64_t tb, uint32_t pb) {
+  return ta > tb || (ta == tb && pa > pb);
+}
+
+__global__ void __launch_bounds__(kMsThreads) k_topk_merge_sort(const SortItem* __restrict__ keys,
+                                                                const uint32_t* __restrict__ idx, uint32_t n,
+                                                                uint32_t N, int K, int cut_bits,
+                                                                uint32_t* __restrict__ out_idx, uint64_t* out_count,
+                                                                uint64_t* reset) {
+  extern __shared__ __align__(16) uint8_t ms_smem[];
+  uint64_t* const st = (uint64_t*)ms_smem;      // leading key words (padding: all ones)
+  uint32_t* const sp = (uint32_t*)(st + N);      // candidate positions
+  __shared__ uint32_t s_m;
+  __shared__ Cand s_l[kMsThreads / 32][32];
+  for (uint32_t i = threadIdx.x; i < N; i += kMsThreads) {
+    uint64_t t = ~0ULL;
+    if (i < n && idx[i] != 0xFFFFFFFFu) t = key_top64(keys[i].w, cut_bits);
+    st[i] = t;
+    sp[i] = i;
   }
   __syncthreads();
-  if (mine) atomicAdd(&s_nsel, mine);
-  __syncthreads();
-  // Few candidates under the cut (the usual case): the warp lists take them
-  // all. Otherwise a radix select of the K-th smallest leading word, most
-  // significant digit first, keeps the K best and their ties.
-  const bool few = s_nsel <= 2u * kMsThreads;
-  __syncthreads();
-  if (threadIdx.x == 0) s_nsel = 0;
-  if (few && threadIdx.x == 0) s_prefix = ~0ULL;
-  __syncthreads();
-  uint64_t mask = 0;
-  for (int shift = 56; shift >= 0 && !few; shift -= 8) {
-    for (int b = threadIdx.x; b < 256; b += kMsThreads) s_hist[b] = 0;
-    __syncthreads();
-    const uint64_t prefix = s_prefix;
-#pragma unroll
-    for (int r = 0; r < kMsPer; ++r)
-      if (v[r] && (t[r] & mask) == prefix) atomicAdd(&s_hist[(t[r] >> shift) & 255u], 1u);
-    __syncthreads();
-    if (warp == 0) {
-      // lane l holds bins [8l, 8l + 8): find the bin where the count reaches s_need
-      uint32_t c[8], sum = 0;
-#pragma unroll
-      for (int j = 0; j < 8; ++j) {
-        c[j] = s_hist[lane * 8 + j];
-        sum += c[j];
+  for (uint32_t k = 2; k <= N; k <<= 1) {
+    for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+      for (uint32_t i = threadIdx.x; i < N; i += kMsThreads) {
+        const uint32_t ixj = i ^ j;
+        if (ixj <= i) continue;
+        const uint64_t ta = st[i], tb = st[ixj];
+        const uint32_t pa = sp[i], pb = sp[ixj];
+        const bool up = (i & k) == 0;
+        if (up ? ms_greater(ta, pa, tb, pb) : ms_greater(tb, pb, ta, pa)) {
+          st[i] = tb;
+          st[ixj] = ta;
+          sp[i] = pb;
+          sp[ixj] = pa;
+        }
       }
-      uint32_t incl = sum;
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
-        if (lane >= o) incl += y;
-      }
-      const uint32_t need = s_need;
-      const uint32_t total = __shfl_sync(0xFFFFFFFFu, incl, 31);
-      // fewer candidates than needed under this prefix: take them all (the
-      // largest digit keeps every one at or below the threshold)
-      const uint32_t want = need <= total ? need : total;
-      const uint32_t excl = incl - sum;
-      const bool mine = want > 0 && excl < want && want <= incl;
-      const uint32_t ball = __ballot_sync(0xFFFFFFFFu, mine);
-      if (ball == 0 && lane == 0) {  // no candidate under the prefix at all
-        s_prefix = prefix | (255ull << shift);
-      } else if (mine) {
-        uint32_t run = excl, d = 0;
-#pragma unroll
-        for (int j = 0; j < 8; ++j)
-          if (run < want && run + c[j] >= want) {
-            d = (uint32_t)(lane * 8 + j);
-            break;
-          } else {
-            run += c[j];
-          }
-        s_prefix = prefix | ((uint64_t)d << shift);
-        s_need = want - run;
-      }
+      __syncthreads();
     }
-    mask |= 255ull << shift;
-    __syncthreads();
   }
-  // the K best have leading words at or below the selected one
-  const uint64_t thr = s_prefix;
-#pragma unroll
-  for (int r = 0; r < kMsPer; ++r)
-    if (v[r] && t[r] <= thr) s_sel[atomicAdd(&s_nsel, 1u)] = (uint16_t)(r * kMsThreads + threadIdx.x);
+  // the candidates at or below the K-th leading word (all valid ones when
+  // there are fewer than K)
+  const uint32_t kk = (uint32_t)K <= N ? (uint32_t)K : N;
+  const uint64_t T = st[kk - 1];
+  if (threadIdx.x == 0) {
+    uint32_t m = 0;
+    while (m < N && st[m] <= T && st[m] != ~0ULL) ++m;
+    s_m = m;
+  }
   __syncthreads();
-  const uint32_t ns = s_nsel;
-  Cand L = cand_inf();
-  for (uint32_t base = (uint32_t)warp * 32; base < ns; base += kMsThreads) {
-    const uint32_t q = base + lane;
+  const uint32_t m = s_m;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  auto cand_at = [&](uint32_t q) {
     Cand c = cand_inf();
-    const bool ok = q < ns;
-    if (ok) {
-      const uint32_t i = s_sel[q];
-      const SortItem k = keys[i];
-      c.w[0] = k.w[0]; c.w[1] = k.w[1]; c.w[2] = k.w[2]; c.w[3] = k.w[3];
+    if (q < m) {
+      const uint32_t i = sp[q];
+      c.w[0] = keys[i].w[0]; c.w[1] = keys[i].w[1]; c.w[2] = keys[i].w[2]; c.w[3] = keys[i].w[3];
       c.ix = idx[i];
     }
-    warp_offer_batch(L, c, ok, K, lane);
+    return c;
+  };
+  if (m <= 32) {
+    if (warp == 0) {
+      Cand c = cand_at((uint32_t)lane);
+      warp_sort32(c, lane);
+      const bool ok = lane < K && c.ix != 0xFFFFFFFFu;
+      const uint32_t valid = __ballot_sync(0xFFFFFFFFu, ok);
+      if (ok) out_idx[lane] = c.ix;
+      if (lane == 0) *out_count = (uint64_t)__popc(valid);
+    }
+  } else {
+    // many ties at T: warp lists over them
+    Cand L = cand_inf();
+    for (uint32_t base = (uint32_t)warp * 32; base < m; base += kMsThreads) {
+      const Cand c = cand_at(base + (uint32_t)lane);
+      warp_offer_batch(L, c, base + (uint32_t)lane < m, K, lane);
+    }
+    block_merge_lists<kMsThreads / 32>(L, s_l, warp, lane);
+    if (warp == 0) {
+      const bool ok = lane < K && L.ix != 0xFFFFFFFFu;
+      const uint32_t valid = __ballot_sync(0xFFFFFFFFu, ok);
+      if (ok) out_idx[lane] = L.ix;
+      if (lane == 0) *out_count = (uint64_t)__popc(valid);
+    }
   }
-  block_merge_lists<WARPS>(L, s_l, warp, lane);
-  if (warp == 0) {
-    const uint32_t valid = __ballot_sync(0xFFFFFFFFu, lane < K && L.ix != 0xFFFFFFFFu);
-    if (lane < K && L.ix != 0xFFFFFFFFu) out_idx[lane] = L.ix;
-    if (lane == 0) *out_count = (uint64_t)__popc(valid);
-  }
-  // every thread read *count and the cut before the barriers above
-  if (reset && threadIdx.x == 0) {
+  if (threadIdx.x == 0 && reset) {
     reset[0] = 0;
     reset[1] = 0;
   }
@@ -898,12 +853,25 @@ cudaError_t launch_topk_final(const TopkFinalSpec& spec, int k, uint32_t* out_g,
   uint32_t* pi = (uint32_t*)(pk + (uint64_t)ctas * k);
   if (phase != 2) k_topk_final<kTfThreads><<<ctas, kTfThreads, 0, s>>>(spec, k, gst, pk, pi);
   if (phase != 1) {
-    if ((uint64_t)ctas * k <= (uint64_t)kMsMax)
-      k_topk_merge_select<<<1, kMsThreads, 0, s>>>(pk, pi, (const uint64_t*)&gst->n_cand, (uint64_t)ctas * k, k,
-                                                   spec.total_bits, out_g, out_count, (uint64_t*)gst);
-    else
-      k_topk_warp<1024><<<1, 1024, 0, s>>>(pk, pi, (const uint64_t*)&gst->n_cand, (uint64_t)ctas * k, k, nullptr,
-                                           out_g, out_count, 1, nullptr, (uint64_t*)gst, spec.total_bits);
+    const uint32_t n = ctas * (uint32_t)k;
+    uint32_t N = 32;
+    while (N < n) N <<= 1;
+    if (N <= kMsMaxN) {
+      // the opt-in shared memory limit, raised once for the largest size used here
+      static std::once_flag once;
+      static cudaError_t attr = cudaSuccess;
+      std::call_once(once, [] {
+        attr = cudaFuncSetAttribute(k_topk_merge_sort, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)(kMsMaxN * (sizeof(uint64_t) + sizeof(uint32_t))));
+      });
+      if (attr != cudaSuccess) return attr;
+      k_topk_merge_sort<<<1, kMsThreads, (size_t)N * (sizeof(uint64_t) + sizeof(uint32_t)), s>>>(
+          pk, pi, n, N, k, spec.total_bits, out_g, out_count, (uint64_t*)gst);
+    } else {
+      // the padded lists as one array (padding skipped)
+      k_topk_warp<1024><<<1, 1024, 0, s>>>(pk, pi, nullptr, (uint64_t)n, k, nullptr, out_g, out_count, 1, nullptr,
+                                           (uint64_t*)gst, spec.total_bits);
+    }
   }
   return cudaGetLastError();
 }

@@ -11,9 +11,9 @@
 // * The array holds kScratchBytes (1 MiB) on every GPU that loads the
 //   library, for as long as the process lives.
 // * All calls share it, and it keeps whatever the last call left in it.
-//   Its first 256 bytes (the pruning cut and the candidate count shared by
-//   the CTAs of one call) must start at zero, so every call clears them on
-//   its stream before the kernels run; the candidate lists need no clearing.
+//   Its first 256 bytes (the pruning cut shared by the CTAs of one call)
+//   must start at zero, so every call clears them on its stream before the
+//   kernels run; the per-CTA candidate slots are all written by every call.
 //   Calls whose kernels overlap on the GPU (on different streams, or from
 //   different host threads without ordering) race on the array and can
 //   return wrong rows; order them on one stream.

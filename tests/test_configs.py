@@ -258,6 +258,48 @@ def test_few_groups_edge_keys_and_wide_sums(conn, tmp_path, monkeypatch):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("groups,dist", [(1, "uniform"), (3, "zipf"), (12, "uniform")])
+def test_fewest_groups_thread_private_states(conn, groups, dist):
+    """The fewest groups: every thread keeps its own states of every group
+    and the threads' states are combined at the end. All ten aggregates of
+    every group against the oracle."""
+    init(conn)
+    d = W.groupby(n=5_000_000, groups=groups, dist=dist, seed_salt=groups + 11)
+    conn.create_table("t", {"k": (L.T_BIGINT, d["k"]), "v": (L.T_BIGINT, d["v"]), "f": (L.T_FLOAT, d["f"])})
+    conn.gpu_register_table("t", upload=True)
+    assert any(s.startswith("agg_few") for s in _step_names(conn, C3_ALL_GROUPS_SQL))
+    want = orc.groupby_c3(d["k"], d["v"], d["f"], limit=-1)
+    _check_c3_all_groups(conn.gpu_processing(C3_ALL_GROUPS_SQL), want)
+    r = conn.gpu_processing(W.C3_SQL)
+    top = orc.groupby_c3(d["k"], d["v"], d["f"], limit=100)
+    assert np.array_equal(r.columns[0], top["k"]) and np.array_equal(r.columns[5], top["avg_v"])
+
+
+@pytest.mark.gpu
+def test_fewest_groups_edge_keys_and_wide_sums(conn):
+    """Five groups whose keys are the empty-slot sentinel (-1; its rows
+    update the global table directly) and both int64 extremes, with sums
+    that need 128 bits."""
+    init(conn)
+    r = np.random.default_rng(5)
+    n = 2_000_000
+    keys = np.array([-1, np.iinfo(np.int64).min, np.iinfo(np.int64).max, 0, 42], dtype=np.int64)
+    k = keys[r.integers(0, 5, n)]
+    v = r.integers(2**61, 2**62, n).astype(np.int64)
+    conn.create_table("w", {"k": (L.T_BIGINT, k), "v": (L.T_BIGINT, v)})
+    conn.gpu_register_table("w")
+    sql = "SELECT k, COUNT(*), SUM(v), MIN(v), MAX(v) FROM w GROUP BY k ORDER BY k"
+    assert any(s.startswith("agg_few") for s in _step_names(conn, sql))
+    rows = conn.gpu_processing(sql).fetchall()
+    want = _grouped(k, {"v": v.astype(object)})
+    assert [x[0] for x in rows] == want["k"].tolist()
+    assert [x[1] for x in rows] == want["cnt"].tolist()
+    assert [int(x[2]) for x in rows] == [int(s) for s in want["v_sum"]]
+    assert [x[3] for x in rows] == [int(s) for s in want["v_min"]]
+    assert [x[4] for x in rows] == [int(s) for s in want["v_max"]]
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("n,groups,dist", [(20_000_000, 4_000_000, "uniform"), (40_000_000, 8_000_000, "zipf")])
 def test_c3_many_partitions_all_groups(conn, n, groups, dist):
     """Millions of groups: the partitioned aggregation at thousands of
