@@ -1234,7 +1234,11 @@ struct Compiler {
   }
 
   // ---- ORDER BY / LIMIT over dense output arrays
-  void order_and_limit(const uint64_t* count, uint64_t n_max, const std::vector<int>& tie_outs) {
+  // With `groups` and `late` (a top-K over a grouped aggregate whose ORDER BY
+  // outputs alone were finalized into dense[]), the winners' group ids are
+  // gathered from `groups` and the visible outputs finalized for them only.
+  void order_and_limit(const uint64_t* count, uint64_t n_max, const std::vector<int>& tie_outs,
+                       const uint32_t* groups = nullptr, const std::vector<FinalOut>* late = nullptr) {
     P.limit = plan.limit;
     std::vector<int> vis;
     for (size_t i = 0; i < plan.outputs.size(); ++i)
@@ -1307,6 +1311,36 @@ struct Compiler {
       final_idx = oidx;
       final_count = ocnt;
       rows_max = std::min<uint64_t>(n_max, (uint64_t)K);
+      if (late) {
+        uint32_t* wg = (uint32_t*)scratch((uint64_t)K * 4);
+        Step g;
+        g.k = Step::GATHER;
+        g.gin = groups;
+        g.width = 4;
+        g.idx = oidx;
+        g.count = ocnt;
+        g.n_max = (uint64_t)K;
+        g.gout = wg;
+        P.steps.push_back(g);
+        P.kernels += 1;
+        std::vector<FinalOut> vf;
+        for (int i : vis) {
+          FinalOut f = (*late)[i];
+          f.out = scratch((uint64_t)K * dense[i].width);
+          vf.push_back(f);
+          OutBuf ob;
+          ob.name = plan.outputs[i].name;
+          ob.type = plan.outputs[i].type;
+          ob.dev = f.out;
+          ob.width = dense[i].width;
+          ob.dict = plan.outputs[i].dict;
+          P.outs.push_back(ob);
+        }
+        if (!vf.empty()) finalize_step(upload_finals(vf), (int)vf.size(), wg, ocnt, (uint64_t)K);
+        P.out_count = ocnt;
+        P.n_max = rows_max;
+        return;
+      }
     } else {
       SortItem* keys2 = (SortItem*)scratch(std::max<uint64_t>(n_max, 1) * sizeof(SortItem));
       uint32_t* kidx2 = (uint32_t*)scratch(std::max<uint64_t>(n_max, 1) * 4);
@@ -1687,6 +1721,23 @@ struct Compiler {
     uint32_t* gidx = (uint32_t*)scratch(n_ent * 4);
     uint64_t* gcnt = (uint64_t*)scratch(8);
     compact_step(pb.d.table.state, n_ent, nullptr, gidx, gcnt, true);
+    if (!plan.order.empty() && plan.limit > 0 && plan.limit <= 1024) {
+      // ORDER BY ... LIMIT K: only the ordering outputs (and tie-breaks) for
+      // every group; the other outputs only for the K winners
+      std::vector<char> need(fo.size(), 0);
+      for (const BOrder& o : plan.order) need[o.out] = 1;
+      for (int t : tie) need[t] = 1;
+      std::vector<FinalOut> ford;
+      for (size_t i = 0; i < fo.size(); ++i)
+        if (need[i]) {
+          FinalOut f = fo[i];
+          f.out = dense[i].dev = scratch(n_ent * dense[i].width);
+          ford.push_back(f);
+        }
+      finalize_step(upload_finals(ford), (int)ford.size(), gidx, gcnt, n_ent);
+      order_and_limit(gcnt, n_ent, tie, gidx, &fo);
+      return;
+    }
     for (size_t i = 0; i < fo.size(); ++i) fo[i].out = dense[i].dev = scratch(n_ent * dense[i].width);
     finalize_step(upload_finals(fo), (int)fo.size(), gidx, gcnt, n_ent);
     order_and_limit(gcnt, n_ent, tie);
