@@ -586,11 +586,11 @@ __device__ __forceinline__ int64_t tc_get(const TileCtx& t, int col, uint32_t r)
 // (the width store_val picks), G whether the column is read from HBM at the
 // driving source's rows rather than from the streamed tile. f maps the
 // loaded value (widened to int64, as the VM holds it) to the stored one.
-// Four rows per lane (eight from HBM) are loaded before any is stored.
+// Four rows per lane are loaded before any is stored.
 template <typename TIn, typename TOut, bool G, class F>
 __device__ __forceinline__ void write_rows(const TIn* __restrict__ src, TOut* __restrict__ dst, uint32_t lim,
                                            bool ident, const uint16_t* sel, int lane, F f) {
-  constexpr int B = G ? 8 : 4;
+  constexpr int B = 4;
   auto ld = [&](uint32_t q) -> int64_t {
     const uint32_t r = ident ? q : (uint32_t)sel[q];
     if (G) return (int64_t)__ldg(src + r);

@@ -264,6 +264,8 @@ __device__ void bitonic_sort(SortItem* sk, uint32_t* si) {
   }
 }
 
+constexpr int kTopkRows = 8;  // rows per thread loaded together in k_topk
+
 // Per-CTA top-K. Rows are taken in rounds of THREADS; a row enters the
 // candidate buffer only if it beats the current K-th best, and the buffer is
 // merged (bitonic sort of best-K + candidates) whenever it could overflow.
@@ -304,21 +306,33 @@ __global__ void __launch_bounds__(THREADS) k_topk(const SortItem* __restrict__ k
     }
     __syncthreads();
   };
-  for (uint64_t base = lo; base < hi; base += THREADS) {
-    const uint64_t g = base + threadIdx.x;
-    if (g < hi) {
-      SortItem k = keys[g];
-      uint32_t ix = idx ? idx[g] : (uint32_t)g;
-      // 0xFFFFFFFF marks padding from the per-CTA pass.
-      bool take = ix != 0xFFFFFFFFu && (s_have < K || item_less(k, ix, sk[K - 1], si[K - 1]));
-      if (take) {
-        int p = atomicAdd(&s_n, 1);
-        sk[p] = k;
-        si[p] = ix;
+  // Rows are loaded kTopkRows per thread at a time (all loads in flight
+  // together), then offered one THREADS-row step at a time.
+  for (uint64_t base = lo; base < hi; base += (uint64_t)THREADS * kTopkRows) {
+    SortItem kr[kTopkRows];
+    uint32_t ir[kTopkRows];
+#pragma unroll
+    for (int r = 0; r < kTopkRows; ++r) {
+      const uint64_t g = base + (uint64_t)r * THREADS + threadIdx.x;
+      ir[r] = 0xFFFFFFFFu;
+      if (g < hi) {
+        kr[r] = keys[g];
+        ir[r] = idx ? idx[g] : (uint32_t)g;
       }
     }
-    __syncthreads();
-    if (s_n > B - THREADS) merge();
+#pragma unroll
+    for (int r = 0; r < kTopkRows; ++r) {
+      if (base + (uint64_t)r * THREADS >= hi) break;  // CTA-uniform
+      // 0xFFFFFFFF marks padding from the per-CTA pass (and rows past the end).
+      const bool take = ir[r] != 0xFFFFFFFFu && (s_have < K || item_less(kr[r], ir[r], sk[K - 1], si[K - 1]));
+      if (take) {
+        const int p = atomicAdd(&s_n, 1);
+        sk[p] = kr[r];
+        si[p] = ir[r];
+      }
+      __syncthreads();
+      if (s_n > B - THREADS) merge();
+    }
   }
   if (s_n > s_have || s_have < K) merge();
   const int m = s_have;
@@ -713,107 +727,81 @@ __global__ void __launch_bounds__(THREADS) k_topk_final(const __grid_constant__ 
 }
 
 // Merge pass of the fused top-K. The first pass leaves each CTA's K best in
-// the CTA's own K slots (padding, index 0xFFFFFFFF, after the last that can
-// still win). One CTA sorts the candidates' leading 64 key bits, with their
-// positions, by a bitonic sort in shared memory (every compare-exchange of a
-// pass in parallel, log^2 passes); the K-th leading word T then bounds the
-// winners: every candidate below T wins, and those equal to T are ordered
-// by their full keys. The m <= 32 candidates at or below T are sorted by
-// their full keys with one warp sort and the first K are the result (more
-// than 32 ties at T go through warp lists). A block-wide sort instead of a
-// serial merge: its depth is the passes, not the candidates or the rounds.
-constexpr int kMsThreads = 1024;
-constexpr uint32_t kMsMaxN = 8192;  // candidates (power of two) the shared arrays hold
+// the CTA's own K slots, best first (padding, index 0xFFFFFFFF, after the last
+// that can still win). The K-th smallest of the lists' heads, H, bounds the
+// result: the K heads at or below H are K candidates, so no candidate above
+// H wins, and only the (at most K) lists whose heads are at or below H hold
+// candidates at or below it: at most K * K survivors. One CTA ranks the heads
+// by counting (each thread one head against all), keeps the candidates at or
+// below H, and ranks those by counting again; every step is parallel over
+// the CTA, with three barriers. (A serial merge of the lists on one warp, a
+// radix select and a bitonic sort of all candidates each measured 35-88 us
+// here: one CTA's dependent steps are latency-bound.)
+constexpr int kMhThreads = 1024;
 
-__device__ __forceinline__ bool ms_greater(uint64_t ta, uint32_t pa, uint64_t tb, uint32_t pb) {
-  return ta > tb || (ta == tb && pa > pb);
-}
-
-__global__ void __launch_bounds__(kMsThreads) k_topk_merge_sort(const SortItem* __restrict__ keys,
-                                                                const uint32_t* __restrict__ idx, uint32_t n,
-                                                                uint32_t N, int K, int cut_bits,
-                                                                uint32_t* __restrict__ out_idx, uint64_t* out_count,
-                                                                uint64_t* reset) {
-  extern __shared__ __align__(16) uint8_t ms_smem[];
-  uint64_t* const st = (uint64_t*)ms_smem;      // leading key words (padding: all ones)
-  uint32_t* const sp = (uint32_t*)(st + N);      // candidate positions
-  __shared__ uint32_t s_m;
-  __shared__ Cand s_l[kMsThreads / 32][32];
-  for (uint32_t i = threadIdx.x; i < N; i += kMsThreads) {
-    uint64_t t = ~0ULL;
-    if (i < n && idx[i] != 0xFFFFFFFFu) t = key_top64(keys[i].w, cut_bits);
-    st[i] = t;
-    sp[i] = i;
-  }
-  __syncthreads();
-  for (uint32_t k = 2; k <= N; k <<= 1) {
-    for (uint32_t j = k >> 1; j > 0; j >>= 1) {
-      for (uint32_t i = threadIdx.x; i < N; i += kMsThreads) {
-        const uint32_t ixj = i ^ j;
-        if (ixj <= i) continue;
-        const uint64_t ta = st[i], tb = st[ixj];
-        const uint32_t pa = sp[i], pb = sp[ixj];
-        const bool up = (i & k) == 0;
-        if (up ? ms_greater(ta, pa, tb, pb) : ms_greater(tb, pb, ta, pa)) {
-          st[i] = tb;
-          st[ixj] = ta;
-          sp[i] = pb;
-          sp[ixj] = pa;
-        }
-      }
-      __syncthreads();
-    }
-  }
-  // the candidates at or below the K-th leading word (all valid ones when
-  // there are fewer than K)
-  const uint32_t kk = (uint32_t)K <= N ? (uint32_t)K : N;
-  const uint64_t T = st[kk - 1];
-  if (threadIdx.x == 0) {
-    uint32_t m = 0;
-    while (m < N && st[m] <= T && st[m] != ~0ULL) ++m;
-    s_m = m;
-  }
-  __syncthreads();
-  const uint32_t m = s_m;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  auto cand_at = [&](uint32_t q) {
+__global__ void __launch_bounds__(kMhThreads) k_topk_merge_heads(const SortItem* __restrict__ keys,
+                                                                 const uint32_t* __restrict__ idx, uint32_t lists,
+                                                                 int K, uint32_t* __restrict__ out_idx,
+                                                                 uint64_t* out_count, uint64_t* reset) {
+  extern __shared__ __align__(16) uint8_t mh_smem[];
+  Cand* const s_head = (Cand*)mh_smem;        // [lists]
+  Cand* const s_sel = s_head + lists;         // [K * K]
+  __shared__ Cand s_h;
+  __shared__ uint32_t s_valid, s_m;
+  auto load = [&](uint64_t i) {
     Cand c = cand_inf();
-    if (q < m) {
-      const uint32_t i = sp[q];
-      c.w[0] = keys[i].w[0]; c.w[1] = keys[i].w[1]; c.w[2] = keys[i].w[2]; c.w[3] = keys[i].w[3];
-      c.ix = idx[i];
+    const uint32_t ix = idx[i];
+    if (ix != 0xFFFFFFFFu) {
+      const SortItem k = keys[i];
+      c.w[0] = k.w[0]; c.w[1] = k.w[1]; c.w[2] = k.w[2]; c.w[3] = k.w[3];
+      c.ix = ix;
     }
     return c;
   };
-  if (m <= 32) {
-    if (warp == 0) {
-      Cand c = cand_at((uint32_t)lane);
-      warp_sort32(c, lane);
-      const bool ok = lane < K && c.ix != 0xFFFFFFFFu;
-      const uint32_t valid = __ballot_sync(0xFFFFFFFFu, ok);
-      if (ok) out_idx[lane] = c.ix;
-      if (lane == 0) *out_count = (uint64_t)__popc(valid);
-    }
-  } else {
-    // many ties at T: warp lists over them
-    Cand L = cand_inf();
-    for (uint32_t base = (uint32_t)warp * 32; base < m; base += kMsThreads) {
-      const Cand c = cand_at(base + (uint32_t)lane);
-      warp_offer_batch(L, c, base + (uint32_t)lane < m, K, lane);
-    }
-    block_merge_lists<kMsThreads / 32>(L, s_l, warp, lane);
-    if (warp == 0) {
-      const bool ok = lane < K && L.ix != 0xFFFFFFFFu;
-      const uint32_t valid = __ballot_sync(0xFFFFFFFFu, ok);
-      if (ok) out_idx[lane] = L.ix;
-      if (lane == 0) *out_count = (uint64_t)__popc(valid);
-    }
+  if (threadIdx.x == 0) {
+    s_valid = 0;
+    s_m = 0;
+    s_h = cand_inf();
   }
-  if (threadIdx.x == 0 && reset) {
-    reset[0] = 0;
-    reset[1] = 0;
+  for (uint32_t l = threadIdx.x; l < lists; l += kMhThreads) s_head[l] = load((uint64_t)l * K);
+  __syncthreads();
+  // the K-th smallest head (its rank among the heads is K - 1)
+  for (uint32_t l = threadIdx.x; l < lists; l += kMhThreads) {
+    const Cand h = s_head[l];
+    if (h.ix == 0xFFFFFFFFu) continue;
+    atomicAdd(&s_valid, 1u);
+    uint32_t rank = 0;
+    for (uint32_t j = 0; j < lists; ++j) rank += cand_less(s_head[j], h) ? 1u : 0u;
+    if (rank == (uint32_t)K - 1) s_h = h;
+  }
+  __syncthreads();
+  // fewer valid heads than K: every valid candidate survives
+  const Cand H = s_valid >= (uint32_t)K ? s_h : cand_inf();
+  const uint32_t n = lists * (uint32_t)K;
+  for (uint32_t i = threadIdx.x; i < n; i += kMhThreads) {
+    const Cand c = load(i);
+    if (c.ix != 0xFFFFFFFFu && !cand_less(H, c)) s_sel[atomicAdd(&s_m, 1u)] = c;
+  }
+  __syncthreads();
+  const uint32_t m = s_m;
+  for (uint32_t p = threadIdx.x; p < m; p += kMhThreads) {
+    const Cand c = s_sel[p];
+    uint32_t rank = 0;
+    for (uint32_t q = 0; q < m; ++q) rank += cand_less(s_sel[q], c) ? 1u : 0u;
+    if (rank < (uint32_t)K) out_idx[rank] = c.ix;
+  }
+  if (threadIdx.x == 0) {
+    *out_count = m < (uint32_t)K ? m : (uint32_t)K;
+    if (reset) {
+      reset[0] = 0;
+      reset[1] = 0;
+    }
   }
 }
+
+// Dynamic shared memory of the merge: the heads and the survivors.
+static size_t merge_heads_smem(unsigned lists, int k) { return ((size_t)lists + (size_t)k * k) * sizeof(Cand); }
+constexpr size_t kMhMaxSmem = 200 * 1024;
 
 constexpr int kTfThreads = 256;  // first pass
 constexpr int kTfItems = 16;     // groups per lane per step
@@ -853,24 +841,20 @@ cudaError_t launch_topk_final(const TopkFinalSpec& spec, int k, uint32_t* out_g,
   uint32_t* pi = (uint32_t*)(pk + (uint64_t)ctas * k);
   if (phase != 2) k_topk_final<kTfThreads><<<ctas, kTfThreads, 0, s>>>(spec, k, gst, pk, pi);
   if (phase != 1) {
-    const uint32_t n = ctas * (uint32_t)k;
-    uint32_t N = 32;
-    while (N < n) N <<= 1;
-    if (N <= kMsMaxN) {
+    const size_t smem = merge_heads_smem(ctas, k);
+    if (smem <= kMhMaxSmem) {
       // the opt-in shared memory limit, raised once for the largest size used here
       static std::once_flag once;
       static cudaError_t attr = cudaSuccess;
       std::call_once(once, [] {
-        attr = cudaFuncSetAttribute(k_topk_merge_sort, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)(kMsMaxN * (sizeof(uint64_t) + sizeof(uint32_t))));
+        attr = cudaFuncSetAttribute(k_topk_merge_heads, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMhMaxSmem);
       });
       if (attr != cudaSuccess) return attr;
-      k_topk_merge_sort<<<1, kMsThreads, (size_t)N * (sizeof(uint64_t) + sizeof(uint32_t)), s>>>(
-          pk, pi, n, N, k, spec.total_bits, out_g, out_count, (uint64_t*)gst);
+      k_topk_merge_heads<<<1, kMhThreads, smem, s>>>(pk, pi, ctas, k, out_g, out_count, (uint64_t*)gst);
     } else {
       // the padded lists as one array (padding skipped)
-      k_topk_warp<1024><<<1, 1024, 0, s>>>(pk, pi, nullptr, (uint64_t)n, k, nullptr, out_g, out_count, 1, nullptr,
-                                           (uint64_t*)gst, spec.total_bits);
+      k_topk_warp<1024><<<1, 1024, 0, s>>>(pk, pi, nullptr, (uint64_t)ctas * k, k, nullptr, out_g, out_count, 1,
+                                           nullptr, (uint64_t*)gst, spec.total_bits);
     }
   }
   return cudaGetLastError();
