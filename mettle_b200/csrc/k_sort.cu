@@ -741,11 +741,13 @@ constexpr int kMhThreads = 1024;
 
 __global__ void __launch_bounds__(kMhThreads) k_topk_merge_heads(const SortItem* __restrict__ keys,
                                                                  const uint32_t* __restrict__ idx, uint32_t lists,
-                                                                 int K, uint32_t* __restrict__ out_idx,
+                                                                 int K, int cut_bits, uint32_t* __restrict__ out_idx,
                                                                  uint64_t* out_count, uint64_t* reset) {
   extern __shared__ __align__(16) uint8_t mh_smem[];
-  Cand* const s_head = (Cand*)mh_smem;        // [lists]
-  Cand* const s_sel = s_head + lists;         // [K * K]
+  Cand* const s_head = (Cand*)mh_smem;             // [lists]
+  Cand* const s_sel = s_head + lists;              // [K * K]
+  uint64_t* const s_ht = (uint64_t*)(s_sel + (size_t)K * K);  // [lists] leading 64 key bits of each head
+  uint32_t* const s_rank = (uint32_t*)(s_ht + lists);         // [lists]
   __shared__ Cand s_h;
   __shared__ uint32_t s_valid, s_m;
   auto load = [&](uint64_t i) {
@@ -758,36 +760,60 @@ __global__ void __launch_bounds__(kMhThreads) k_topk_merge_heads(const SortItem*
     }
     return c;
   };
+  // a before b in the result's order: leading words first, full keys on ties
+  auto before = [&](uint64_t ta, const Cand& a, uint64_t tb, const Cand& b) {
+    return ta < tb || (ta == tb && cand_less(a, b));
+  };
   if (threadIdx.x == 0) {
     s_valid = 0;
     s_m = 0;
     s_h = cand_inf();
   }
-  for (uint32_t l = threadIdx.x; l < lists; l += kMhThreads) s_head[l] = load((uint64_t)l * K);
-  __syncthreads();
-  // the K-th smallest head (its rank among the heads is K - 1)
   for (uint32_t l = threadIdx.x; l < lists; l += kMhThreads) {
+    const Cand h = load((uint64_t)l * K);
+    s_head[l] = h;
+    s_ht[l] = h.ix == 0xFFFFFFFFu ? ~0ULL : key_top64(h.w, cut_bits);
+    s_rank[l] = 0;
+  }
+  __syncthreads();
+  // Rank of every valid head among the heads: P threads per head, each
+  // counting the heads before it in one share of the list.
+  const uint32_t P = lists >= kMhThreads ? 1u : (kMhThreads / lists < 32 ? kMhThreads / lists : 32);
+  for (uint32_t t = threadIdx.x; t < lists * P; t += kMhThreads) {
+    const uint32_t l = t / P, part = t % P;
     const Cand h = s_head[l];
     if (h.ix == 0xFFFFFFFFu) continue;
-    atomicAdd(&s_valid, 1u);
-    uint32_t rank = 0;
-    for (uint32_t j = 0; j < lists; ++j) rank += cand_less(s_head[j], h) ? 1u : 0u;
-    if (rank == (uint32_t)K - 1) s_h = h;
+    const uint64_t th = s_ht[l];
+    if (part == 0) atomicAdd(&s_valid, 1u);
+    uint32_t r = 0;
+    for (uint32_t j = part; j < lists; j += P) {
+      const uint64_t tj = s_ht[j];
+      if (tj < th) ++r;
+      else if (tj == th && j != l && cand_less(s_head[j], h)) ++r;
+    }
+    atomicAdd(&s_rank[l], r);
   }
+  __syncthreads();
+  for (uint32_t l = threadIdx.x; l < lists; l += kMhThreads)
+    if (s_head[l].ix != 0xFFFFFFFFu && s_rank[l] == (uint32_t)K - 1) s_h = s_head[l];
   __syncthreads();
   // fewer valid heads than K: every valid candidate survives
   const Cand H = s_valid >= (uint32_t)K ? s_h : cand_inf();
+  const uint64_t tH = H.ix == 0xFFFFFFFFu ? ~0ULL : key_top64(H.w, cut_bits);
   const uint32_t n = lists * (uint32_t)K;
   for (uint32_t i = threadIdx.x; i < n; i += kMhThreads) {
     const Cand c = load(i);
-    if (c.ix != 0xFFFFFFFFu && !cand_less(H, c)) s_sel[atomicAdd(&s_m, 1u)] = c;
+    if (c.ix == 0xFFFFFFFFu) continue;
+    const uint64_t tc = key_top64(c.w, cut_bits);
+    if (tc < tH || (tc == tH && !cand_less(H, c))) s_sel[atomicAdd(&s_m, 1u)] = c;
   }
   __syncthreads();
   const uint32_t m = s_m;
   for (uint32_t p = threadIdx.x; p < m; p += kMhThreads) {
     const Cand c = s_sel[p];
+    const uint64_t tc = key_top64(c.w, cut_bits);
     uint32_t rank = 0;
-    for (uint32_t q = 0; q < m; ++q) rank += cand_less(s_sel[q], c) ? 1u : 0u;
+    for (uint32_t q = 0; q < m; ++q) rank += before(key_top64(s_sel[q].w, cut_bits), s_sel[q], tc, c) ? 1u : 0u;
     if (rank < (uint32_t)K) out_idx[rank] = c.ix;
   }
   if (threadIdx.x == 0) {
@@ -800,7 +826,9 @@ __global__ void __launch_bounds__(kMhThreads) k_topk_merge_heads(const SortItem*
 }
 
 // Dynamic shared memory of the merge: the heads and the survivors.
-static size_t merge_heads_smem(unsigned lists, int k) { return ((size_t)lists + (size_t)k * k) * sizeof(Cand); }
+static size_t merge_heads_smem(unsigned lists, int k) {
+  return ((size_t)lists + (size_t)k * k) * sizeof(Cand) + (size_t)lists * (sizeof(uint64_t) + sizeof(uint32_t));
+}
 constexpr size_t kMhMaxSmem = 200 * 1024;
 
 constexpr int kTfThreads = 256;  // first pass
@@ -850,7 +878,8 @@ cudaError_t launch_topk_final(const TopkFinalSpec& spec, int k, uint32_t* out_g,
         attr = cudaFuncSetAttribute(k_topk_merge_heads, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMhMaxSmem);
       });
       if (attr != cudaSuccess) return attr;
-      k_topk_merge_heads<<<1, kMhThreads, smem, s>>>(pk, pi, ctas, k, out_g, out_count, (uint64_t*)gst);
+      k_topk_merge_heads<<<1, kMhThreads, smem, s>>>(pk, pi, ctas, k, spec.total_bits, out_g, out_count,
+                                                     (uint64_t*)gst);
     } else {
       // the padded lists as one array (padding skipped)
       k_topk_warp<1024><<<1, 1024, 0, s>>>(pk, pi, nullptr, (uint64_t)ctas * k, k, nullptr, out_g, out_count, 1,
