@@ -195,7 +195,8 @@ class Workload:
             # count pass, a scan and a write pass (the autotuner picks)
             self.dom_candidates = [("pipeline:materialize:numbers", self.dom_bytes),
                                    ("pipeline:mat_write:numbers", self.dom_bytes),
-                                   ("pipeline:mat_count:numbers", 4 * self.rows), ("radix_sort", 8 * sel)]
+                                   ("pipeline:mat_count:numbers", 4 * self.rows), ("radix_sort", 8 * sel),
+                                   ("gather_outs", 16 * sel)]
             self.desc = "c1 numbers 1M rows: SELECT value, value*10 WHERE value > 500000 ORDER BY value"
         elif name == "c2":
             self.rows = int(100_000_000 * scale)
@@ -209,7 +210,7 @@ class Workload:
             # moves every selected row: the query's bytes; the count pass
             # reads `a` only
             self.dom_candidates = [("pipeline:materialize:t", self.bytes), ("pipeline:mat_write:t", self.bytes),
-                                   ("pipeline:mat_count:t", 4 * self.rows)]
+                                   ("pipeline:mat_count:t", 4 * self.rows), ("gather_outs", 56 * sel)]
             self.desc = f"c2 scan {self.rows} rows (a,b,c,d,e): SELECT a, b+5, c*10, d, e WHERE a < 2^30 (50%)"
         elif name == "c3":
             g = groups or int(os.environ.get("C3_GROUPS", "1000000"))

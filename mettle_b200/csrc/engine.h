@@ -188,7 +188,8 @@ struct Step {
     MEMSET, FILL, PIPELINE, COMPACT_FLAGS, COMPACT_READY, FINALIZE, ENCODE, RADIX, TOPK, TOPK_FINAL, GATHER,
     PART_SCAN, PART_AGG,  // partitioned aggregation (descriptor in `pipe`)
     AGG_FEW,              // one-pass few-group aggregation (descriptor in `pipe`)
-    MAT_SCAN              // scan between the two passes of the compaction (descriptor in `pipe`)
+    MAT_SCAN,             // scan between the two passes of the compaction (descriptor in `pipe`)
+    GATHER_OUTS           // a scan's outputs gathered at its compacted row ids (go[0 .. n_go))
   } k;
   std::string name;  // for per-step profiles, e.g. "pipeline:agg_slot:lineitem"
   // MEMSET / FILL (u64 words)
@@ -217,6 +218,8 @@ struct Step {
   // FINALIZE
   FinalOut* fin_dev = nullptr;
   int n_fin = 0;
+  GatherOut* go = nullptr;
+  int n_go = 0;
   const uint32_t* idx = nullptr;
   const uint64_t* count = nullptr;
   uint64_t n_max = 0;

@@ -1515,6 +1515,33 @@ struct Compiler {
       const bool injected = ctx.inject_kind.load() == MTL_INJECT_LOOKBACK_STALL;
       const int mstrat = injected ? 1 : tune_mat_strategy(ctx, root_rows);
       P.mat_strategy_key = injected ? "" : tune_key_mat(root_rows);
+      // Late gather: a scan of one table whose outputs are its columns,
+      // plain or combined with one constant, writes only the surviving row
+      // ids in the write pass; one kernel then gathers every output at them
+      // (all source loads of a row in flight together).
+      std::vector<GatherOut> gos;
+      if (mstrat != 1 && root_rows < (1ull << 32) && plan.sources.size() == 1 && pb.d.n_probes == 0)
+        for (size_t i = 0; i < plan.outputs.size(); ++i) {
+          const VmProg& pg = pb.d.progs[pb.d.out_prog[i]];
+          const bool plain = pg.n == 1 && pg.ins[0].op == VM_COL;
+          const bool arith = pg.n == 3 && pg.ins[0].op == VM_COL && pg.ins[1].op == VM_CONST &&
+                             pg.ins[2].op >= VM_ADD && pg.ins[2].op <= VM_MUL && pg.ins[2].type != P_I128;
+          if (!plain && !arith) break;
+          const DCol& c = pb.d.cols[pg.ins[0].arg];
+          const int w = ptype_width(c.ptype), ow = ptype_width(pg.out_type);
+          if ((w != 4 && w != 8) || (ow != 4 && ow != 8) || c.src != root) break;
+          GatherOut g;
+          memset(&g, 0, sizeof(g));
+          g.src = c.ptr;
+          g.out = dense[i].dev;
+          g.in_kind = w == 8 ? 2 : c.ptype == P_I32 ? 0 : 1;
+          g.out_width = ow;
+          g.op = arith ? pg.ins[2].op : 0;
+          g.type = arith ? pg.ins[2].type : 0;
+          g.k = arith ? pg.ins[1].k : 0;
+          gos.push_back(g);
+        }
+      const bool late = !gos.empty() && gos.size() == plan.outputs.size();
       if (mstrat != 1 && root_rows < (1ull << 32)) {
         const uint64_t chunks = (tiles + kMatScanTiles - 1) / kMatScanTiles;
         pb.d.tile_pos = (uint32_t*)scratch(std::max<uint64_t>(tiles, 1) * 4);
@@ -1530,7 +1557,26 @@ struct Compiler {
         P.steps.push_back(sc);
         P.kernels += 2;
         pb.d.sink = SK_MAT_WRITE;
-        push_pipeline(pb, root_rows);
+        if (late) {
+          uint32_t* rid = (uint32_t*)scratch(std::max<uint64_t>(1, n_max) * 4);
+          pb.d.n_out = 0;
+          pb.d.out_rid_mask = 1u << root;
+          pb.d.out_rids[root] = rid;
+          push_pipeline(pb, root_rows);
+          GatherOut* go = (GatherOut*)scratch(gos.size() * sizeof(GatherOut));
+          upload(go, gos.data(), gos.size() * sizeof(GatherOut));
+          Step g;
+          g.k = Step::GATHER_OUTS;
+          g.go = go;
+          g.n_go = (int)gos.size();
+          g.idx = rid;
+          g.count = pb.d.out_count;
+          g.n_max = n_max;
+          P.steps.push_back(g);
+          P.kernels += 1;
+        } else {
+          push_pipeline(pb, root_rows);
+        }
         order_and_limit(pb.d.out_count, n_max, {});
         return;
       }
@@ -1803,12 +1849,6 @@ struct Compiler {
     t.out_count = oc;
     t.temp = scratch(topk_final_temp_bytes(cap, K));
     memset_step(t.temp, 0, 256);  // the launch's cross-CTA state starts at zero
-    t.topk_phase = 1;  // the first pass, then the merge as its own step
-    P.steps.push_back(t);
-    t.topk_phase = 2;
-    t.name = "topk_merge";
-    P.steps.push_back(t);
-    P.kernels += 2;
     std::vector<FinalOut> vis;
     for (size_t i = 0; i < plan.outputs.size(); ++i) {
       if (plan.outputs[i].hidden) continue;
@@ -1823,7 +1863,15 @@ struct Compiler {
       ob.dict = plan.outputs[i].dict;
       P.outs.push_back(ob);
     }
-    if (!vis.empty()) finalize_step(upload_finals(vis), (int)vis.size(), og, oc, (uint64_t)K);
+    t.topk_phase = 1;  // the first pass, then the merge as its own step
+    P.steps.push_back(t);
+    // the merge pass writes the winners' visible outputs itself
+    t.topk_phase = 2;
+    t.name = "topk_merge";
+    t.fin_dev = vis.empty() ? nullptr : upload_finals(vis);
+    t.n_fin = (int)vis.size();
+    P.steps.push_back(t);
+    P.kernels += 2;
     P.limit = plan.limit;
     P.out_count = oc;
     P.n_max = (uint64_t)K;
@@ -2099,6 +2147,7 @@ static const char* step_kind_name(Step::Kind k) {
     case Step::PART_AGG: return "part_agg";
     case Step::AGG_FEW: return "agg_few";
     case Step::MAT_SCAN: return "mat_scan";
+    case Step::GATHER_OUTS: return "gather_outs";
   }
   return "step";
 }
@@ -2139,9 +2188,11 @@ void run_program(Ctx& ctx, Program& p, cudaStream_t s) {
                        s, st.remap));
         break;
       case Step::TOPK_FINAL:
-        CK(launch_topk_final(st.tfs, st.topk, st.out_idx, st.out_count, st.temp, s, 0, st.topk_phase));
+        CK(launch_topk_final(st.tfs, st.topk, st.out_idx, st.out_count, st.temp, s, 0, st.topk_phase, st.fin_dev,
+                             st.n_fin));
         break;
       case Step::GATHER: CK(launch_gather_width(st.gin, st.width, st.idx, st.count, st.n_max, st.gout, s)); break;
+      case Step::GATHER_OUTS: CK(launch_gather_outs(st.go, st.n_go, st.idx, st.count, st.n_max, p.status, s)); break;
       case Step::PART_SCAN: CK(launch_part_scan(st.pipe, s)); break;
       case Step::PART_AGG: CK(launch_part_agg(st.pipe, st.n_hint, s)); break;
       case Step::AGG_FEW: CK(launch_agg_few(st.pipe, st.n_hint, s)); break;

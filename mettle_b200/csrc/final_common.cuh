@@ -155,4 +155,22 @@ __device__ __forceinline__ void key_part(U256& k, int32_t pt, bool desc, uint64_
   shl_or(k, bits, lo, hi);
 }
 
+// Writes output f of group g into result row i (the stores of k_finalize).
+__device__ __forceinline__ void finalize_row(const FinalOut& f, uint64_t g, uint64_t i) {
+  uint64_t lo, hi;
+  final_value(f, g, lo, hi);
+  switch (f.kind) {
+    case F_SUM_I128:
+    case F_SUM_I64_AS_I128: ((longlong2*)f.out)[i] = make_longlong2((long long)lo, (long long)hi); break;
+    case F_COPY_I32:
+    case F_COPY_F32:
+    case F_MINMAX_F32: ((uint32_t*)f.out)[i] = (uint32_t)lo; break;
+    case F_GATHER_COL:
+      if (f.width == 4) ((uint32_t*)f.out)[i] = (uint32_t)lo;
+      else ((uint64_t*)f.out)[i] = lo;
+      break;
+    default: ((uint64_t*)f.out)[i] = lo; break;
+  }
+}
+
 }  // namespace mtl

@@ -148,24 +148,81 @@ __global__ void k_finalize(const FinalOut* __restrict__ outs, int n_outs, const 
   const uint64_t n = count ? *count : n_max;
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
     const uint64_t g = idx ? idx[i] : i;
+    for (int o = 0; o < n_outs; ++o) finalize_row(outs[o], g, i);
+  }
+}
+
+// ------------------------------------------------------------ late materialization
+// Each thread takes kGoRows output rows (one per 256-row stripe of the
+// CTA's step, so that every warp access is 32 consecutive rows), reads their
+// row ids once, and then writes every output for them with its source loads
+// issued before any value is stored.
+constexpr int kGoThreads = 256;
+constexpr int kGoRows = 4;
+
+__device__ __forceinline__ int64_t gather_apply(const GatherOut& g, int64_t x, uint32_t& st) {
+  if (g.op == 0) return x;
+  const int64_t k = g.k;
+  switch (g.type) {
+    case P_I32: return fit32(g.op == VM_ADD ? x + k : g.op == VM_SUB ? x - k : x * k, st);
+    case P_I64: return g.op == VM_ADD ? add64(x, k, st) : g.op == VM_SUB ? sub64(x, k, st) : mul64(x, k, st);
+    case P_F32: {
+      const float a = as_f32(x), y = as_f32(k);
+      return f32_bits(g.op == VM_ADD ? __fadd_rn(a, y) : g.op == VM_SUB ? __fsub_rn(a, y) : __fmul_rn(a, y));
+    }
+    default: {
+      const double a = as_f64(x), y = as_f64(k);
+      return f64_bits(g.op == VM_ADD ? __dadd_rn(a, y) : g.op == VM_SUB ? __dsub_rn(a, y) : __dmul_rn(a, y));
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kGoThreads) k_gather_outs(const GatherOut* __restrict__ outs, int n_outs,
+                                                            const uint32_t* __restrict__ rid, const uint64_t* count,
+                                                            uint64_t n_max, uint32_t* status) {
+  uint64_t n = count ? *count : n_max;
+  if (n > n_max) n = n_max;
+  uint32_t st = 0;
+  const uint64_t step = (uint64_t)kGoThreads * kGoRows;
+  for (uint64_t base = (uint64_t)blockIdx.x * step; base < n; base += (uint64_t)gridDim.x * step) {
+    uint32_t r[kGoRows];
+#pragma unroll
+    for (int j = 0; j < kGoRows; ++j) {
+      const uint64_t i = base + (uint64_t)j * kGoThreads + threadIdx.x;
+      r[j] = i < n ? __ldg(rid + i) : 0u;
+    }
     for (int o = 0; o < n_outs; ++o) {
-      const FinalOut f = outs[o];
-      uint64_t lo, hi;
-      final_value(f, g, lo, hi);
-      switch (f.kind) {
-        case F_SUM_I128:
-        case F_SUM_I64_AS_I128: ((longlong2*)f.out)[i] = make_longlong2((long long)lo, (long long)hi); break;
-        case F_COPY_I32:
-        case F_COPY_F32:
-        case F_MINMAX_F32: ((uint32_t*)f.out)[i] = (uint32_t)lo; break;
-        case F_GATHER_COL:
-          if (f.width == 4) ((uint32_t*)f.out)[i] = (uint32_t)lo;
-          else ((uint64_t*)f.out)[i] = lo;
-          break;
-        default: ((uint64_t*)f.out)[i] = lo; break;
+      const GatherOut g = outs[o];
+      int64_t v[kGoRows];
+#pragma unroll
+      for (int j = 0; j < kGoRows; ++j) {
+        const uint64_t i = base + (uint64_t)j * kGoThreads + threadIdx.x;
+        v[j] = 0;
+        if (i < n) {
+          if (g.in_kind == 2) v[j] = __ldg((const long long*)g.src + r[j]);
+          else if (g.in_kind == 0) v[j] = (int64_t)__ldg((const int*)g.src + r[j]);
+          else v[j] = (int64_t)(uint32_t)__ldg((const unsigned int*)g.src + r[j]);
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < kGoRows; ++j) {
+        const uint64_t i = base + (uint64_t)j * kGoThreads + threadIdx.x;
+        if (i >= n) continue;
+        const int64_t y = gather_apply(g, v[j], st);
+        if (g.out_width == 4) ((uint32_t*)g.out)[i] = (uint32_t)y;
+        else ((int64_t*)g.out)[i] = y;
       }
     }
   }
+  if (st && status) atomicOr(status, st);
+}
+
+cudaError_t launch_gather_outs(const GatherOut* outs, int n_outs, const uint32_t* rid, const uint64_t* count,
+                               uint64_t n_max, uint32_t* status, cudaStream_t s) {
+  if (n_outs <= 0) return cudaSuccess;
+  k_gather_outs<<<grid_for((n_max + kGoRows - 1) / kGoRows, kGoThreads), kGoThreads, 0, s>>>(outs, n_outs, rid, count,
+                                                                                          n_max, status);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_finalize(const FinalOut* outs, int n_outs, const uint32_t* idx, const uint64_t* count,

@@ -742,7 +742,8 @@ constexpr int kMhThreads = 1024;
 __global__ void __launch_bounds__(kMhThreads) k_topk_merge_heads(const SortItem* __restrict__ keys,
                                                                  const uint32_t* __restrict__ idx, uint32_t lists,
                                                                  int K, int cut_bits, uint32_t* __restrict__ out_idx,
-                                                                 uint64_t* out_count, uint64_t* reset) {
+                                                                 uint64_t* out_count, uint64_t* reset,
+                                                                 const FinalOut* __restrict__ fin, int n_fin) {
   extern __shared__ __align__(16) uint8_t mh_smem[];
   Cand* const s_head = (Cand*)mh_smem;             // [lists]
   Cand* const s_sel = s_head + lists;              // [K * K]
@@ -814,7 +815,11 @@ __global__ void __launch_bounds__(kMhThreads) k_topk_merge_heads(const SortItem*
     const uint64_t tc = key_top64(c.w, cut_bits);
     uint32_t rank = 0;
     for (uint32_t q = 0; q < m; ++q) rank += before(key_top64(s_sel[q].w, cut_bits), s_sel[q], tc, c) ? 1u : 0u;
-    if (rank < (uint32_t)K) out_idx[rank] = c.ix;
+    if (rank < (uint32_t)K) {
+      out_idx[rank] = c.ix;
+      // the winner's final outputs, in its result row
+      for (int o = 0; o < n_fin; ++o) finalize_row(fin[o], c.ix, rank);
+    }
   }
   if (threadIdx.x == 0) {
     *out_count = m < (uint32_t)K ? m : (uint32_t)K;
@@ -858,7 +863,7 @@ unsigned topk_final_max_ctas_for(size_t temp_bytes, int k) {
 }
 
 cudaError_t launch_topk_final(const TopkFinalSpec& spec, int k, uint32_t* out_g, uint64_t* out_count, void* temp,
-                              cudaStream_t s, unsigned max_ctas, int phase) {
+                              cudaStream_t s, unsigned max_ctas, int phase, const FinalOut* fin, int n_fin) {
   if (k <= 0 || k > 32 || spec.n_parts <= 0 || spec.n_parts > kMaxOrder || spec.total_bits > 256 ||
       spec.bits0 <= 0 || spec.bits0 > spec.total_bits)
     return cudaErrorInvalidValue;
@@ -879,11 +884,15 @@ cudaError_t launch_topk_final(const TopkFinalSpec& spec, int k, uint32_t* out_g,
       });
       if (attr != cudaSuccess) return attr;
       k_topk_merge_heads<<<1, kMhThreads, smem, s>>>(pk, pi, ctas, k, spec.total_bits, out_g, out_count,
-                                                     (uint64_t*)gst);
+                                                     (uint64_t*)gst, fin, n_fin);
     } else {
-      // the padded lists as one array (padding skipped)
+      // the padded lists as one array (padding skipped), then the outputs
       k_topk_warp<1024><<<1, 1024, 0, s>>>(pk, pi, nullptr, (uint64_t)ctas * k, k, nullptr, out_g, out_count, 1,
                                            nullptr, (uint64_t*)gst, spec.total_bits);
+      if (n_fin > 0) {
+        const cudaError_t e = launch_finalize(fin, n_fin, out_g, out_count, (uint64_t)k, s);
+        if (e != cudaSuccess) return e;
+      }
     }
   }
   return cudaGetLastError();

@@ -146,14 +146,32 @@ size_t topk_final_temp_bytes(uint64_t n_max, int k, unsigned max_ctas = 0);
 // The largest max_ctas whose temp fits in temp_bytes.
 unsigned topk_final_max_ctas_for(size_t temp_bytes, int k);
 // phase: 0 both kernels, 1 the first pass only, 2 the merge pass only (the
-// two phases as separate steps of a program, each timed on its own).
+// two phases as separate steps of a program, each timed on its own). With
+// `fin` (n_fin outputs) the merge pass also writes the winners' final
+// outputs, row i for winner i (as launch_finalize over out_g would).
 cudaError_t launch_topk_final(const TopkFinalSpec& spec, int k, uint32_t* out_g, uint64_t* out_count, void* temp,
-                              cudaStream_t s, unsigned max_ctas = 0, int phase = 0);
+                              cudaStream_t s, unsigned max_ctas = 0, int phase = 0, const FinalOut* fin = nullptr,
+                              int n_fin = 0);
 
 // ---- gathers for final materialization (k_misc.cu)
 // out[i] = in[idx[i]] for fixed width elements (4, 8 or 16 bytes).
 cudaError_t launch_gather_width(const void* in, int width, const uint32_t* idx, const uint64_t* count,
                                 uint64_t n_max, void* out, cudaStream_t s);
+
+// Late materialization of a scan's outputs (k_misc.cu): out[i] = f(src[rid[i]])
+// for i < *count, f a plain copy or one + - * with a constant in a
+// non-128-bit type (the VM's arithmetic and overflow rules).
+struct GatherOut {
+  const void* src;    // column, indexed by row id
+  void* out;
+  int32_t in_kind;    // 0: 32-bit signed (widened by sign), 1: 32-bit other (zero), 2: 64-bit
+  int32_t out_width;  // 4 or 8
+  int32_t op;         // 0: copy, else VM_ADD, VM_SUB or VM_MUL
+  int32_t type;       // arithmetic type of the op (P_I32, P_I64, P_F32, P_F64)
+  int64_t k;          // constant (bits)
+};
+cudaError_t launch_gather_outs(const GatherOut* outs, int n_outs, const uint32_t* rid, const uint64_t* count,
+                               uint64_t n_max, uint32_t* status, cudaStream_t s);
 
 // ---- scalar hooks (k_misc.cu): gpu_{add,mul}_scalar, gpu_{eq,lt,le,gt,ge}_scalar
 cudaError_t launch_scalar_arith(int op, int ptype, const void* in, uint64_t n, int64_t ilit, double flit, void* out,
