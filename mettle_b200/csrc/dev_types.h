@@ -257,6 +257,10 @@ struct PipeDesc {
   // kMatScanTiles tiles; chunk_pos[c] = rows before chunk c
   uint32_t* tile_pos;
   uint64_t* chunk_pos;
+  // with it, the count pass also writes each tile's survivors as a 256-bit
+  // mask (8 words), and the scan expands the masks into the surviving row
+  // ids (out_rids[drive_src]) in place of a write pass
+  uint32_t* tile_mask;
   int32_t lb_stall_first;           // failure injection: tile 0 never publishes its prefix
   // aggregates
   int32_t n_aggs;

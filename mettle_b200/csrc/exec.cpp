@@ -1546,6 +1546,14 @@ struct Compiler {
         const uint64_t chunks = (tiles + kMatScanTiles - 1) / kMatScanTiles;
         pb.d.tile_pos = (uint32_t*)scratch(std::max<uint64_t>(tiles, 1) * 4);
         pb.d.chunk_pos = (uint64_t*)scratch(std::max<uint64_t>(chunks, 1) * 8);
+        uint32_t* rid = nullptr;
+        if (late) {
+          // the count pass also writes the survivor masks, which the scan
+          // expands into row ids: no second pass over the table
+          rid = (uint32_t*)scratch(std::max<uint64_t>(1, n_max) * 4);
+          pb.d.tile_mask = (uint32_t*)scratch(std::max<uint64_t>(tiles, 1) * 32);
+          pb.d.out_rids[root] = rid;
+        }
         PipeBuilder count = pb;
         count.d.sink = SK_MAT_COUNT;
         push_pipeline(count, root_rows);
@@ -1555,14 +1563,9 @@ struct Compiler {
         sc.n_hint = root_rows;
         sc.name = "mat_scan";
         P.steps.push_back(sc);
-        P.kernels += 2;
+        P.kernels += late ? 3 : 2;
         pb.d.sink = SK_MAT_WRITE;
         if (late) {
-          uint32_t* rid = (uint32_t*)scratch(std::max<uint64_t>(1, n_max) * 4);
-          pb.d.n_out = 0;
-          pb.d.out_rid_mask = 1u << root;
-          pb.d.out_rids[root] = rid;
-          push_pipeline(pb, root_rows);
           GatherOut* go = (GatherOut*)scratch(gos.size() * sizeof(GatherOut));
           upload(go, gos.data(), gos.size() * sizeof(GatherOut));
           Step g;

@@ -1406,6 +1406,18 @@ __global__ void __launch_bounds__(kThreads, (SINK == SK_AGG_SCALAR || SINK == SK
     if (SINK == SK_MAT_COUNT) {
       // first pass of the two-pass compaction: the tile's survivors
       if (lane == 0) d.tile_pos[tile] = n_sel;
+      if (d.tile_mask) {
+        // and their 256-bit mask, built in the free selection buffer
+        uint32_t* const m = (uint32_t*)sel_out;
+        if (lane < 8) m[lane] = 0u;
+        __syncwarp();
+        for (uint32_t p = lane; p < n_sel; p += 32) {
+          const uint32_t r = ident ? p : (uint32_t)sel_in[p];
+          atomicOr(&m[r >> 5], 1u << (r & 31));
+        }
+        __syncwarp();
+        if (lane < 8) d.tile_mask[tile * 8 + lane] = m[lane];
+      }
     } else if (SINK == SK_MATERIALIZE || SINK == SK_MAT_WRITE) {
       const uint32_t total = n_sel;
       uint64_t base;
@@ -2393,12 +2405,41 @@ __global__ void __launch_bounds__(kMatScanThreads) k_mat_scan_chunks(uint64_t* _
   if (threadIdx.x == 0) *out_count = s_w[kMatScanThreads / 32 - 1];
 }
 
+// Survivor masks into row ids: one thread per mask word; the 8 words of a
+// tile are 8 consecutive lanes, which add up their counts with shuffles.
+__global__ void __launch_bounds__(256) k_mat_expand(const uint32_t* __restrict__ mask,
+                                                    const uint32_t* __restrict__ pos,
+                                                    const uint64_t* __restrict__ chunk_pos, uint64_t n_tiles,
+                                                    uint32_t* __restrict__ rid) {
+  const uint64_t w = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const uint64_t tile = w >> 3;
+  uint32_t bits = tile < n_tiles ? mask[w] : 0u;
+  const uint32_t c = __popc(bits);
+  uint32_t incl = c;
+#pragma unroll
+  for (int o = 1; o < 8; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o, 8);
+    if ((threadIdx.x & 7) >= (unsigned)o) incl += y;
+  }
+  if (tile >= n_tiles) return;
+  uint64_t at = (uint64_t)pos[tile] + chunk_pos[tile / kMatScanTiles] + (incl - c);
+  const uint32_t row0 = (uint32_t)(tile * kTile + (w & 7) * 32);
+  while (bits) {
+    const int b = __ffs(bits) - 1;
+    bits &= bits - 1;
+    rid[at++] = row0 + (uint32_t)b;
+  }
+}
+
 cudaError_t launch_mat_scan(const PipeDesc& d, uint64_t n_rows, cudaStream_t s) {
   const uint64_t n_tiles = (n_rows + kTile - 1) / kTile;
   const uint64_t n_chunks = (n_tiles + kMatScanTiles - 1) / kMatScanTiles;
   if (n_chunks > (uint64_t)kMatScanTiles) return cudaErrorInvalidValue;  // beyond 2^32 rows
   if (n_tiles) k_mat_scan_local<<<(unsigned)n_chunks, kMatScanThreads, 0, s>>>(d.tile_pos, n_tiles, d.chunk_pos);
   k_mat_scan_chunks<<<1, kMatScanThreads, 0, s>>>(d.chunk_pos, (uint32_t)n_chunks, d.out_count);
+  if (d.tile_mask && n_tiles)
+    k_mat_expand<<<(unsigned)((n_tiles * 8 + 255) / 256), 256, 0, s>>>(d.tile_mask, d.tile_pos, d.chunk_pos, n_tiles,
+                                                                       d.out_rids[d.drive_src]);
   return cudaGetLastError();
 }
 
