@@ -2405,29 +2405,27 @@ __global__ void __launch_bounds__(kMatScanThreads) k_mat_scan_chunks(uint64_t* _
   if (threadIdx.x == 0) *out_count = s_w[kMatScanThreads / 32 - 1];
 }
 
-// Survivor masks into row ids: one thread per mask word; the 8 words of a
-// tile are 8 consecutive lanes, which add up their counts with shuffles.
+// Survivor masks into row ids: one warp per tile at a time; for each of the
+// tile's 8 mask words every lane writes its own row when its bit is set, at
+// the word's offset plus the set bits below it, so each store instruction
+// covers consecutive positions.
 __global__ void __launch_bounds__(256) k_mat_expand(const uint32_t* __restrict__ mask,
                                                     const uint32_t* __restrict__ pos,
                                                     const uint64_t* __restrict__ chunk_pos, uint64_t n_tiles,
                                                     uint32_t* __restrict__ rid) {
-  const uint64_t w = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const uint64_t tile = w >> 3;
-  uint32_t bits = tile < n_tiles ? mask[w] : 0u;
-  const uint32_t c = __popc(bits);
-  uint32_t incl = c;
+  const uint32_t lane = threadIdx.x & 31, lt = (1u << lane) - 1u;
+  const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
+  for (uint64_t tile = (uint64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); tile < n_tiles;
+       tile += warps) {
+    const uint32_t mw = lane < 8 ? mask[tile * 8 + lane] : 0u;
+    uint64_t at = (uint64_t)pos[tile] + chunk_pos[tile / kMatScanTiles];
+    const uint32_t row0 = (uint32_t)(tile * kTile);
 #pragma unroll
-  for (int o = 1; o < 8; o <<= 1) {
-    const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o, 8);
-    if ((threadIdx.x & 7) >= (unsigned)o) incl += y;
-  }
-  if (tile >= n_tiles) return;
-  uint64_t at = (uint64_t)pos[tile] + chunk_pos[tile / kMatScanTiles] + (incl - c);
-  const uint32_t row0 = (uint32_t)(tile * kTile + (w & 7) * 32);
-  while (bits) {
-    const int b = __ffs(bits) - 1;
-    bits &= bits - 1;
-    rid[at++] = row0 + (uint32_t)b;
+    for (int w = 0; w < 8; ++w) {
+      const uint32_t bits = __shfl_sync(0xFFFFFFFFu, mw, w);
+      if ((bits >> lane) & 1u) rid[at + (uint64_t)__popc(bits & lt)] = row0 + (uint32_t)w * 32 + lane;
+      at += (uint64_t)__popc(bits);
+    }
   }
 }
 
@@ -2437,9 +2435,12 @@ cudaError_t launch_mat_scan(const PipeDesc& d, uint64_t n_rows, cudaStream_t s) 
   if (n_chunks > (uint64_t)kMatScanTiles) return cudaErrorInvalidValue;  // beyond 2^32 rows
   if (n_tiles) k_mat_scan_local<<<(unsigned)n_chunks, kMatScanThreads, 0, s>>>(d.tile_pos, n_tiles, d.chunk_pos);
   k_mat_scan_chunks<<<1, kMatScanThreads, 0, s>>>(d.chunk_pos, (uint32_t)n_chunks, d.out_count);
-  if (d.tile_mask && n_tiles)
-    k_mat_expand<<<(unsigned)((n_tiles * 8 + 255) / 256), 256, 0, s>>>(d.tile_mask, d.tile_pos, d.chunk_pos, n_tiles,
-                                                                       d.out_rids[d.drive_src]);
+  if (d.tile_mask && n_tiles) {
+    uint64_t blocks = (n_tiles + 7) / 8;
+    if (blocks > (uint64_t)sm_count() * 8) blocks = (uint64_t)sm_count() * 8;
+    k_mat_expand<<<(unsigned)blocks, 256, 0, s>>>(d.tile_mask, d.tile_pos, d.chunk_pos, n_tiles,
+                                                  d.out_rids[d.drive_src]);
+  }
   return cudaGetLastError();
 }
 
