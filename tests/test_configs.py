@@ -118,6 +118,30 @@ def test_c2_multi_predicate_and_empty(scan_conn):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("n", [1, 255, 256, 257, 100_003])
+def test_scan_row_ids_and_gather_edges(conn, n):
+    """The scan's late gather (survivor masks per 256-row tile, expanded into
+    row ids, outputs gathered at them) at sizes around a tile, with every row,
+    no row and the first half selected; each output type and constant
+    arithmetic compared with numpy in row order."""
+    init(conn, "1 GB", "1 GB")
+    r = np.random.default_rng(n)
+    d = {"a": np.arange(n, dtype=np.int32), "b": r.integers(-2**40, 2**40, n).astype(np.int64),
+         "c": r.random(n, dtype=np.float32), "e": r.integers(0, 2**50, n).astype(np.int64)}
+    conn.create_table("t", {"a": (L.T_INTEGER, d["a"]), "b": (L.T_BIGINT, d["b"]), "c": (L.T_FLOAT, d["c"]),
+                            "e": (L.T_TIMESTAMP, d["e"])})
+    conn.gpu_register_table("t")
+    for where, m in (("a >= 0", d["a"] >= 0), ("a < 0", d["a"] < 0), (f"a < {n // 2}", d["a"] < n // 2)):
+        res = conn.gpu_processing(f"SELECT a, b - 7 AS b7, c * 3 AS c3, e, a * 2 AS a2 FROM t WHERE {where}")
+        assert res.rows == int(m.sum()), where
+        assert np.array_equal(res.columns[0], d["a"][m])
+        assert np.array_equal(res.columns[1], d["b"][m] - 7)
+        assert np.array_equal(res.columns[2], (d["c"][m] * np.float32(3)).astype(np.float32))
+        assert np.array_equal(res.columns[3], d["e"][m])
+        assert np.array_equal(res.columns[4], d["a"][m] * 2)
+
+
+@pytest.mark.gpu
 def test_c2_full_size(conn):
     """The measured scan at its full size: 10^8 rows, half of them selected,
     every output column compared in row order with the oracle's gathers."""
