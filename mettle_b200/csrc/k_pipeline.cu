@@ -1241,7 +1241,9 @@ __global__ void __launch_bounds__(kThreads, (SINK == SK_AGG_SCALAR || SINK == SK
         kk[j] = (uint64_t)((int64_t)kv[j] - fz_kmin);
         const bool inb = pass && kk[j] < fz_cap;
         w[j] = inb ? __ldg(fz_bits + (kk[j] >> 5)) : 0u;
-        mv[j] = inb ? __ldg(fz_map + kk[j]) : 0u;
+        // the slot only when grouping by it (always loaded by the slot sink,
+        // whose code then stays that of the common case)
+        mv[j] = inb && (SINK == SK_AGG_SLOT || fz_want_slot) ? __ldg(fz_map + kk[j]) : 0u;
       }
       uint32_t km = 0;
 #pragma unroll
